@@ -1,0 +1,597 @@
+"""Benchmark of photon-differential splatting forward+backward on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
+                    [--workload batch64|uniform1m|contention]
+
+Workloads (synthetic, seeded; the reference publishes no benchmark and its photons come from
+OptiX tracing, which these generators replace):
+  batch64     (default) 64 independent simulations, photon counts ~ logU[2^16, 2^22]
+              (62.6 M photons in all), square images drawn from {256, 512, 1024}^2,
+              half-uniform/half-clustered photons with differentials s ~ logU[0.5, 4] px,
+              max_pixel_radius 20, fp32. One step = binning + forward + backward of every
+              simulation (one Landweber iteration's splatting work) with fixed upstream
+              gradients.
+  uniform1m   2^20 photons on one 512^2 image (the CPU-runnable case).
+  contention  2^26 photons on 2048^2, 80% on 4 sharp caustic curves, s ~ logU[0.25, 16].
+
+Arms:
+  ours           the sm_100a kernels through the C ABI; batched steps replay one CUDA graph.
+  reference      the reference's splat formula on the host cores: the CPU port in
+                 oracle/pds_oracle.c in the reference's float32 arithmetic (REF32 mode), all
+                 host threads, on a bounded photon sample per step (the reference itself has
+                 no CPU implementation of this path).
+  reference-gpu  the reference's own CUDA extension (built unmodified from its sources into
+                 oracle/_ref), run as the reference runs it: one pds_forward + pds_backward
+                 per simulation.
+
+Prints one JSON line (rank 0). Multi-GPU (torchrun, one process per GPU): every rank runs
+its own independently seeded batch (the simulations shard with no data-path exchange), the
+step time is the max over ranks, and value counts the photons of all ranks ("weak").
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from shapefromcaustics_b200 import synthetic as S  # noqa: E402
+
+METRIC = "photon fwd+bwd splats/s"
+UNIT = "photons/s"
+MPR = 20
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4, nominal (no measured figure)
+# FLOPs per visited box pixel, counted from the reference formula
+# (photon_differentials.cu:98-106 forward, :179-205 backward).
+FLOP_FWD_PX = 22
+FLOP_BWD_PX = 55
+
+
+# ------------------------------------------------------------------ environment ----------
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms; keeps the samples whose
+    timestamps fall in the windows marked with mark_start/mark_stop."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.windows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._reader, daemon=True)
+        self.thread.start()
+
+    def _reader(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), line.strip()))
+
+    def mark_start(self):
+        self.windows.append([time.time(), None])
+
+    def mark_stop(self):
+        self.windows[-1][1] = time.time()
+
+    def stop(self):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for t, line in self.samples:
+            if any(a <= t <= (b or 1e300) + 0.15 for a, b in self.windows):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples in window"],
+                    "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def barrier(world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(v, world, device):
+    if world == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world, device):
+    if world == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ workloads ------------
+
+def workload(name, rank, device):
+    """-> (specs, concatenated photons on device, flat upstream gradient on device, desc)."""
+    seed = 1000 + rank
+    if name == "batch64":
+        specs = S.batch_specs(64, seed=seed)
+        photons = S.batch_photons(specs, seed=seed, device=device)
+        desc = ("64 simulations, N_i ~ logU[2^16,2^22], images {256,512,1024}^2, "
+                "uniform+cluster photons, s ~ logU[0.5,4] px, mpr 20, fp32")
+    elif name == "uniform1m":
+        specs = [(2 ** 20, (1, 512, 512))]
+        photons = S.uniform_cluster_photons(2 ** 20, 512, 512, seed=seed, device=device)
+        desc = "2^20 photons, 512^2, uniform+cluster, s ~ logU[0.5,4] px, mpr 20, fp32"
+    elif name == "contention":
+        specs = [(2 ** 26, (1, 2048, 2048))]
+        photons = S.caustic_curve_photons(2 ** 26, 2048, 2048, seed=seed, device=device)
+        desc = ("2^26 photons, 2048^2, 80% on 4 caustic curves (1.5 px), "
+                "s ~ logU[0.25,16] px, mpr 20, fp32")
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    grads = [S.upstream_grad(shape, seed=seed * 7919 + s, device=device).reshape(-1)
+             for s, (_, shape) in enumerate(specs)]
+    return specs, photons, torch.cat(grads).contiguous(), desc
+
+
+def split_photons(specs, photons):
+    """Per-simulation contiguous copies (the plain per-simulation loop needs them)."""
+    out, b = [], 0
+    for n, _ in specs:
+        out.append(tuple(t[..., b:b + n].contiguous() for t in photons))
+        b += n
+    return out
+
+
+def box_pixels(specs, photons, mpr):
+    """Visited box pixels per direction (the reference's loop trip count, clipped to the
+    image), computed with the reference's double-precision footprint rule."""
+    E, X, M, C, R = photons
+    total, b = 0, 0
+    for n, (_, H, W) in specs:
+        x = X[0, b:b + n].double()
+        y = X[1, b:b + n].double()
+        r = R[b:b + n].double()
+        rx = torch.clamp(torch.ceil(r * 0.5 * W), max=mpr)
+        ry = torch.clamp(torch.ceil(r * 0.5 * H), max=mpr)
+        pxc = torch.trunc((0.5 * x + 0.5) * W)
+        pyc = torch.trunc((0.5 * y + 0.5) * H)
+        w = (torch.clamp(pxc + rx, max=W - 1) - torch.clamp(pxc - rx, min=0) + 1).clamp(min=0)
+        h = (torch.clamp(pyc + ry, max=H - 1) - torch.clamp(pyc - ry, min=0) + 1).clamp(min=0)
+        total += float((w * h).sum().item())
+        b += n
+    return total
+
+
+# ------------------------------------------------------------------ our arm --------------
+
+def sort_launches(batch):
+    from shapefromcaustics_b200._lib import lib  # noqa: F401
+    cb = batch.cfg.class_bits
+    bits = ((batch.n_tiles + 1) << cb).bit_length()
+    return (bits + 7) // 8
+
+
+def time_graph(graph, steps, stream):
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(steps):
+            graph.replay()
+            ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    return [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+
+
+def run_ours(args, rank, world, device):
+    from shapefromcaustics_b200.splatting import BatchedSplat, SplatPlan
+    torch.cuda.set_device(device)
+    specs, photons, gflat, desc = workload(args.workload, rank, device)
+    n_total = sum(n for n, _ in specs)
+    pixels = sum(C * H * W for _, (C, H, W) in specs)
+    batch = BatchedSplat(specs, MPR, device)
+    out = torch.empty(batch.image_elems, device=device)
+    grads = tuple(torch.empty_like(t) for t in photons[:3])
+    stream = torch.cuda.Stream(device)
+
+    def step():
+        batch.plan(*photons)
+        batch.forward(out)
+        batch.backward(gflat, grads)
+
+    # eager warm-up (also sets kernel attributes), then capture one graph of the whole step
+    stream.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        step()
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 3)):
+        graph.replay()
+    torch.cuda.synchronize()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    gpu_id = vis.split(",")[device.index].strip() if vis else str(device.index)
+    clocks = ClockSampler(gpu_id)
+    clocks.start()
+    time.sleep(0.3)
+    # ---- timed region: K graph replays ----
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.mark_start()
+    per_step = time_graph(graph, args.steps, stream)
+    clocks.mark_stop()
+    barrier(world)
+    total_ms = max_over_ranks(sum(per_step), world, device)
+    ms_per_step = total_ms / args.steps
+    photons_all = sum_over_ranks(float(n_total), world, device)
+    value = photons_all / (ms_per_step / 1e3)
+
+    # ---- roofline window: the same steps eager, CUDA events around each phase ----
+    phases = {"plan": [], "forward": [], "backward": []}
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(stream)
+            batch.plan(*photons)
+            e[1].record(stream)
+            batch.forward(out)
+            e[2].record(stream)
+            batch.backward(gflat, grads)
+            e[3].record(stream)
+            torch.cuda.synchronize()
+            phases["plan"].append(e[0].elapsed_time(e[1]))
+            phases["forward"].append(e[1].elapsed_time(e[2]))
+            phases["backward"].append(e[2].elapsed_time(e[3]))
+    ph_ms = {k: statistics.median(v) for k, v in phases.items()}
+
+    # ---- plain: one plan + forward + backward per simulation, like the reference's loop ----
+    per_sim = split_photons(specs, photons)
+    gviews = []
+    b = 0
+    for _, (C, H, W) in specs:
+        gviews.append(gflat[b:b + C * H * W].view(C, H, W))
+        b += C * H * W
+
+    def plain_step():
+        for (n, shape), ph, g in zip(specs, per_sim, gviews):
+            p = SplatPlan(*ph, shape, MPR)
+            p.forward()
+            p.backward(g)
+
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            plain_step()
+        torch.cuda.synchronize()
+        plain_steps = max(1, min(args.steps, 5))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        clocks.mark_start()
+        e0.record(stream)
+        for _ in range(plain_steps):
+            plain_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks.mark_stop()
+    plain_ms = max_over_ranks(e0.elapsed_time(e1) / plain_steps, world, device)
+    del per_sim
+
+    # ---- parity spot check: batched vs plain forward on simulation 0 ----
+    imgs = batch.images(out)
+    p0 = SplatPlan(*split_photons(specs[:1], photons)[0], specs[0][1], MPR)
+    ref0 = p0.forward()
+    torch.cuda.synchronize()
+    parity = float((imgs[0] - ref0).norm() / ref0.norm())
+
+    # ---- e2e: host (pinned) photons and gradients in, loss out, through the public API ----
+    host_ph = [t.cpu().pin_memory() for t in photons]
+    host_g = gflat.cpu().pin_memory()
+    dev_ph = [torch.empty_like(t) for t in photons]
+    dev_g = torch.empty_like(gflat)
+    loss_host = torch.empty(1, dtype=torch.float32).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host_ph) + host_g.numel() * 4
+    e2e_steps = max(1, min(args.steps, 5))
+    with torch.cuda.stream(stream):
+        def e2e_step():
+            for d, h in zip(dev_ph, host_ph):
+                d.copy_(h, non_blocking=True)
+            dev_g.copy_(host_g, non_blocking=True)
+            batch.plan(*dev_ph)
+            batch.forward(out)
+            batch.backward(dev_g, grads)
+            loss_host.copy_(torch.dot(out, dev_g).reshape(1), non_blocking=True)
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world, device)
+    clocks.stop()
+
+    # ---- roofline of the dominant phase ----
+    peak, peak_kind = measured_peaks()
+    pix_box = box_pixels(specs, photons, MPR)
+    alg = {"plan": n_total * 40,
+           "forward": n_total * 40 + pixels * 4,
+           "backward": n_total * 76 + pixels * 4}
+    flops = {"plan": 0, "forward": pix_box * FLOP_FWD_PX, "backward": pix_box * FLOP_BWD_PX}
+    dom = max(("forward", "backward"), key=lambda k: ph_ms[k])
+    achieved = alg[dom] / (ph_ms[dom] / 1e3) / 1e9
+    simt = flops[dom] / (ph_ms[dom] / 1e3) / 1e12
+    passes = sort_launches(batch)
+    launches_per_step = 1 + 5 * passes + 2 + 2
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators; photons resident in HBM)",
+        "config": {"workload": f"{args.workload}: {desc}", "photons_per_gpu": n_total,
+                   "simulations_per_gpu": len(specs), "image_pixels_per_gpu": pixels,
+                   "max_pixel_radius": MPR, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"simulation-sharded x{world}, no collective",
+                   "mode": "batched: one CUDA graph per step (plan + fwd + bwd)"},
+        "landweber_it_per_s": {"batched": 1e3 / ms_per_step, "plain": 1e3 / plain_ms,
+                               "batched_over_plain": plain_ms / ms_per_step},
+        "phase_ms": ph_ms,
+        "roofline": {"bound": "hbm", "kernel": f"{dom} (tile kernel + tail)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes": alg[dom], "traffic": None},
+        "roofline_simt": {"kernel": dom, "achieved": simt, "peak": FP32_SIMT_NOMINAL_TFLOPS,
+                          "unit": "TFLOP/s", "frac": simt / FP32_SIMT_NOMINAL_TFLOPS,
+                          "peak_source": "nominal (148 SM x 128 FP32 x 2 x 1.965 GHz)",
+                          "box_pixels_per_step": pix_box},
+        "e2e": {"value": photons_all / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+        "gpu_launches": launches_per_step * args.steps,
+        "parity_batched_vs_plain_relL2": parity,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(specs, photons, gflat, budget_s=args.cpu_seconds)
+    return result
+
+
+# ------------------------------------------------------------------ CPU (reference) ------
+
+def cpu_sample(specs, photons, gflat, target):
+    """A bounded sample of the workload: the first simulations' photons up to `target`."""
+    take, b, gb = [], 0, 0
+    got = 0
+    for n, shape in specs:
+        C, H, W = shape
+        k = min(n, target - got)
+        if k <= 0:
+            break
+        take.append((k, shape, b, gb))
+        got += k
+        b += n
+        gb += C * H * W
+    return take
+
+
+def cpu_run(take, photons_cpu, g_cpu, threads, mode="ref32"):
+    from oracle import oracle as O
+    E, X, M, C, R = photons_cpu
+    t0 = time.perf_counter()
+    n = 0
+    for k, shape, b, gb in take:
+        sl = slice(b, b + k)
+        Cc, H, W = shape
+        G = g_cpu[gb:gb + Cc * H * W].reshape(Cc, H, W).double().numpy()
+        args = (E[sl].numpy(), X[:, sl].numpy(), M[:, :, sl].numpy(), C[:, sl].numpy(), R[sl].numpy())
+        O.forward(*args, shape, MPR, mode=mode, threads=threads)
+        O.backward(G, *args, MPR, mode=mode, threads=threads)
+        n += k
+    return n, time.perf_counter() - t0
+
+
+def cpu_baseline(specs, photons, gflat, budget_s=15.0):
+    threads = os.cpu_count() or 1
+    photons_cpu = [t.cpu() for t in photons]
+    g_cpu = gflat.cpu()
+    # size the sample from a short probe so the timed CPU run takes about budget_s
+    probe = cpu_sample(specs, photons_cpu, g_cpu, 2 ** 17)
+    n, dt = cpu_run(probe, photons_cpu, g_cpu, threads)
+    target = int(max(2 ** 17, min(sum(n for n, _ in specs), n / max(dt, 1e-3) * budget_s)))
+    take = cpu_sample(specs, photons_cpu, g_cpu, target)
+    n, dt = cpu_run(take, photons_cpu, g_cpu, threads)
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {n} photons of the workload ({len(take)} simulations), "
+                      f"fwd+bwd, reference float32 arithmetic, {dt:.1f} s"}
+
+
+def run_reference_cpu(args, rank, world):
+    if rank != 0:
+        return None
+    sample = int(args.ref_sample)
+    specs, photons, gflat, desc = workload_cpu(args.workload, sample)
+    threads = os.cpu_count() or 1
+    take = cpu_sample(specs, photons, gflat, sample)
+    for _ in range(args.warmup):
+        cpu_run(take[:1], photons, gflat, threads)
+    times, n = [], 0
+    for _ in range(args.steps):
+        n, dt = cpu_run(take, photons, gflat, threads)
+        times.append(dt)
+    ms = 1e3 * sum(times) / len(times)
+    value = n / (ms / 1e3)
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"{args.workload}: {desc}", "max_pixel_radius": MPR,
+                       "sample_photons_per_step": n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{n} photons per step (first simulations of the "
+                                       f"workload), fwd+bwd, reference float32 arithmetic"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def workload_cpu(name, target):
+    """The workload's leading simulations (enough for `target` photons), drawn on the CPU."""
+    if name != "batch64":
+        specs, photons, gflat, desc = workload(name, 0, "cpu")
+        return specs, photons, gflat, desc
+    seed = 1000
+    specs_all = S.batch_specs(64, seed=seed)
+    specs, got = [], 0
+    for sp in specs_all:
+        if got >= target:
+            break
+        specs.append(sp)
+        got += sp[0]
+    parts = [S.uniform_cluster_photons(n, H, W, seed=seed * 1000003 + s, device="cpu")
+             for s, (n, (C, H, W)) in enumerate(specs)]
+    photons = tuple(torch.cat([p[k] for p in parts], dim=-1).contiguous() for k in range(5))
+    grads = [S.upstream_grad(shape, seed=seed * 7919 + s).reshape(-1)
+             for s, (_, shape) in enumerate(specs)]
+    desc = ("64 simulations, N_i ~ logU[2^16,2^22], images {256,512,1024}^2, "
+            "uniform+cluster photons, s ~ logU[0.5,4] px, mpr 20, fp32")
+    return specs, photons, torch.cat(grads), desc
+
+
+def run_reference_gpu(args, rank, world, device):
+    try:
+        from oracle import build_ref
+        ref = build_ref.load_module()
+    except Exception as e:
+        return {"impl": "reference-gpu", "unavailable": f"reference extension not built: {e}"}
+    torch.cuda.set_device(device)
+    specs, photons, gflat, desc = workload(args.workload, rank, device)
+    n_total = sum(n for n, _ in specs)
+    per_sim = split_photons(specs, photons)
+    gviews, b = [], 0
+    for _, (C, H, W) in specs:
+        gviews.append(gflat[b:b + C * H * W].view(C, H, W))
+        b += C * H * W
+
+    def step():
+        for (n, shape), ph, g in zip(specs, per_sim, gviews):
+            ref.pds_forward(*ph, list(shape), MPR)
+            ref.pds_backward(g, *ph, MPR)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, device)
+    photons_all = sum_over_ranks(float(n_total), world, device)
+    return {"metric": METRIC, "value": photons_all / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference-gpu",
+            "config": {"workload": f"{args.workload}: {desc}", "max_pixel_radius": MPR,
+                       "mode": "plain: pds_forward + pds_backward per simulation"}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--workload", default="batch64", choices=["batch64", "uniform1m", "contention"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-sample", type=float, default=2 ** 21)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if world > 1:
+            import datetime
+            torch.distributed.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        res = run_reference_cpu(args, rank, world)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(res))
+        return
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(device)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=device)
+    if args.impl == "reference-gpu":
+        res = run_reference_gpu(args, rank, world, device)
+    else:
+        res = run_ours(args, rank, world, device)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * pds_b200.h -- C ABI of the B200 (sm_100a) photon-differential splatting library
+ * (libpds_b200.so).
+ *
+ * Drop-in boundary for the reference's torch extension module `PhotonDifferentialSplatting`
+ * (PyOptix/PhotonDifferentialSplattig.cpp:34-38), whose two ops are
+ *   pds_forward(Ep, xp, Mp, cp, radius, output_size, max_pixel_radius) -> [pds_grid]
+ *     (PhotonDifferentialSplattig.cpp:12-25 -> PyOptix/kernel/photon_differentials.cu:115-134)
+ *   pds_backward(grad_pds, Ep, xp, Mp, cp, radius, max_pixel_radius) -> [gE, gx, gM]
+ *     (PhotonDifferentialSplattig.cpp:27-32 -> PyOptix/kernel/photon_differentials.cu:223-247)
+ *
+ * Layouts are the reference's (all contiguous, photon index fastest):
+ *   Ep[N] f32, xp[2][N] f32 (normalised receiver coordinates in [-1,1]), Mp[2][3][N] f32
+ *   (change-of-basis rows; column 2 multiplies zero and is never read), cp[1][N] int64
+ *   (channel), radius[N] f32, images [C][H][W] f32.
+ *
+ * Conventions of every entry point:
+ *   - Nothing is allocated. Outputs and a device workspace come from the caller; the
+ *     workspace size comes from the *_workspace_bytes queries.
+ *   - Work is enqueued on `stream` (a cudaStream_t passed as void*; NULL = legacy default
+ *     stream) and is asynchronous. No entry point synchronises, so every entry point can be
+ *     captured into a CUDA graph.
+ *   - Return 0 (PDS_OK) on success, a PDS_ERR_* code otherwise; pds_last_error() gives the
+ *     message of the calling thread's last failure.
+ *   - Photons whose channel lies outside [0, C) contribute nothing and get zero gradients
+ *     (the reference checks only c < C, photon_differentials.cu:75, and leaves its
+ *     empty_like gradient outputs unwritten for them).
+ */
+#ifndef PDS_B200_H
+#define PDS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDS_OK 0
+#define PDS_ERR_INVALID_ARGUMENT 1 /* shapes, sizes, pointers or alignment */
+#define PDS_ERR_WORKSPACE 2        /* workspace missing or smaller than required */
+#define PDS_ERR_CUDA 3             /* a CUDA launch or runtime call failed */
+#define PDS_ERR_UNSUPPORTED 4      /* configuration outside what the kernels handle */
+
+/* Kernel tuning. A NULL pointer or a zero field selects the default. */
+typedef struct pds_config {
+    int32_t tile;       /* screen-tile edge in pixels: 16, 32 or 64 (default 32) */
+    int32_t chunk;      /* sorted photons per CTA work item, multiple of 256 (default 2048) */
+    int32_t class_bits; /* footprint-size bits appended to the sort key, 0..4 (default 0) */
+    int32_t apron_max;  /* largest footprint radius (px) the tile path holds (default 32);
+                           larger footprints take the direct path */
+} pds_config;
+
+/* One simulation of a batch. The caller fills photon_begin, n_photons, image_offset,
+ * channels, height, width; pds_batch_layout fills the tile fields. */
+typedef struct pds_sim {
+    int64_t photon_begin; /* first photon of this simulation in the concatenated arrays */
+    int64_t n_photons;
+    int64_t image_offset; /* element offset of this simulation's [C][H][W] image */
+    int32_t channels, height, width;
+    int32_t tiles_x, tiles_y; /* filled by pds_batch_layout */
+    int32_t tile_base;        /* filled by pds_batch_layout */
+    int32_t reserved[2];
+} pds_sim;
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* pds_last_error(void);
+
+/* Library version string. */
+const char* pds_version(void);
+
+/* ---- single simulation: the reference's two ops ---------------------------------- */
+
+/* Workspace bytes for one forward or backward call over N photons into [C][H][W]. */
+size_t pds_workspace_bytes(int64_t n_photons, int64_t channels, int64_t height, int64_t width,
+                           const pds_config* cfg);
+
+/* pds_forward (PhotonDifferentialSplattig.cpp:12-25, photon_differentials.cu:60-134):
+ * out[C][H][W] is overwritten (the callee zeroes it). */
+int pds_forward_f32(const float* Ep, const float* xp, const float* Mp, const int64_t* cp,
+                    const float* radius, int64_t n_photons, int64_t channels, int64_t height,
+                    int64_t width, int32_t max_pixel_radius, float* out, void* workspace,
+                    size_t workspace_bytes, const pds_config* cfg, void* stream);
+
+/* pds_backward (PhotonDifferentialSplattig.cpp:27-32, photon_differentials.cu:136-247):
+ * grad_pds[C][H][W] in; grad_Ep[N], grad_xp[2][N], grad_Mp[2][3][N] overwritten
+ * (grad_Mp[.][2] = 0). */
+int pds_backward_f32(const float* grad_pds, const float* Ep, const float* xp, const float* Mp,
+                     const int64_t* cp, const float* radius, int64_t n_photons,
+                     int64_t channels, int64_t height, int64_t width, int32_t max_pixel_radius,
+                     float* grad_Ep, float* grad_xp, float* grad_Mp, void* workspace,
+                     size_t workspace_bytes, const pds_config* cfg, void* stream);
+
+/* ---- plan reuse: one binning + sort shared by a forward and its backward ------------ */
+/* The plan lives in the workspace. pds_plan_f32 builds it; the *_planned calls use it and
+ * must get the same photon arrays, sizes, max_pixel_radius and config. Same references as
+ * the two ops above (the reference recomputes the footprints in each kernel,
+ * photon_differentials.cu:76-89 and :155-167). */
+int pds_plan_f32(const float* Ep, const float* xp, const float* Mp, const int64_t* cp,
+                 const float* radius, int64_t n_photons, int64_t channels, int64_t height,
+                 int64_t width, int32_t max_pixel_radius, void* workspace,
+                 size_t workspace_bytes, const pds_config* cfg, void* stream);
+int pds_forward_planned_f32(const float* Ep, const float* xp, const float* Mp,
+                            const int64_t* cp, const float* radius, int64_t n_photons,
+                            int64_t channels, int64_t height, int64_t width,
+                            int32_t max_pixel_radius, float* out, void* workspace,
+                            size_t workspace_bytes, const pds_config* cfg, void* stream);
+int pds_backward_planned_f32(const float* grad_pds, const float* Ep, const float* xp,
+                             const float* Mp, const int64_t* cp, const float* radius,
+                             int64_t n_photons, int64_t channels, int64_t height,
+                             int64_t width, int32_t max_pixel_radius, float* grad_Ep,
+                             float* grad_xp, float* grad_Mp, void* workspace,
+                             size_t workspace_bytes, const pds_config* cfg, void* stream);
+
+/* ---- batches of uneven simulations in one launch sequence -------------------------- */
+/* The reference runs its simulations one after another and sums them
+ * (shape_from_caustics.py:351-353); these entry points run many simulations, each with
+ * its own photon count and image size, through one binning, one sort and one persistent
+ * launch per direction. Photon arrays are the simulations' arrays concatenated (stride
+ * n_total); images live in one flat buffer at each simulation's image_offset. */
+
+/* Fills tiles_x, tiles_y, tile_base of sims[0..n_sims) (host memory) for cfg and returns
+ * the total tile count in *n_tiles_total. */
+int pds_batch_layout(pds_sim* sims, int32_t n_sims, const pds_config* cfg,
+                     int64_t* n_tiles_total);
+
+size_t pds_batch_workspace_bytes(int64_t n_total, int64_t n_tiles_total, const pds_config* cfg);
+
+/* sims_dev: the laid-out table in device memory. out: flat image buffer, overwritten over
+ * [0, image_elems) where image_elems = max(image_offset + C*H*W). */
+int pds_batch_plan_f32(const float* Ep, const float* xp, const float* Mp, const int64_t* cp,
+                       const float* radius, int64_t n_total, const pds_sim* sims_dev,
+                       int32_t n_sims, int64_t n_tiles_total, int32_t max_pixel_radius,
+                       void* workspace, size_t workspace_bytes, const pds_config* cfg,
+                       void* stream);
+int pds_batch_forward_planned_f32(const float* Ep, const float* xp, const float* Mp,
+                                  const int64_t* cp, const float* radius, int64_t n_total,
+                                  const pds_sim* sims_dev, int32_t n_sims,
+                                  int64_t n_tiles_total, int64_t image_elems,
+                                  int32_t max_pixel_radius, float* out, void* workspace,
+                                  size_t workspace_bytes, const pds_config* cfg, void* stream);
+int pds_batch_backward_planned_f32(const float* grad, const float* Ep, const float* xp,
+                                   const float* Mp, const int64_t* cp, const float* radius,
+                                   int64_t n_total, const pds_sim* sims_dev, int32_t n_sims,
+                                   int64_t n_tiles_total, int32_t max_pixel_radius,
+                                   float* grad_Ep, float* grad_xp, float* grad_Mp,
+                                   void* workspace, size_t workspace_bytes,
+                                   const pds_config* cfg, void* stream);
+
+/* ---- device radix sort (exposed for its bit-exactness tests) ----------------------- */
+/* Stable ascending sort of keys[n] (only the low key_bits bits are compared) carrying the
+ * original index: perm_out[k] = index of the k-th smallest key, keys_out the sorted keys. */
+size_t pds_sort_workspace_bytes(int64_t n);
+int pds_sort_u32(const uint32_t* keys, int64_t n, int32_t key_bits, uint32_t* keys_out,
+                 uint32_t* perm_out, void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDS_B200_H */

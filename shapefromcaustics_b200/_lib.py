@@ -1,0 +1,109 @@
+"""ctypes binding of ``libpds_b200.so`` (the C ABI declared in ``include/pds_b200.h``).
+
+The library is the only compute path: if it is missing or fails to load, every op raises.
+There is no CPU or eager-PyTorch fallback.
+"""
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpds_b200.so")
+
+PDS_OK = 0
+PDS_ERR_INVALID_ARGUMENT = 1
+PDS_ERR_WORKSPACE = 2
+PDS_ERR_CUDA = 3
+PDS_ERR_UNSUPPORTED = 4
+
+
+class PdsConfig(ctypes.Structure):
+    """Mirror of ``pds_config``."""
+    _fields_ = [("tile", ctypes.c_int32), ("chunk", ctypes.c_int32),
+                ("class_bits", ctypes.c_int32), ("apron_max", ctypes.c_int32)]
+
+
+class PdsSim(ctypes.Structure):
+    """Mirror of ``pds_sim`` (56 bytes)."""
+    _fields_ = [("photon_begin", ctypes.c_int64), ("n_photons", ctypes.c_int64),
+                ("image_offset", ctypes.c_int64), ("channels", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("width", ctypes.c_int32),
+                ("tiles_x", ctypes.c_int32), ("tiles_y", ctypes.c_int32),
+                ("tile_base", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
+
+
+assert ctypes.sizeof(PdsSim) == 56
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I32 = ctypes.c_int32
+_SZ = ctypes.c_size_t
+_CFG = ctypes.POINTER(PdsConfig)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "pds_last_error": (ctypes.c_char_p, []),
+    "pds_version": (ctypes.c_char_p, []),
+    "pds_workspace_bytes": (_SZ, [_I64, _I64, _I64, _I64, _CFG]),
+    "pds_forward_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _I32, _P, _P,
+                                       _SZ, _CFG, _P]),
+    "pds_backward_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _I32, _P,
+                                        _P, _P, _P, _SZ, _CFG, _P]),
+    "pds_plan_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _I32, _P, _SZ,
+                                    _CFG, _P]),
+    "pds_forward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _I64, _I64, _I64, _I32,
+                                               _P, _P, _SZ, _CFG, _P]),
+    "pds_backward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I64, _I64,
+                                                _I32, _P, _P, _P, _P, _SZ, _CFG, _P]),
+    "pds_batch_layout": (ctypes.c_int, [ctypes.POINTER(PdsSim), _I32, _CFG,
+                                        ctypes.POINTER(_I64)]),
+    "pds_batch_workspace_bytes": (_SZ, [_I64, _I64, _CFG]),
+    "pds_batch_plan_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P, _I32, _I64, _I32, _P, _SZ,
+                                          _CFG, _P]),
+    "pds_batch_forward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P, _I32, _I64,
+                                                     _I64, _I32, _P, _P, _SZ, _CFG, _P]),
+    "pds_batch_backward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _P, _I32,
+                                                      _I64, _I32, _P, _P, _P, _P, _SZ, _CFG, _P]),
+    "pds_sort_workspace_bytes": (_SZ, [_I64]),
+    "pds_sort_u32": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P, _SZ, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class PdsError(RuntimeError):
+    """A failure reported by the library (carries the PDS_ERR_* code)."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+def lib():
+    """The loaded library; raises ImportError if it has not been built."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.isfile(LIB_PATH):
+                    raise ImportError(
+                        f"{LIB_PATH} is missing: build it with "
+                        "`python -m shapefromcaustics_b200.build` (nvcc, sm_100a)")
+                l = ctypes.CDLL(LIB_PATH)
+                for name, (res, args) in SIGNATURES.items():
+                    f = getattr(l, name)
+                    f.restype = res
+                    f.argtypes = args
+                _lib = l
+    return _lib
+
+
+def check(rc):
+    if rc != PDS_OK:
+        msg = lib().pds_last_error().decode(errors="replace")
+        raise PdsError(rc, msg)
+
+
+def config(tile=0, chunk=0, class_bits=0, apron_max=0):
+    return PdsConfig(int(tile), int(chunk), int(class_bits), int(apron_max))

@@ -1,0 +1,480 @@
+// extern "C" entry points of libpds_b200.so (declared in include/pds_b200.h).
+//
+// This layer validates arguments the way the reference's binding does
+// (PyOptix/PhotonDifferentialSplattig.cpp:14-22: matching photon counts, 2-row positions,
+// 2x3 matrices, one channel row), lays the workspace out, and enqueues
+//   plan:     counters reset, plan_kernel, radix sort
+//   forward:  output reset, fwd_tiles_kernel, tail_fwd_kernel
+//   backward: grad_Mp column-2 reset, bwd_tiles_kernel, tail_bwd_kernel
+// on the caller's stream. It allocates nothing and never synchronises. Failures return a
+// PDS_ERR_* code and leave a message for pds_last_error() (the reference raises through
+// TORCH_CHECK and does not check its launches, photon_differentials.cu:125, :234).
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "pds_internal.h"
+#include "pds_splat.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return PDS_ERR_CUDA;
+}
+
+int bit_length(uint64_t v) {
+    int b = 0;
+    while (v) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+struct Resolved {
+    pds::Cfg cfg;
+    int key_bits;
+    uint32_t key_big, key_invalid;
+};
+
+int resolve_cfg(const pds_config* in, pds_config& out) {
+    out.tile = (in && in->tile) ? in->tile : 32;
+    out.chunk = (in && in->chunk) ? in->chunk : 2048;
+    out.class_bits = in ? in->class_bits : 0;
+    out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
+    if (out.tile != 16 && out.tile != 32 && out.tile != 64)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.tile must be 16, 32 or 64");
+    if (out.chunk < 256 || out.chunk > (1 << 20) || out.chunk % 256 != 0)
+        return fail(PDS_ERR_INVALID_ARGUMENT,
+                    "pds_config.chunk must be a multiple of 256 in [256, 1048576]");
+    if (out.class_bits < 0 || out.class_bits > 4)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be in [0, 4]");
+    if (out.apron_max < 1 || out.apron_max > 63 || out.tile + 2 * out.apron_max > 255)
+        return fail(PDS_ERR_INVALID_ARGUMENT,
+                    "pds_config.apron_max must be in [1, 63] with tile + 2*apron_max <= 255");
+    return PDS_OK;
+}
+
+int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
+    pds_config c;
+    int rc = resolve_cfg(in, c);
+    if (rc) return rc;
+    if (n_tiles < 1 || n_tiles >= (int64_t(1) << 30))
+        return fail(PDS_ERR_UNSUPPORTED, "tile count outside [1, 2^30)");
+    const uint64_t inv = uint64_t(n_tiles + 1) << c.class_bits;
+    if (inv >= (uint64_t(1) << 32))
+        return fail(PDS_ERR_UNSUPPORTED, "sort key space exceeds 32 bits; lower class_bits");
+    r.cfg.tile = c.tile;
+    r.cfg.chunk = c.chunk;
+    r.cfg.class_bits = c.class_bits;
+    r.cfg.apron = mpr < 0 ? 0 : (mpr < c.apron_max ? mpr : c.apron_max);
+    r.cfg.sw = c.tile + 2 * r.cfg.apron;
+    r.key_big = uint32_t(uint64_t(n_tiles) << c.class_bits);
+    r.key_invalid = uint32_t(inv);
+    r.key_bits = bit_length(inv);
+    return PDS_OK;
+}
+
+struct Layout {
+    size_t counters, k0, k1, v0, v1, recs, aux, total;
+};
+
+Layout make_layout(int64_t n) {
+    Layout L;
+    const size_t nn = size_t(n > 0 ? n : 1);
+    size_t off = 0;
+    L.counters = off; off += 256;
+    L.k0 = off; off += pds::align_up(nn * 4, 256);
+    L.k1 = off; off += pds::align_up(nn * 4, 256);
+    L.v0 = off; off += pds::align_up(nn * 4, 256);
+    L.v1 = off; off += pds::align_up(nn * 4, 256);
+    L.recs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
+    L.aux = off; off += pds::sort_aux_bytes(n);
+    L.total = off;
+    return L;
+}
+
+struct Bufs {
+    uint32_t* counters;
+    uint32_t *k0, *k1, *v0, *v1;
+    pds::Rec* recs;
+    void* aux;
+};
+
+Bufs bufs(void* ws, const Layout& L) {
+    char* b = static_cast<char*>(ws);
+    Bufs r;
+    r.counters = reinterpret_cast<uint32_t*>(b + L.counters);
+    r.k0 = reinterpret_cast<uint32_t*>(b + L.k0);
+    r.k1 = reinterpret_cast<uint32_t*>(b + L.k1);
+    r.v0 = reinterpret_cast<uint32_t*>(b + L.v0);
+    r.v1 = reinterpret_cast<uint32_t*>(b + L.v1);
+    r.recs = reinterpret_cast<pds::Rec*>(b + L.recs);
+    r.aux = b + L.aux;
+    return r;
+}
+
+// The plan kernel writes raw keys into k1; pass p of the sort writes buffer (p & 1).
+void sorted_bufs(const Bufs& b, int key_bits, const uint32_t** keys, const uint32_t** idx) {
+    const int passes = pds::sort_passes(key_bits);
+    const bool in0 = passes == 0 || ((passes - 1) & 1) == 0;
+    *keys = in0 ? b.k0 : b.k1;
+    *idx = in0 ? b.v0 : b.v1;
+}
+
+int check_photons(const float* E, const float* X, const float* M, const int64_t* cp,
+                  const float* R, int64_t n) {
+    if (n < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative photon count");
+    if (n >= int64_t(0xFFFFFFFFll))
+        return fail(PDS_ERR_UNSUPPORTED, "photon count must be below 2^32 - 1");
+    if (n > 0 && (!E || !X || !M || !cp || !R))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null photon array");
+    return PDS_OK;
+}
+
+int check_ws(void* ws, size_t have, size_t need) {
+    if (!ws) return fail(PDS_ERR_WORKSPACE, "workspace is null");
+    if (reinterpret_cast<uintptr_t>(ws) % 256 != 0)
+        return fail(PDS_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+    if (have < need)
+        return fail(PDS_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) +
+                                           " bytes, got " + std::to_string(have));
+    return PDS_OK;
+}
+
+int check_image(int64_t C, int64_t H, int64_t W) {
+    if (C < 1 || H < 1 || W < 1)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "output_size entries must be positive");
+    if (H > 65535 || W > 65535)
+        return fail(PDS_ERR_UNSUPPORTED, "image height and width must be at most 65535");
+    if (C > 65535) return fail(PDS_ERR_UNSUPPORTED, "at most 65535 channels");
+    return PDS_OK;
+}
+
+pds_sim single_sim(int64_t n, int64_t C, int64_t H, int64_t W, int tile) {
+    pds_sim s;
+    std::memset(&s, 0, sizeof(s));
+    s.photon_begin = 0;
+    s.n_photons = n;
+    s.image_offset = 0;
+    s.channels = int32_t(C);
+    s.height = int32_t(H);
+    s.width = int32_t(W);
+    s.tiles_x = int32_t((W + tile - 1) / tile);
+    s.tiles_y = int32_t((H + tile - 1) / tile);
+    s.tile_base = 0;
+    return s;
+}
+
+pds::SimTable table_one(const pds_sim& s) {
+    pds::SimTable t;
+    t.dev = nullptr;
+    t.n = 1;
+    t.one = s;
+    return t;
+}
+
+pds::SimTable table_dev(const pds_sim* dev, int32_t n) {
+    pds::SimTable t;
+    std::memset(&t, 0, sizeof(t));
+    t.dev = dev;
+    t.n = n;
+    return t;
+}
+
+// ---- shared implementations -------------------------------------------------------
+
+int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, int32_t mpr,
+              const pds_config* cfg, void* ws, size_t ws_bytes, cudaStream_t s) {
+    Resolved r;
+    int rc = resolve(cfg, mpr, n_tiles, r);
+    if (rc) return rc;
+    const Layout L = make_layout(ph.n);
+    rc = check_ws(ws, ws_bytes, L.total);
+    if (rc) return rc;
+    const Bufs b = bufs(ws, L);
+    cudaError_t e = cudaMemsetAsync(b.counters, 0, 16, s);
+    if (e != cudaSuccess) return cuda_fail(e, "plan: counter reset");
+    if (ph.n == 0) return PDS_OK;
+    pds::PlanArgs a;
+    a.ph = ph;
+    a.sims = st;
+    a.mpr = mpr;
+    a.cfg = r.cfg;
+    a.key_big = r.key_big;
+    a.key_invalid = r.key_invalid;
+    a.keys = b.k1;
+    a.recs = b.recs;
+    a.counters = b.counters;
+    e = pds::launch_plan(a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "plan_kernel");
+    uint32_t *ko, *vo;
+    e = pds::radix_sort(b.k1, b.k0, b.k1, b.v0, b.v1, ph.n, r.key_bits, b.aux, s, &ko, &vo);
+    if (e != cudaSuccess) return cuda_fail(e, "radix sort");
+    return PDS_OK;
+}
+
+int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, int32_t mpr,
+              const pds_config* cfg, void* ws, size_t ws_bytes, pds::TileArgs& a) {
+    Resolved r;
+    int rc = resolve(cfg, mpr, n_tiles, r);
+    if (rc) return rc;
+    const Layout L = make_layout(ph.n);
+    rc = check_ws(ws, ws_bytes, L.total);
+    if (rc) return rc;
+    const Bufs b = bufs(ws, L);
+    std::memset(&a, 0, sizeof(a));
+    a.ph = ph;
+    a.sims = st;
+    a.mpr = mpr;
+    a.cfg = r.cfg;
+    sorted_bufs(b, r.key_bits, &a.skeys, &a.sidx);
+    a.recs = b.recs;
+    a.counters = b.counters;
+    return PDS_OK;
+}
+
+int forward_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles,
+                 int64_t image_elems, int32_t mpr, float* out, const pds_config* cfg, void* ws,
+                 size_t ws_bytes, cudaStream_t s) {
+    if (!out) return fail(PDS_ERR_INVALID_ARGUMENT, "null output image");
+    pds::TileArgs a;
+    int rc = tile_args(ph, st, n_tiles, mpr, cfg, ws, ws_bytes, a);
+    if (rc) return rc;
+    a.out = out;
+    cudaError_t e = cudaMemsetAsync(out, 0, size_t(image_elems) * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_fail(e, "forward: output reset");
+    if (ph.n == 0) return PDS_OK;
+    e = pds::launch_forward(a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "fwd_tiles_kernel");
+    return PDS_OK;
+}
+
+int backward_impl(const float* grad, const pds::Photons& ph, const pds::SimTable& st,
+                  int64_t n_tiles, int32_t mpr, float* gE, float* gX, float* gM,
+                  const pds_config* cfg, void* ws, size_t ws_bytes, cudaStream_t s) {
+    if (ph.n > 0 && (!grad || !gE || !gX || !gM))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
+    pds::TileArgs a;
+    int rc = tile_args(ph, st, n_tiles, mpr, cfg, ws, ws_bytes, a);
+    if (rc) return rc;
+    if (ph.n == 0) return PDS_OK;
+    a.grad = grad;
+    a.gE = gE;
+    a.gX = gX;
+    a.gM = gM;
+    // grad_Mp[0][2] and grad_Mp[1][2] multiply a zero in the reference (:198-205, :215, :218)
+    cudaError_t e = cudaMemsetAsync(gM + 2 * ph.n, 0, size_t(ph.n) * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(gM + 5 * ph.n, 0, size_t(ph.n) * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_fail(e, "backward: grad_Mp column-2 reset");
+    e = pds::launch_backward(a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bwd_tiles_kernel");
+    return PDS_OK;
+}
+
+pds::Photons photons(const float* E, const float* X, const float* M, const int64_t* cp,
+                     const float* R, int64_t n) {
+    pds::Photons p;
+    p.E = E; p.X = X; p.M = M; p.cp = cp; p.R = R; p.n = n;
+    return p;
+}
+
+int single_tiles(const pds_config* cfg, int64_t C, int64_t H, int64_t W, int64_t* n_tiles,
+                 pds_sim* sim, int64_t n) {
+    pds_config c;
+    int rc = resolve_cfg(cfg, c);
+    if (rc) return rc;
+    rc = check_image(C, H, W);
+    if (rc) return rc;
+    *sim = single_sim(n, C, H, W, c.tile);
+    *n_tiles = C * int64_t(sim->tiles_x) * sim->tiles_y;
+    return PDS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pds_last_error(void) { return g_err.c_str(); }
+
+const char* pds_version(void) { return "pds_b200 1.0 (sm_100a)"; }
+
+size_t pds_workspace_bytes(int64_t n, int64_t C, int64_t H, int64_t W, const pds_config* cfg) {
+    (void)C; (void)H; (void)W; (void)cfg;
+    return make_layout(n).total;
+}
+
+size_t pds_batch_workspace_bytes(int64_t n_total, int64_t n_tiles_total, const pds_config* cfg) {
+    (void)n_tiles_total; (void)cfg;
+    return make_layout(n_total).total;
+}
+
+int pds_plan_f32(const float* E, const float* X, const float* M, const int64_t* cp,
+                 const float* R, int64_t n, int64_t C, int64_t H, int64_t W, int32_t mpr,
+                 void* ws, size_t ws_bytes, const pds_config* cfg, void* stream) {
+    int rc = check_photons(E, X, M, cp, R, n);
+    if (rc) return rc;
+    pds_sim sim;
+    int64_t nt;
+    rc = single_tiles(cfg, C, H, W, &nt, &sim, n);
+    if (rc) return rc;
+    return plan_impl(photons(E, X, M, cp, R, n), table_one(sim), nt, mpr, cfg, ws, ws_bytes,
+                     static_cast<cudaStream_t>(stream));
+}
+
+int pds_forward_planned_f32(const float* E, const float* X, const float* M, const int64_t* cp,
+                            const float* R, int64_t n, int64_t C, int64_t H, int64_t W,
+                            int32_t mpr, float* out, void* ws, size_t ws_bytes,
+                            const pds_config* cfg, void* stream) {
+    int rc = check_photons(E, X, M, cp, R, n);
+    if (rc) return rc;
+    pds_sim sim;
+    int64_t nt;
+    rc = single_tiles(cfg, C, H, W, &nt, &sim, n);
+    if (rc) return rc;
+    return forward_impl(photons(E, X, M, cp, R, n), table_one(sim), nt, C * H * W, mpr, out,
+                        cfg, ws, ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int pds_backward_planned_f32(const float* G, const float* E, const float* X, const float* M,
+                             const int64_t* cp, const float* R, int64_t n, int64_t C, int64_t H,
+                             int64_t W, int32_t mpr, float* gE, float* gX, float* gM, void* ws,
+                             size_t ws_bytes, const pds_config* cfg, void* stream) {
+    int rc = check_photons(E, X, M, cp, R, n);
+    if (rc) return rc;
+    pds_sim sim;
+    int64_t nt;
+    rc = single_tiles(cfg, C, H, W, &nt, &sim, n);
+    if (rc) return rc;
+    return backward_impl(G, photons(E, X, M, cp, R, n), table_one(sim), nt, mpr, gE, gX, gM,
+                         cfg, ws, ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int pds_forward_f32(const float* E, const float* X, const float* M, const int64_t* cp,
+                    const float* R, int64_t n, int64_t C, int64_t H, int64_t W, int32_t mpr,
+                    float* out, void* ws, size_t ws_bytes, const pds_config* cfg, void* stream) {
+    int rc = pds_plan_f32(E, X, M, cp, R, n, C, H, W, mpr, ws, ws_bytes, cfg, stream);
+    if (rc) return rc;
+    return pds_forward_planned_f32(E, X, M, cp, R, n, C, H, W, mpr, out, ws, ws_bytes, cfg,
+                                   stream);
+}
+
+int pds_backward_f32(const float* G, const float* E, const float* X, const float* M,
+                     const int64_t* cp, const float* R, int64_t n, int64_t C, int64_t H,
+                     int64_t W, int32_t mpr, float* gE, float* gX, float* gM, void* ws,
+                     size_t ws_bytes, const pds_config* cfg, void* stream) {
+    int rc = pds_plan_f32(E, X, M, cp, R, n, C, H, W, mpr, ws, ws_bytes, cfg, stream);
+    if (rc) return rc;
+    return pds_backward_planned_f32(G, E, X, M, cp, R, n, C, H, W, mpr, gE, gX, gM, ws,
+                                    ws_bytes, cfg, stream);
+}
+
+int pds_batch_layout(pds_sim* sims, int32_t n_sims, const pds_config* cfg, int64_t* n_tiles) {
+    pds_config c;
+    int rc = resolve_cfg(cfg, c);
+    if (rc) return rc;
+    if (!sims || n_sims < 1 || !n_tiles)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_batch_layout: empty or null table");
+    int64_t base = 0, next_photon = 0;
+    for (int32_t s = 0; s < n_sims; ++s) {
+        pds_sim& d = sims[s];
+        rc = check_image(d.channels, d.height, d.width);
+        if (rc) return rc;
+        if (d.n_photons < 0 || d.photon_begin != next_photon)
+            return fail(PDS_ERR_INVALID_ARGUMENT,
+                        "simulations must cover the photon arrays contiguously and in order");
+        if (d.image_offset < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative image_offset");
+        next_photon += d.n_photons;
+        d.tiles_x = int32_t((d.width + c.tile - 1) / c.tile);
+        d.tiles_y = int32_t((d.height + c.tile - 1) / c.tile);
+        d.tile_base = int32_t(base);
+        base += int64_t(d.channels) * d.tiles_x * d.tiles_y;
+        if (base >= (int64_t(1) << 30)) return fail(PDS_ERR_UNSUPPORTED, "too many tiles");
+    }
+    *n_tiles = base;
+    return PDS_OK;
+}
+
+int pds_batch_plan_f32(const float* E, const float* X, const float* M, const int64_t* cp,
+                       const float* R, int64_t n_total, const pds_sim* sims_dev, int32_t n_sims,
+                       int64_t n_tiles, int32_t mpr, void* ws, size_t ws_bytes,
+                       const pds_config* cfg, void* stream) {
+    int rc = check_photons(E, X, M, cp, R, n_total);
+    if (rc) return rc;
+    if (!sims_dev || n_sims < 1) return fail(PDS_ERR_INVALID_ARGUMENT, "null simulation table");
+    return plan_impl(photons(E, X, M, cp, R, n_total), table_dev(sims_dev, n_sims), n_tiles, mpr,
+                     cfg, ws, ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int pds_batch_forward_planned_f32(const float* E, const float* X, const float* M,
+                                  const int64_t* cp, const float* R, int64_t n_total,
+                                  const pds_sim* sims_dev, int32_t n_sims, int64_t n_tiles,
+                                  int64_t image_elems, int32_t mpr, float* out, void* ws,
+                                  size_t ws_bytes, const pds_config* cfg, void* stream) {
+    int rc = check_photons(E, X, M, cp, R, n_total);
+    if (rc) return rc;
+    if (!sims_dev || n_sims < 1) return fail(PDS_ERR_INVALID_ARGUMENT, "null simulation table");
+    if (image_elems < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative image_elems");
+    return forward_impl(photons(E, X, M, cp, R, n_total), table_dev(sims_dev, n_sims), n_tiles,
+                        image_elems, mpr, out, cfg, ws, ws_bytes,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int pds_batch_backward_planned_f32(const float* G, const float* E, const float* X,
+                                   const float* M, const int64_t* cp, const float* R,
+                                   int64_t n_total, const pds_sim* sims_dev, int32_t n_sims,
+                                   int64_t n_tiles, int32_t mpr, float* gE, float* gX, float* gM,
+                                   void* ws, size_t ws_bytes, const pds_config* cfg,
+                                   void* stream) {
+    int rc = check_photons(E, X, M, cp, R, n_total);
+    if (rc) return rc;
+    if (!sims_dev || n_sims < 1) return fail(PDS_ERR_INVALID_ARGUMENT, "null simulation table");
+    return backward_impl(G, photons(E, X, M, cp, R, n_total), table_dev(sims_dev, n_sims),
+                         n_tiles, mpr, gE, gX, gM, cfg, ws, ws_bytes,
+                         static_cast<cudaStream_t>(stream));
+}
+
+size_t pds_sort_workspace_bytes(int64_t n) {
+    const size_t nn = size_t(n > 0 ? n : 1);
+    return 2 * pds::align_up(nn * 4, 256) + pds::sort_aux_bytes(n);
+}
+
+int pds_sort_u32(const uint32_t* keys, int64_t n, int32_t key_bits, uint32_t* keys_out,
+                 uint32_t* perm_out, void* ws, size_t ws_bytes, void* stream) {
+    if (n < 0 || n >= int64_t(0xFFFFFFFFll))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "sort size outside [0, 2^32 - 1)");
+    if (key_bits < 0 || key_bits > 32)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "key_bits outside [0, 32]");
+    if (n == 0) return PDS_OK;
+    if (!keys || !keys_out || !perm_out)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null sort array");
+    int rc = check_ws(ws, ws_bytes, pds_sort_workspace_bytes(n));
+    if (rc) return rc;
+    const size_t nn = size_t(n);
+    char* b = static_cast<char*>(ws);
+    uint32_t* kt = reinterpret_cast<uint32_t*>(b);
+    uint32_t* vt = reinterpret_cast<uint32_t*>(b + pds::align_up(nn * 4, 256));
+    void* aux = b + 2 * pds::align_up(nn * 4, 256);
+    const int passes = pds::sort_passes(key_bits);
+    // the last pass must land in the caller's buffers
+    const bool last_in0 = passes == 0 || ((passes - 1) & 1) == 0;
+    uint32_t* k0 = last_in0 ? keys_out : kt;
+    uint32_t* k1 = last_in0 ? kt : keys_out;
+    uint32_t* v0 = last_in0 ? perm_out : vt;
+    uint32_t* v1 = last_in0 ? vt : perm_out;
+    uint32_t *ko, *vo;
+    cudaError_t e = pds::radix_sort(keys, k0, k1, v0, v1, n, key_bits, aux,
+                                    static_cast<cudaStream_t>(stream), &ko, &vo);
+    if (e != cudaSuccess) return cuda_fail(e, "radix sort");
+    return PDS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+// Device-side definitions shared by the photon-differential splatting kernels.
+//
+// Semantics follow the reference kernel PyOptix/kernel/photon_differentials.cu:
+//   footprint set-up  :76-89   (radius cut in double through the 0.5 literal, :80-81;
+//                               coord_to_pixel in double, truncating, :46-51)
+//   ellipse test      :93      (against the image half-size, in double)
+//   kernel            :23-29   (K(s) = 3/pi (1 - s)^2 for s = |u|^2 < 1)
+//   derivative        :31-37   (dK/dr = -12/pi r (1 - r^2))
+//   pixel position    :39-44   (pixel corner: 2 px / w - 1)
+// The integer decisions (centre pixel, radii, ellipse) reproduce the reference bit for bit.
+// The real-valued per-pixel offset is evaluated as k * (2/w) + delta, where delta is the
+// offset of the centre pixel's corner from the photon, formed in double once per photon;
+// the reference forms (2 px / w - 1) - x in float per pixel, which cancels and carries
+// ~1e-5 relative error for sub-pixel offsets. Both approximate the same quantity; ours is
+// the closer one to the FP64 oracle.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pds_b200.h"
+
+namespace pds {
+
+constexpr float kThreeOverPi = 0.954929658551372f;     // 3 / pi
+constexpr float kTwelveOverPi = 3.819718634205488f;    // 12 / pi
+
+// Record flags (low 4 bits of Rec::packed).
+constexpr uint32_t kFlagEllipseAll = 1u;  // :93 test passes for the whole box
+constexpr uint32_t kFlagFwdSkip = 2u;     // E <= 0 or NaN: forward deposits nothing (:106)
+
+// One photon of the tile path, 32 bytes, written once in photon order by the plan kernel
+// and gathered by sorted index by the tile kernels.
+struct __align__(16) Rec {
+    float dx0, dy0;       // corner of the centre pixel minus the photon, normalised units
+    float m00, m01, m10, m11;
+    float e;              // energy Ep
+    uint32_t packed;      // lx:8 | ly:8 | rx:6 | ry:6 | flags:4 (lx, ly: centre pixel in
+                          // the tile's apron frame)
+};
+
+__host__ __device__ __forceinline__ uint32_t pack_rec(int lx, int ly, int rx, int ry,
+                                                      uint32_t flags) {
+    return (uint32_t(lx) << 24) | (uint32_t(ly) << 16) | (uint32_t(rx) << 10) |
+           (uint32_t(ry) << 4) | flags;
+}
+__device__ __forceinline__ int rec_lx(uint32_t p) { return int(p >> 24); }
+__device__ __forceinline__ int rec_ly(uint32_t p) { return int((p >> 16) & 0xFFu); }
+__device__ __forceinline__ int rec_rx(uint32_t p) { return int((p >> 10) & 0x3Fu); }
+__device__ __forceinline__ int rec_ry(uint32_t p) { return int((p >> 4) & 0x3Fu); }
+__device__ __forceinline__ uint32_t rec_flags(uint32_t p) { return p & 0xFu; }
+
+// Resolved launch configuration (host fills it from pds_config).
+struct Cfg {
+    int32_t tile;
+    int32_t chunk;
+    int32_t class_bits;
+    int32_t apron;       // min(max_pixel_radius, apron_max), >= 0
+    int32_t sw;          // tile + 2 * apron: edge of the shared accumulator
+};
+
+// Simulation table: either a device array or one inline descriptor.
+struct SimTable {
+    const pds_sim* dev;
+    int32_t n;
+    pds_sim one;
+};
+
+__device__ __forceinline__ pds_sim load_sim(const SimTable& t, int s) {
+    if (t.dev == nullptr) return t.one;
+    return t.dev[s];
+}
+
+// Simulation owning photon i (photons of a simulation are contiguous).
+__device__ __forceinline__ int find_sim_of_photon(const SimTable& t, int64_t i) {
+    if (t.dev == nullptr) return 0;
+    int lo = 0, hi = t.n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&t.dev[mid].photon_begin) <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Simulation owning global tile id g.
+__device__ __forceinline__ int find_sim_of_tile(const SimTable& t, int64_t g) {
+    if (t.dev == nullptr) return 0;
+    int lo = 0, hi = t.n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&t.dev[mid].tile_base) <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Footprint of one photon (photon_differentials.cu:76-87), integer part exact.
+struct Footprint {
+    int32_t px_c, py_c, rx, ry;
+    bool ellipse_all;
+};
+
+// The :93 test for one offset, evaluated exactly as the reference does (int32 square,
+// float conversion, double division and sum).
+__device__ __forceinline__ bool ellipse_ok(int32_t xo, int32_t yo, double w, double h) {
+    const float fx = float(int32_t(uint32_t(xo) * uint32_t(xo)));
+    const float fy = float(int32_t(uint32_t(yo) * uint32_t(yo)));
+    return double(fx) / (0.25 * w * w) + double(fy) / (0.25 * h * h) <= 1.0;
+}
+
+__device__ __forceinline__ Footprint make_footprint(float x, float y, float r, int32_t H,
+                                                    int32_t W, int32_t mpr) {
+    Footprint f;
+    const double w = double(float(W)), h = double(float(H));
+    // __double2int_rz: truncation with saturation, NaN -> 0 (the GPU semantics of the
+    // reference's int32_t(...) casts).
+    const int32_t rx = __double2int_rz(ceil(double(r) * 0.5 * w));
+    const int32_t ry = __double2int_rz(ceil(double(r) * 0.5 * h));
+    f.rx = min(rx, mpr);
+    f.ry = min(ry, mpr);
+    f.px_c = __double2int_rz((0.5 * double(x) + 0.5) * w);
+    f.py_c = __double2int_rz((0.5 * double(y) + 0.5) * h);
+    f.ellipse_all = (f.rx < 0 || f.ry < 0) ? true : ellipse_ok(f.rx, f.ry, w, h);
+    return f;
+}
+
+// Clipped box in 64-bit arithmetic; false when empty.
+__device__ __forceinline__ bool clip_box(const Footprint& f, int32_t H, int32_t W, int32_t& x0,
+                                         int32_t& x1, int32_t& y0, int32_t& y1) {
+    if (f.rx < 0 || f.ry < 0) return false;
+    const int64_t a = max(int64_t(f.px_c) - f.rx, int64_t(0));
+    const int64_t b = min(int64_t(f.px_c) + f.rx, int64_t(W) - 1);
+    const int64_t c = max(int64_t(f.py_c) - f.ry, int64_t(0));
+    const int64_t d = min(int64_t(f.py_c) + f.ry, int64_t(H) - 1);
+    if (a > b || c > d) return false;
+    x0 = int32_t(a); x1 = int32_t(b); y0 = int32_t(c); y1 = int32_t(d);
+    return true;
+}
+
+// delta = (2 p_c / w - 1) - x in double, rounded once to float.
+__device__ __forceinline__ float corner_offset(int32_t p_c, int32_t W, float x) {
+    return float(2.0 * double(p_c) / double(W) - 1.0 - double(x));
+}
+
+}  // namespace pds

@@ -1,0 +1,582 @@
+// Photon-differential splatting kernels for sm_100a.
+//
+// Reference: PyOptix/kernel/photon_differentials.cu. The reference runs one thread per
+// photon over its whole footprint box with one global atomicAdd per covered pixel (forward,
+// :60-113) and the same walk reading the upstream gradient (backward, :136-221). Here:
+//
+//   plan_kernel      one pass over the photons (coalesced SoA reads): exact integer
+//                    footprint, a sort key (simulation, channel, screen tile of the centre
+//                    pixel, footprint class) and a 32-byte record in photon order.
+//   radix sort       pds_sort.cu: stable, so the order equals a CPU stable sort.
+//   fwd_tiles_kernel persistent CTAs walk fixed-size chunks of the sorted photons; each
+//                    tile segment is rasterised into a shared-memory accumulator covering
+//                    the tile plus an apron of the largest footprint radius, then flushed
+//                    with one coalesced pass of global adds over the touched box.
+//   bwd_tiles_kernel same walk; the segment's tile+apron of the upstream gradient is staged
+//                    in shared memory once, each photon gathers over its box from there and
+//                    writes its gradients (no atomics). The per-pixel work is reduced to the
+//                    moments sum(t g), sum(t^2 g), sum(t g d), sum(t g d d^T) of the offset d,
+//                    from which dL/dE, dL/dx and dL/dM follow by 2x2 algebra per photon.
+//   tail kernels     footprints wider than the apron (direct global path, a warp per photon)
+//                    and zero gradients for photons that touch no pixel.
+#include <climits>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pds_device.cuh"
+#include "pds_internal.h"
+#include "pds_splat.h"
+
+namespace pds {
+
+namespace {
+
+// ------------------------------------------------------------------ plan ---------------
+
+__global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
+    const int64_t n = a.ph.n;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    uint32_t c_tile = 0, c_big = 0, c_inv = 0;
+    const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
+    const uint32_t cls_max = (1u << cb) - 1u;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int s = find_sim_of_photon(a.sims, i);
+        const pds_sim sim = load_sim(a.sims, s);
+        const int64_t ch = __ldg(a.ph.cp + i);
+        uint32_t key = a.key_invalid;
+        if (ch >= 0 && ch < sim.channels) {
+            const float x = __ldg(a.ph.X + i), y = __ldg(a.ph.X + n + i);
+            const Footprint f = make_footprint(x, y, __ldg(a.ph.R + i), sim.height, sim.width,
+                                               a.mpr);
+            int32_t x0, x1, y0, y1;
+            if (clip_box(f, sim.height, sim.width, x0, x1, y0, y1)) {
+                if (f.rx > A || f.ry > A) {
+                    key = a.key_big;
+                } else {
+                    const int pcx = min(max(f.px_c, 0), sim.width - 1);
+                    const int pcy = min(max(f.py_c, 0), sim.height - 1);
+                    const int tx = pcx / T, ty = pcy / T;
+                    const uint32_t tile = uint32_t(sim.tile_base) +
+                                          uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
+                    const uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
+                    key = (tile << cb) | cls;
+                    const float e = __ldg(a.ph.E + i);
+                    const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) |
+                                           (e > 0.f ? 0u : kFlagFwdSkip);
+                    Rec r;
+                    r.dx0 = corner_offset(f.px_c, sim.width, x);
+                    r.dy0 = corner_offset(f.py_c, sim.height, y);
+                    r.m00 = __ldg(a.ph.M + i);
+                    r.m01 = __ldg(a.ph.M + n + i);
+                    r.m10 = __ldg(a.ph.M + 3 * n + i);
+                    r.m11 = __ldg(a.ph.M + 4 * n + i);
+                    r.e = e;
+                    r.packed = pack_rec(f.px_c - (tx * T - A), f.py_c - (ty * T - A), f.rx, f.ry,
+                                        flags);
+                    a.recs[i] = r;
+                }
+            }
+        }
+        a.keys[i] = key;
+        c_tile += key < a.key_big;
+        c_big += key == a.key_big;
+        c_inv += key == a.key_invalid;
+    }
+    // block totals -> three global counters
+    __shared__ uint32_t red[3];
+    if (threadIdx.x < 3) red[threadIdx.x] = 0;
+    __syncthreads();
+    c_tile = __reduce_add_sync(0xFFFFFFFFu, c_tile);
+    c_big = __reduce_add_sync(0xFFFFFFFFu, c_big);
+    c_inv = __reduce_add_sync(0xFFFFFFFFu, c_inv);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&red[0], c_tile);
+        atomicAdd(&red[1], c_big);
+        atomicAdd(&red[2], c_inv);
+    }
+    __syncthreads();
+    if (threadIdx.x < 3 && red[threadIdx.x]) atomicAdd(a.counters + threadIdx.x, red[threadIdx.x]);
+}
+
+// ------------------------------------------------------------------ tiles --------------
+
+struct TileInfo {
+    int64_t img_off;  // element offset of the (simulation, channel) image plane
+    int32_t W, H;
+    int32_t ox, oy;   // pixel coordinates of the accumulator's (0, 0)
+    float sx, sy;     // 2 / W, 2 / H
+    double wd, hd;    // float(W), float(H) in double (the reference's w, h)
+};
+
+__device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t tile, const Cfg& cfg) {
+    const int s = find_sim_of_tile(st, tile);
+    const pds_sim sim = load_sim(st, s);
+    const int32_t local = int32_t(tile) - sim.tile_base;
+    const int32_t tx = local % sim.tiles_x;
+    const int32_t r = local / sim.tiles_x;
+    const int32_t ty = r % sim.tiles_y;
+    const int32_t ch = r / sim.tiles_y;
+    TileInfo t;
+    t.W = sim.width;
+    t.H = sim.height;
+    t.img_off = sim.image_offset + int64_t(ch) * sim.height * sim.width;
+    t.ox = tx * cfg.tile - cfg.apron;
+    t.oy = ty * cfg.tile - cfg.apron;
+    t.sx = float(2.0 / double(sim.width));
+    t.sy = float(2.0 / double(sim.height));
+    t.wd = double(float(sim.width));
+    t.hd = double(float(sim.height));
+    return t;
+}
+
+// Forward deposit of one photon into the shared accumulator (photon_differentials.cu:91-110).
+__device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, float* acc,
+                                        int& bx0, int& bx1, int& by0, int& by1) {
+    const uint32_t p = r.packed;
+    const uint32_t fl = rec_flags(p);
+    if (fl & kFlagFwdSkip) return;
+    const int pxc = ti.ox + rec_lx(p), pyc = ti.oy + rec_ly(p);
+    const int rx = rec_rx(p), ry = rec_ry(p);
+    const int x0 = max(pxc - rx, 0), x1 = min(pxc + rx, ti.W - 1);
+    const int y0 = max(pyc - ry, 0), y1 = min(pyc + ry, ti.H - 1);
+    bx0 = x0; bx1 = x1; by0 = y0; by1 = y1;
+    const float e3 = r.e * kThreeOverPi;
+    const bool all = fl & kFlagEllipseAll;
+    for (int py = y0; py <= y1; ++py) {
+        const int ky = py - pyc;
+        const float dy = fmaf(float(ky), ti.sy, r.dy0);
+        const float a0 = r.m01 * dy, a1 = r.m11 * dy;
+        float* row = acc + (py - ti.oy) * sw - ti.ox;
+        for (int px = x0; px <= x1; ++px) {
+            const int kx = px - pxc;
+            const float dx = fmaf(float(kx), ti.sx, r.dx0);
+            const float u0 = fmaf(r.m00, dx, a0), u1 = fmaf(r.m10, dx, a1);
+            const float s = fmaf(u0, u0, u1 * u1);
+            if (s < 1.f && (all || ellipse_ok(kx, ky, ti.wd, ti.hd))) {
+                const float t = 1.f - s;
+                atomicAdd(row + px, t * t * e3);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void bbox_publish(int* sb, int x0, int x1, int y0, int y1) {
+    x0 = __reduce_min_sync(0xFFFFFFFFu, x0);
+    x1 = __reduce_max_sync(0xFFFFFFFFu, x1);
+    y0 = __reduce_min_sync(0xFFFFFFFFu, y0);
+    y1 = __reduce_max_sync(0xFFFFFFFFu, y1);
+    if ((threadIdx.x & 31) == 0 && x0 <= x1) {
+        atomicMin(sb + 0, x0);
+        atomicMax(sb + 1, x1);
+        atomicMin(sb + 2, y0);
+        atomicMax(sb + 3, y1);
+    }
+}
+
+// Adds the touched box of the accumulator into the image and clears it.
+__device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& ti, float* out,
+                                           int* sb) {
+    __syncthreads();
+    const int x0 = sb[0], x1 = sb[1], y0 = sb[2], y1 = sb[3];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
+    }
+    if (x0 <= x1) {
+        const int bw = x1 - x0 + 1;
+        const int total = bw * (y1 - y0 + 1);
+        float* img = out + ti.img_off;
+        for (int k = threadIdx.x; k < total; k += blockDim.x) {
+            const int rr = k / bw;
+            const int cc = k - rr * bw;
+            const int gx = x0 + cc, gy = y0 + rr;
+            float* a = acc + (gy - ti.oy) * sw + (gx - ti.ox);
+            const float v = *a;
+            if (v != 0.f) {
+                atomicAdd(img + int64_t(gy) * ti.W + gx, v);
+                *a = 0.f;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__global__ __launch_bounds__(NT) void fwd_tiles_kernel(TileArgs a) {
+    extern __shared__ float acc[];
+    __shared__ int sb[4];
+    const Cfg cfg = a.cfg;
+    const int sw = cfg.sw, cb = cfg.class_bits;
+    for (int k = threadIdx.x; k < sw * sw; k += NT) acc[k] = 0.f;
+    if (threadIdx.x == 0) {
+        sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
+    }
+    __syncthreads();
+    const int64_t n_tile = a.counters[0];
+    const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
+    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
+        uint32_t cur = a.skeys[p0] >> cb;
+        TileInfo ti = decode_tile(a.sims, cur, cfg);
+        for (int64_t base = p0; base < p1; base += NT) {
+            const int64_t i = base + threadIdx.x;
+            const bool have = i < p1;
+            uint32_t key = 0xFFFFFFFFu;
+            Rec r;
+            if (have) {
+                key = a.skeys[i] >> cb;
+                r = a.recs[a.sidx[i]];
+            }
+            const int64_t bend = min(base + NT, p1);
+            while (true) {
+                const bool mine = have && key == cur;
+                int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
+                if (mine) deposit(r, ti, sw, acc, x0, x1, y0, y1);
+                bbox_publish(sb, x0, x1, y0, y1);
+                const int cnt = __syncthreads_count(mine);
+                const int64_t nxt = base + cnt;
+                if (nxt >= bend) break;
+                flush_tile(acc, sw, ti, a.out, sb);
+                cur = a.skeys[nxt] >> cb;
+                ti = decode_tile(a.sims, cur, cfg);
+            }
+        }
+        flush_tile(acc, sw, ti, a.out, sb);
+    }
+}
+
+// Stages the tile+apron of the upstream gradient (clipped to the image).
+__device__ __forceinline__ void load_region(float* tg, int sw, const TileInfo& ti,
+                                            const float* grad) {
+    const int gx0 = max(ti.ox, 0), gx1 = min(ti.ox + sw, ti.W);
+    const int gy0 = max(ti.oy, 0), gy1 = min(ti.oy + sw, ti.H);
+    const int bw = gx1 - gx0;
+    if (bw <= 0 || gy1 <= gy0) return;
+    const int total = bw * (gy1 - gy0);
+    const float* img = grad + ti.img_off;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+        const int rr = k / bw;
+        const int cc = k - rr * bw;
+        const int gy = gy0 + rr, gx = gx0 + cc;
+        tg[(gy - ti.oy) * sw + (gx - ti.ox)] = __ldg(img + int64_t(gy) * ti.W + gx);
+    }
+}
+
+// Backward gather of one photon (photon_differentials.cu:169-218) from the staged gradient.
+__device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
+                                       const float* tg, uint32_t rid, const TileArgs& a) {
+    const uint32_t p = r.packed;
+    const uint32_t fl = rec_flags(p);
+    const int pxc = ti.ox + rec_lx(p), pyc = ti.oy + rec_ly(p);
+    const int rx = rec_rx(p), ry = rec_ry(p);
+    const int x0 = max(pxc - rx, 0), x1 = min(pxc + rx, ti.W - 1);
+    const int y0 = max(pyc - ry, 0), y1 = min(pyc + ry, ti.H - 1);
+    const bool all = fl & kFlagEllipseAll;
+    float sE = 0.f, Sx = 0.f, Sy = 0.f, Sxx = 0.f, Sxy = 0.f, Syy = 0.f;
+    for (int py = y0; py <= y1; ++py) {
+        const int ky = py - pyc;
+        const float dy = fmaf(float(ky), ti.sy, r.dy0);
+        const float a0 = r.m01 * dy, a1 = r.m11 * dy;
+        const float* row = tg + (py - ti.oy) * sw - ti.ox;
+        float A0 = 0.f, A1 = 0.f, A2 = 0.f;
+        for (int px = x0; px <= x1; ++px) {
+            const int kx = px - pxc;
+            if (!all && !ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
+            const float dx = fmaf(float(kx), ti.sx, r.dx0);
+            const float u0 = fmaf(r.m00, dx, a0), u1 = fmaf(r.m10, dx, a1);
+            const float s = fmaf(u0, u0, u1 * u1);
+            const float t = s < 1.f ? 1.f - s : 0.f;
+            const float g = row[px];
+            const float tgv = t * g;
+            sE = fmaf(t, tgv, sE);
+            A0 += tgv;
+            const float adx = tgv * dx;
+            A1 += adx;
+            A2 = fmaf(adx, dx, A2);
+        }
+        Sx += A1;
+        Sy = fmaf(dy, A0, Sy);
+        Sxx += A2;
+        Sxy = fmaf(dy, A1, Sxy);
+        Syy = fmaf(dy * dy, A0, Syy);
+    }
+    const float c = -kTwelveOverPi * r.e;
+    const float v0 = c * fmaf(r.m00, Sx, r.m01 * Sy);
+    const float v1 = c * fmaf(r.m10, Sx, r.m11 * Sy);
+    const int64_t n = a.ph.n;
+    a.gE[rid] = kThreeOverPi * sE;
+    a.gX[rid] = -fmaf(r.m00, v0, r.m10 * v1);
+    a.gX[n + rid] = -fmaf(r.m01, v0, r.m11 * v1);
+    a.gM[rid] = c * fmaf(r.m00, Sxx, r.m01 * Sxy);
+    a.gM[n + rid] = c * fmaf(r.m00, Sxy, r.m01 * Syy);
+    a.gM[3 * n + rid] = c * fmaf(r.m10, Sxx, r.m11 * Sxy);
+    a.gM[4 * n + rid] = c * fmaf(r.m10, Sxy, r.m11 * Syy);
+}
+
+template <int NT>
+__global__ __launch_bounds__(NT) void bwd_tiles_kernel(TileArgs a) {
+    extern __shared__ float tg[];
+    const Cfg cfg = a.cfg;
+    const int sw = cfg.sw, cb = cfg.class_bits;
+    const int64_t n_tile = a.counters[0];
+    const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
+    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
+        uint32_t cur = a.skeys[p0] >> cb;
+        TileInfo ti = decode_tile(a.sims, cur, cfg);
+        uint32_t loaded = 0xFFFFFFFFu;
+        for (int64_t base = p0; base < p1; base += NT) {
+            const int64_t i = base + threadIdx.x;
+            const bool have = i < p1;
+            uint32_t key = 0xFFFFFFFFu, rid = 0;
+            Rec r;
+            if (have) {
+                key = a.skeys[i] >> cb;
+                rid = a.sidx[i];
+                r = a.recs[rid];
+            }
+            const int64_t bend = min(base + NT, p1);
+            while (true) {
+                if (cur != loaded) {
+                    __syncthreads();
+                    load_region(tg, sw, ti, a.grad);
+                    __syncthreads();
+                    loaded = cur;
+                }
+                const bool mine = have && key == cur;
+                if (mine) gather(r, ti, sw, tg, rid, a);
+                const int cnt = __syncthreads_count(mine);
+                const int64_t nxt = base + cnt;
+                if (nxt >= bend) break;
+                cur = a.skeys[nxt] >> cb;
+                ti = decode_tile(a.sims, cur, cfg);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ tail ---------------
+// Sorted positions [n_tile, n_tile + n_big) hold footprints wider than the apron; they are
+// splatted straight into global memory, one warp per photon. Positions after that hold
+// photons that touch no pixel.
+
+struct Direct {
+    int pxc, pyc, x0, x1, y0, y1;
+    bool all;
+    float dx0, dy0, m00, m01, m10, m11, e;
+    float sx, sy;
+    double wd, hd;
+    int64_t img_off;
+    int W;
+};
+
+__device__ __forceinline__ bool direct_setup(const TileArgs& a, uint32_t rid, Direct& d) {
+    const int64_t n = a.ph.n;
+    const int s = find_sim_of_photon(a.sims, rid);
+    const pds_sim sim = load_sim(a.sims, s);
+    const int64_t ch = a.ph.cp[rid];
+    const float x = a.ph.X[rid], y = a.ph.X[n + rid];
+    const Footprint f = make_footprint(x, y, a.ph.R[rid], sim.height, sim.width, a.mpr);
+    if (!clip_box(f, sim.height, sim.width, d.x0, d.x1, d.y0, d.y1)) return false;
+    d.pxc = f.px_c;
+    d.pyc = f.py_c;
+    d.all = f.ellipse_all;
+    d.dx0 = corner_offset(f.px_c, sim.width, x);
+    d.dy0 = corner_offset(f.py_c, sim.height, y);
+    d.m00 = a.ph.M[rid];
+    d.m01 = a.ph.M[n + rid];
+    d.m10 = a.ph.M[3 * n + rid];
+    d.m11 = a.ph.M[4 * n + rid];
+    d.e = a.ph.E[rid];
+    d.sx = float(2.0 / double(sim.width));
+    d.sy = float(2.0 / double(sim.height));
+    d.wd = double(float(sim.width));
+    d.hd = double(float(sim.height));
+    d.img_off = sim.image_offset + ch * sim.height * sim.width;
+    d.W = sim.width;
+    return true;
+}
+
+__global__ __launch_bounds__(256) void tail_fwd_kernel(TileArgs a) {
+    const int64_t n_tile = a.counters[0], n_big = a.counters[1];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_big;
+         w += warps) {
+        const uint32_t rid = a.sidx[n_tile + w];
+        Direct d;
+        if (!direct_setup(a, rid, d) || !(d.e > 0.f)) continue;
+        const float e3 = d.e * kThreeOverPi;
+        const int bw = d.x1 - d.x0 + 1;
+        const int64_t total = int64_t(bw) * (d.y1 - d.y0 + 1);
+        float* img = a.out + d.img_off;
+        for (int64_t k = lane; k < total; k += 32) {
+            const int py = d.y0 + int(k / bw), px = d.x0 + int(k % bw);
+            const int kx = px - d.pxc, ky = py - d.pyc;
+            if (!d.all && !ellipse_ok(kx, ky, d.wd, d.hd)) continue;
+            const float dx = fmaf(float(kx), d.sx, d.dx0), dy = fmaf(float(ky), d.sy, d.dy0);
+            const float u0 = fmaf(d.m00, dx, d.m01 * dy), u1 = fmaf(d.m10, dx, d.m11 * dy);
+            const float s = fmaf(u0, u0, u1 * u1);
+            if (s < 1.f) {
+                const float t = 1.f - s;
+                atomicAdd(img + int64_t(py) * d.W + px, t * t * e3);
+            }
+        }
+    }
+}
+
+__global__ __launch_bounds__(256) void tail_bwd_kernel(TileArgs a) {
+    const int64_t n = a.ph.n;
+    const int64_t n_tile = a.counters[0], n_big = a.counters[1];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_big;
+         w += warps) {
+        const uint32_t rid = a.sidx[n_tile + w];
+        Direct d;
+        float sE = 0.f, Sx = 0.f, Sy = 0.f, Sxx = 0.f, Sxy = 0.f, Syy = 0.f;
+        const bool any = direct_setup(a, rid, d);
+        if (any) {
+            const int bw = d.x1 - d.x0 + 1;
+            const int64_t total = int64_t(bw) * (d.y1 - d.y0 + 1);
+            const float* img = a.grad + d.img_off;
+            for (int64_t k = lane; k < total; k += 32) {
+                const int py = d.y0 + int(k / bw), px = d.x0 + int(k % bw);
+                const int kx = px - d.pxc, ky = py - d.pyc;
+                if (!d.all && !ellipse_ok(kx, ky, d.wd, d.hd)) continue;
+                const float dx = fmaf(float(kx), d.sx, d.dx0), dy = fmaf(float(ky), d.sy, d.dy0);
+                const float u0 = fmaf(d.m00, dx, d.m01 * dy), u1 = fmaf(d.m10, dx, d.m11 * dy);
+                const float s = fmaf(u0, u0, u1 * u1);
+                const float t = s < 1.f ? 1.f - s : 0.f;
+                const float tgv = t * __ldg(img + int64_t(py) * d.W + px);
+                sE = fmaf(t, tgv, sE);
+                Sx = fmaf(tgv, dx, Sx);
+                Sy = fmaf(tgv, dy, Sy);
+                Sxx = fmaf(tgv * dx, dx, Sxx);
+                Sxy = fmaf(tgv * dx, dy, Sxy);
+                Syy = fmaf(tgv * dy, dy, Syy);
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            sE += __shfl_xor_sync(0xFFFFFFFFu, sE, off);
+            Sx += __shfl_xor_sync(0xFFFFFFFFu, Sx, off);
+            Sy += __shfl_xor_sync(0xFFFFFFFFu, Sy, off);
+            Sxx += __shfl_xor_sync(0xFFFFFFFFu, Sxx, off);
+            Sxy += __shfl_xor_sync(0xFFFFFFFFu, Sxy, off);
+            Syy += __shfl_xor_sync(0xFFFFFFFFu, Syy, off);
+        }
+        if (lane == 0) {
+            if (!any) {
+                d.m00 = d.m01 = d.m10 = d.m11 = d.e = 0.f;
+            }
+            const float c = -kTwelveOverPi * d.e;
+            const float v0 = c * fmaf(d.m00, Sx, d.m01 * Sy);
+            const float v1 = c * fmaf(d.m10, Sx, d.m11 * Sy);
+            a.gE[rid] = kThreeOverPi * sE;
+            a.gX[rid] = -fmaf(d.m00, v0, d.m10 * v1);
+            a.gX[n + rid] = -fmaf(d.m01, v0, d.m11 * v1);
+            a.gM[rid] = c * fmaf(d.m00, Sxx, d.m01 * Sxy);
+            a.gM[n + rid] = c * fmaf(d.m00, Sxy, d.m01 * Syy);
+            a.gM[3 * n + rid] = c * fmaf(d.m10, Sxx, d.m11 * Sxy);
+            a.gM[4 * n + rid] = c * fmaf(d.m10, Sxy, d.m11 * Syy);
+        }
+    }
+    // photons that touch no pixel: zero gradients
+    const int64_t inv0 = n_tile + n_big;
+    const int64_t threads = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t p = inv0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += threads) {
+        const uint32_t rid = a.sidx[p];
+        a.gE[rid] = 0.f;
+        a.gX[rid] = 0.f;
+        a.gX[n + rid] = 0.f;
+        a.gM[rid] = 0.f;
+        a.gM[n + rid] = 0.f;
+        a.gM[3 * n + rid] = 0.f;
+        a.gM[4 * n + rid] = 0.f;
+    }
+}
+
+__global__ void iota_kernel(uint32_t* dst, int64_t n) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x)
+        dst[i] = uint32_t(i);
+}
+
+constexpr int kTileThreads = 256;
+
+int num_sms() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+// Grid of a persistent tile kernel: resident CTAs per SM x SMs, capped by the work.
+template <typename K>
+int persistent_grid(K kernel, size_t smem, int64_t n_units) {
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTileThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int64_t g = int64_t(per_sm) * num_sms();
+    const int64_t need = n_units > 0 ? n_units : 1;
+    return int(g < need ? g : need);
+}
+
+template <typename K>
+cudaError_t set_smem(K kernel, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+}
+
+}  // namespace
+
+void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st) {
+    if (n <= 0) return;
+    const int64_t blocks = (n + 255) / 256;
+    iota_kernel<<<unsigned(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(dst, n);
+}
+
+cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st) {
+    if (a.ph.n <= 0) return cudaSuccess;
+    const int64_t blocks = (a.ph.n + 255) / 256;
+    const int64_t cap = int64_t(num_sms()) * 8;
+    plan_kernel<<<unsigned(blocks < cap ? blocks : cap), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
+    const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
+    cudaError_t e = set_smem(fwd_tiles_kernel<kTileThreads>, smem);
+    if (e != cudaSuccess) return e;
+    const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
+    if (chunks > 0) {
+        const int grid = persistent_grid(fwd_tiles_kernel<kTileThreads>, smem, chunks);
+        fwd_tiles_kernel<kTileThreads><<<grid, kTileThreads, smem, st>>>(a);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const int tgrid = num_sms() * 2;
+        tail_fwd_kernel<<<tgrid, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t launch_backward(const TileArgs& a, cudaStream_t st) {
+    const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
+    cudaError_t e = set_smem(bwd_tiles_kernel<kTileThreads>, smem);
+    if (e != cudaSuccess) return e;
+    const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
+    if (chunks > 0) {
+        const int grid = persistent_grid(bwd_tiles_kernel<kTileThreads>, smem, chunks);
+        bwd_tiles_kernel<kTileThreads><<<grid, kTileThreads, smem, st>>>(a);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const int tgrid = num_sms() * 2;
+        tail_bwd_kernel<<<tgrid, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+}  // namespace pds

@@ -1,0 +1,80 @@
+"""The C ABI library loads without a GPU, exports every function include/pds_b200.h declares,
+and rejects bad arguments before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from shapefromcaustics_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))
+           if f.endswith(".h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(pds_\w+)\s*\(", src, re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_header_declares_the_entry_points():
+    names = declared_functions()
+    for n in ("pds_forward_f32", "pds_backward_f32", "pds_plan_f32", "pds_batch_layout",
+              "pds_sort_u32", "pds_last_error", "pds_workspace_bytes"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.lib()
+    for n in declared_functions():
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_version_and_workspace_query():
+    lib = _lib.lib()
+    assert b"sm_100a" in lib.pds_version()
+    a = lib.pds_workspace_bytes(1 << 20, 1, 512, 512, None)
+    b = lib.pds_workspace_bytes(1 << 21, 1, 512, 512, None)
+    assert 40 * (1 << 20) < a < b
+
+
+def test_argument_errors_without_a_device():
+    lib = _lib.lib()
+    rc = lib.pds_forward_f32(None, None, None, None, None, 5, 1, 8, 8, 20, None, None, 0, None, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT
+    assert b"null" in lib.pds_last_error()
+    p = ctypes.c_void_p(16)
+    cfg = _lib.config(tile=24)
+    rc = lib.pds_plan_f32(p, p, p, p, p, 5, 1, 8, 8, 20, p, 1 << 20, ctypes.byref(cfg), None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"tile" in lib.pds_last_error()
+    rc = lib.pds_plan_f32(p, p, p, p, p, 5, 0, 8, 8, 20, p, 1 << 20, None, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"positive" in lib.pds_last_error()
+    rc = lib.pds_plan_f32(p, p, p, p, p, 5, 1, 8, 8, 20, p, 10, None, None)
+    assert rc == _lib.PDS_ERR_WORKSPACE
+    rc = lib.pds_sort_u32(p, 10, 40, p, p, p, 1 << 20, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT
+
+
+def test_batch_layout_on_host():
+    lib = _lib.lib()
+    t = (_lib.PdsSim * 3)()
+    shapes = [(1, 512, 512), (2, 100, 70), (1, 16, 16)]
+    b = 0
+    for k, (c, h, w) in enumerate(shapes):
+        t[k].photon_begin, t[k].n_photons = b, 10 + k
+        t[k].channels, t[k].height, t[k].width = c, h, w
+        b += 10 + k
+    nt = ctypes.c_int64()
+    _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))
+    assert [t[k].tile_base for k in range(3)] == [0, 256, 256 + 2 * 4 * 3]
+    assert nt.value == 256 + 24 + 1
+    t[1].photon_begin = 3  # not contiguous
+    with pytest.raises(_lib.PdsError):
+        _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))

@@ -1,0 +1,276 @@
+"""Parity of the sm_100a splatting kernels (through the C ABI) with the FP64 oracle.
+
+Tolerances (stated by the target): forward images relative L2 <= 1e-5, gradients relative
+L2 <= 1e-4, both against the FP64 oracle on the same float32 inputs.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from shapefromcaustics_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+FWD_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def to_np(ts):
+    return [t.detach().cpu().numpy() for t in ts]
+
+
+def run_gpu(photons, shape, mpr, grad, cfg=None, dev="cuda:0"):
+    from shapefromcaustics_b200 import splatting as SP
+    E, X, M, C, R = (t.to(dev) for t in photons)
+    if cfg is not None:
+        SP.set_default_config(**cfg)
+    try:
+        img = SP.pds_forward(E, X, M, C, R, list(shape), mpr)[0]
+        g = SP.pds_backward(grad.to(dev).contiguous(), E, X, M, C, R, mpr)
+    finally:
+        SP.set_default_config()
+    torch.cuda.synchronize()
+    return img.cpu().numpy(), to_np(g)
+
+
+def run_oracle(photons, shape, mpr, grad):
+    E, X, M, C, R = to_np(photons)
+    img = O.forward(E, X, M, C, R, shape, mpr)
+    g = O.backward(grad.numpy().astype(np.float64), E, X, M, C, R, mpr)
+    return img, g
+
+
+def assert_parity(photons, shape, mpr, grad=None, cfg=None, fwd_tol=FWD_TOL, grad_tol=GRAD_TOL):
+    if grad is None:
+        grad = S.upstream_grad(shape, seed=7)
+    img, (gE, gX, gM) = run_gpu(photons, shape, mpr, grad, cfg)
+    rimg, (rE, rX, rM) = run_oracle(photons, shape, mpr, grad)
+    assert rel_l2(img, rimg) <= fwd_tol, rel_l2(img, rimg)
+    assert rel_l2(gE, rE) <= grad_tol, rel_l2(gE, rE)
+    assert rel_l2(gX, rX) <= grad_tol, rel_l2(gX, rX)
+    assert rel_l2(gM, rM) <= grad_tol, rel_l2(gM, rM)
+    assert np.all(gM[:, 2] == 0)
+    return img, rimg
+
+
+def test_uniform_cluster_512(cuda):
+    ph = S.uniform_cluster_photons(2 ** 17, 512, 512, seed=0)
+    assert_parity(ph, (1, 512, 512), 20)
+
+
+@pytest.mark.parametrize("cfg", [dict(tile=16), dict(tile=64), dict(chunk=256),
+                                 dict(class_bits=2), dict(class_bits=4, chunk=4096),
+                                 dict(tile=32, apron_max=3)])
+def test_tuning_variants(cuda, cfg):
+    ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
+    assert_parity(ph, (1, 256, 256), 20, cfg=cfg)
+
+
+def test_non_square_ragged_image_and_channels(cuda):
+    n = 20000
+    E, X, M, C, R = S.uniform_cluster_photons(n, 70, 100, seed=2, s_range=(0.5, 6.0))
+    g = torch.Generator().manual_seed(5)
+    C = torch.randint(-1, 4, (1, n), generator=g)  # channels -1..3 with C = 3: some skipped
+    assert_parity((E, X, M, C, R), (3, 70, 100), 20)
+
+
+def test_wide_footprints_take_the_direct_path(cuda):
+    # radii up to 40 px > apron_max (8): direct path; mpr 30 truncates some boxes
+    ph = S.uniform_cluster_photons(3000, 128, 128, seed=3, s_range=(0.5, 40.0))
+    assert_parity(ph, (1, 128, 128), 30, cfg=dict(apron_max=8))
+
+
+def test_photons_partly_and_fully_off_image(cuda):
+    n = 8000
+    g = torch.Generator().manual_seed(4)
+    pos = torch.rand((2, n), generator=g, dtype=torch.float64) * 80 - 8  # [-8, 72) on 64^2
+    th = torch.rand(n, generator=g, dtype=torch.float64) * np.pi
+    s1 = 0.5 + torch.rand(n, generator=g, dtype=torch.float64) * 5
+    s2 = 0.5 + torch.rand(n, generator=g, dtype=torch.float64) * 5
+    e = torch.rand(n, generator=g, dtype=torch.float64) - 0.2  # some E <= 0
+    ph = S.photons_from_pixels(pos, th, s1, s2, e, 64, 64)
+    assert_parity(ph, (1, 64, 64), 20)
+
+
+def test_tiny_image_ellipse_quirk(cuda):
+    ph = S.uniform_cluster_photons(500, 8, 8, seed=5, s_range=(2.0, 20.0), sigma=2.0)
+    assert_parity(ph, (1, 8, 8), 20)
+
+
+@pytest.mark.parametrize("mpr", [0, 1, -1])
+def test_small_and_negative_max_pixel_radius(cuda, mpr):
+    ph = S.uniform_cluster_photons(4000, 64, 64, seed=6)
+    assert_parity(ph, (1, 64, 64), mpr)
+
+
+@pytest.mark.parametrize("n", [0, 1, 255, 257])
+def test_tiny_photon_counts(cuda, n):
+    ph = S.uniform_cluster_photons(max(n, 1), 64, 64, seed=8)
+    ph = tuple(t[..., :n].contiguous() for t in ph)
+    img, rimg = assert_parity(ph, (1, 64, 64), 20)
+    if n == 0:
+        assert not img.any()
+
+
+def test_dense_contention_hot_tile(cuda):
+    # all photons in a 6x6 px spot: one tile segment spans many chunks
+    n = 200000
+    g = torch.Generator().manual_seed(9)
+    pos = 100.0 + torch.randn((2, n), generator=g, dtype=torch.float64) * 1.5
+    th = torch.rand(n, generator=g, dtype=torch.float64) * np.pi
+    s = torch.exp(torch.rand((2, n), generator=g, dtype=torch.float64) * np.log(64) + np.log(0.25))
+    e = 0.5 + torch.rand(n, generator=g, dtype=torch.float64) * 0.5
+    ph = S.photons_from_pixels(pos, th, s[0], s[1], e, 256, 256)
+    assert_parity(ph, (1, 256, 256), 20)
+
+
+def test_planned_and_unplanned_agree_bitwise_in_backward(cuda):
+    from shapefromcaustics_b200.splatting import SplatPlan, pds_backward
+    E, X, M, C, R = (t.cuda() for t in S.uniform_cluster_photons(50000, 256, 256, seed=10))
+    G = S.upstream_grad((1, 256, 256), seed=3).cuda()
+    plan = SplatPlan(E, X, M, C, R, (1, 256, 256), 20)
+    a = plan.backward(G)
+    b = pds_backward(G, E, X, M, C, R, 20)
+    for u, v in zip(a, b):
+        assert torch.equal(u, v)
+
+
+def test_autograd_function_and_shim(cuda):
+    import shapefromcaustics_b200 as P
+    mod = P.shim.install()
+    import PhotonDifferentialSplatting as PDSmod
+    assert PDSmod.pds_forward is P.pds_forward
+    E, X, M, C, R = (t.cuda() for t in S.uniform_cluster_photons(30000, 128, 128, seed=11))
+    E.requires_grad_(True); X.requires_grad_(True); M.requires_grad_(True)
+    G = S.upstream_grad((1, 128, 128), seed=4).cuda()
+    img = P.PDS.apply(E, X, M, C, R, (1, 128, 128), 20)
+    (img * G).sum().backward()
+    rimg, (rE, rX, rM) = run_oracle((E.detach().cpu(), X.detach().cpu(), M.detach().cpu(),
+                                     C.cpu(), R.cpu()), (1, 128, 128), 20, G.cpu())
+    assert rel_l2(img.detach().cpu().numpy(), rimg) <= FWD_TOL
+    assert rel_l2(E.grad.cpu().numpy(), rE) <= GRAD_TOL
+    assert rel_l2(X.grad.cpu().numpy(), rX) <= GRAD_TOL
+    assert rel_l2(M.grad.cpu().numpy(), rM) <= GRAD_TOL
+    # the same with the plan rebuilt in backward
+    P.set_keep_plan(False)
+    try:
+        E.grad = None
+        img2 = P.PDS.apply(E, X, M, C, R, (1, 128, 128), 20)
+        (img2 * G).sum().backward()
+        assert rel_l2(E.grad.cpu().numpy(), rE) <= GRAD_TOL
+    finally:
+        P.set_keep_plan(True)
+
+
+def test_input_validation_messages(cuda):
+    from shapefromcaustics_b200 import pds_forward
+    E, X, M, C, R = (t.cuda() for t in S.uniform_cluster_photons(100, 32, 32, seed=12))
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        pds_forward(E.cpu(), X, M, C, R, [1, 32, 32], 20)
+    with pytest.raises(RuntimeError, match="must be contiguous"):
+        pds_forward(E, X.t().contiguous().t(), M, C, R, [1, 32, 32], 20)
+    with pytest.raises(RuntimeError, match="don't match"):
+        pds_forward(E[:50].contiguous(), X, M, C, R, [1, 32, 32], 20)
+    with pytest.raises(RuntimeError, match="2x3"):
+        pds_forward(E, X, M[:, :2].contiguous(), C, R, [1, 32, 32], 20)
+    with pytest.raises(RuntimeError, match="Long"):
+        pds_forward(E, X, M, C.int(), R, [1, 32, 32], 20)
+    with pytest.raises(RuntimeError, match="float32"):
+        pds_forward(E.double(), X, M, C, R, [1, 32, 32], 20)
+
+
+def test_batched_uneven_simulations_match_per_simulation_oracle(cuda):
+    from shapefromcaustics_b200.splatting import BatchedSplat
+    specs = [(3000, (1, 64, 64)), (0, (1, 32, 32)), (12000, (2, 96, 80)), (700, (1, 16, 16)),
+             (40000, (1, 256, 256))]
+    parts = []
+    for s, (n, (C, H, W)) in enumerate(specs):
+        ph = S.uniform_cluster_photons(max(n, 1), H, W, seed=100 + s, sigma=H / 8)
+        ph = tuple(t[..., :n] for t in ph)
+        if C > 1:
+            ph = (ph[0], ph[1], ph[2], torch.randint(0, C, (1, n), generator=torch.Generator().manual_seed(s)), ph[4])
+        parts.append(ph)
+    cat = [torch.cat([p[k] for p in parts], dim=-1).contiguous().cuda() for k in range(5)]
+    b = BatchedSplat(specs, 20, "cuda:0")
+    b.plan(*cat)
+    flat = b.forward()
+    grads = [S.upstream_grad(shape, seed=50 + s) for s, (_, shape) in enumerate(specs)]
+    gflat = torch.cat([g.reshape(-1) for g in grads]).cuda()
+    gE, gX, gM = b.backward(gflat)
+    torch.cuda.synchronize()
+    imgs = b.images(flat)
+    off = 0
+    for s, ((n, shape), ph) in enumerate(zip(specs, parts)):
+        rimg, (rE, rX, rM) = run_oracle(ph, shape, 20, grads[s])
+        assert rel_l2(imgs[s].cpu().numpy(), rimg) <= FWD_TOL
+        sl = slice(off, off + n)
+        if n:
+            assert rel_l2(gE[sl].cpu().numpy(), rE) <= GRAD_TOL
+            assert rel_l2(gX[:, sl].cpu().numpy(), rX) <= GRAD_TOL
+            assert rel_l2(gM[:, :, sl].cpu().numpy(), rM) <= GRAD_TOL
+        off += n
+
+
+def test_batched_graph_replay_equals_eager(cuda):
+    from shapefromcaustics_b200.splatting import BatchedSplat
+    specs = S.batch_specs(6, seed=3, n_range=(2 ** 10, 2 ** 14), sizes=(64, 128))
+    photons = [t.cuda() for t in S.batch_photons(specs, seed=3)]
+    b = BatchedSplat(specs, 20, "cuda:0")
+    gflat = torch.randn(b.image_elems, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    b.plan(*photons)
+    ref_img = b.forward().clone()
+    ref_g = [t.clone() for t in b.backward(gflat)]
+    out = torch.empty(b.image_elems, device="cuda")
+    grads = tuple(torch.empty_like(t) for t in photons[:3])
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        b.plan(*photons); b.forward(out); b.backward(gflat, grads)
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        b.plan(*photons)
+        b.forward(out)
+        b.backward(gflat, grads)
+    out.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), ref_img.cpu().numpy()) <= 1e-6
+    for u, v in zip(grads, ref_g):
+        assert torch.equal(u, v)
+
+
+@pytest.mark.parametrize("n,bits", [(1, 3), (4097, 0), (4097, 5), (100000, 9), (300000, 16),
+                                    (300000, 17), (70000, 32)])
+def test_radix_sort_is_bit_exact_stable(cuda, n, bits):
+    from shapefromcaustics_b200 import _lib
+    g = torch.Generator().manual_seed(n + bits)
+    hi = 1 << bits if bits < 32 else 1 << 32
+    keys = torch.randint(0, max(hi, 1), (n,), generator=g, dtype=torch.int64)
+    if bits >= 8:  # heavy duplicates in part of the range
+        keys[: n // 3] = keys[: n // 3] % 7
+    keys_u = keys.to(torch.int64).numpy().astype(np.uint32)
+    kd = torch.from_numpy(keys_u.view(np.int32)).cuda()
+    ko = torch.empty_like(kd)
+    po = torch.empty_like(kd)
+    lib = _lib.lib()
+    ws = torch.empty(int(lib.pds_sort_workspace_bytes(n)), dtype=torch.uint8, device="cuda")
+    _lib.check(lib.pds_sort_u32(ctypes.c_void_p(kd.data_ptr()), n, bits,
+                                ctypes.c_void_p(ko.data_ptr()), ctypes.c_void_p(po.data_ptr()),
+                                ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    perm = po.cpu().numpy().view(np.uint32).astype(np.int64)
+    expect = np.argsort(keys_u, kind="stable")
+    assert np.array_equal(perm, expect)
+    assert np.array_equal(ko.cpu().numpy().view(np.uint32), keys_u[expect])
