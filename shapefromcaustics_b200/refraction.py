@@ -1,0 +1,236 @@
+"""Refraction-to-receiver for a glass plate with a height-field top surface, in PyTorch ops.
+
+The differentiable step between a height field and the splat inputs, for collimated light
+falling on the plate (the analytic height-field case the reference's OptiX tracer handles for
+this scene). Per photon:
+
+  1. surface sample: bilinear height and bilinear (unnormalised) Sobel normal at a jittered
+     position; the Sobel normal field follows ``get_normal_from_height_field``
+     (``model/caustics.py:215-221``: replicate padding, kernel scaled by -1/(8 texel)).
+  2. positional-differential transfer onto the surface (Frisvad 2014,
+     ``model/photon_differential.py:69-78``): ``D' = D - (n.D)/(n.d) d + t (Dd - (n.Dd)/(n.d) d)``.
+  3. Snell refraction of the direction and of its differentials (Igehy 1999,
+     ``model/caustics.py:152-212``, refraction branch): with ``cosi = d.N``, ``eta``,
+     ``k = 1 - eta^2 (1 - cosi^2)``, ``coso = eta cosi + sqrt(k)``,
+     ``d' = eta d - coso N`` and
+     ``Dd' = eta Dd - (coso dN + (eta - eta^2 cosi / -sqrt(k)) (Dd.N + d.dN) N)``;
+     the normal derivative ``dN`` along the positional differential uses
+     ``(|N|^2 dN~ - (N.dN~) N) / |N|^3`` of the un-normalised normal ``N~``
+     (``model/renderable_object.py:391-401``).
+  4. propagation inside the glass to the flat bottom face (z = 0), refraction out
+     (flat face: ``dN = 0``), propagation to the receiver plane ``z = -receiver_distance``.
+  5. receiver coordinates normalised by the receiver half-extent, and the splat inputs of
+     ``model/caustics.py:224-239`` (``caustics.splat_inputs``).
+
+The normal derivative is taken along the photon's whole positional differential at the hit
+(position and direction parts). The reference passes only the direction-induced part
+(``model/caustics.py:271`` uses ``Dtheta_hit``), which is the whole differential for its
+point light (Du = Dv = 0 at the first hit) but is zero for collimated light.
+
+Units: millimetres. Everything is written over tensors of any float dtype, so the same code
+runs in float64 on the CPU (the finite-difference reference) and float32 on the GPU.
+"""
+import math
+
+import torch
+import torch.nn.functional as F
+
+from .caustics import splat_inputs
+
+__all__ = ["PlateScene", "sobel_normals", "sample_surface", "trace_to_receiver",
+           "height_field_bumps", "jittered_photons"]
+
+
+class PlateScene:
+    """Glass plate over a receiver.
+
+    ``texel``: height-field texel size (mm), the field spans ``[-W texel/2, W texel/2]`` in x
+    (columns) and the same in y (rows); ``ior``: refractive index; ``receiver_distance``:
+    from the flat bottom face (z = 0) to the receiver (mm); ``receiver_half``: half-extent of
+    the square receiver (mm); ``light_dir``: unit propagation direction (default straight
+    down).
+    """
+
+    def __init__(self, texel=0.1, ior=1.5, receiver_distance=50.0, receiver_half=14.08,
+                 light_dir=(0.0, 0.0, -1.0)):
+        self.texel = float(texel)
+        self.ior = float(ior)
+        self.receiver_distance = float(receiver_distance)
+        self.receiver_half = float(receiver_half)
+        d = torch.tensor(light_dir, dtype=torch.float64)
+        self.light_dir = tuple((d / d.norm()).tolist())
+
+
+def sobel_normals(h, texel):
+    """Un-normalised normal field ``[3, H, W]`` = (-dh/dx, -dh/dy, 1) by the Sobel operator."""
+    k = torch.tensor([[[[-1, 0, 1], [-2, 0, 2], [-1, 0, 1]]],
+                      [[[-1, -2, -1], [0, 0, 0], [1, 2, 1]]]], dtype=h.dtype, device=h.device)
+    k = k * (-1.0 / (8.0 * texel))
+    g = F.conv2d(F.pad(h[None, None], (1, 1, 1, 1), mode="replicate"), k)[0]
+    return torch.cat((g, torch.ones_like(h)[None]), dim=0)
+
+
+def _bilinear(field, fx, fy):
+    """Bilinear sample of ``field [C, H, W]`` at continuous texel coordinates (texel centres
+    at integers, clamped to the border) -> values ``[C, N]`` and d/dfx, d/dfy ``[C, N]``."""
+    C, H, W = field.shape
+    fx = fx.clamp(0, W - 1)
+    fy = fy.clamp(0, H - 1)
+    x0 = fx.detach().floor().clamp(max=W - 2).long() if W > 1 else torch.zeros_like(fx, dtype=torch.long)
+    y0 = fy.detach().floor().clamp(max=H - 2).long() if H > 1 else torch.zeros_like(fy, dtype=torch.long)
+    x1 = (x0 + 1).clamp(max=W - 1)
+    y1 = (y0 + 1).clamp(max=H - 1)
+    ax = fx - x0
+    ay = fy - y0
+    flat = field.reshape(C, -1)
+    v00 = flat[:, y0 * W + x0]
+    v01 = flat[:, y0 * W + x1]
+    v10 = flat[:, y1 * W + x0]
+    v11 = flat[:, y1 * W + x1]
+    top = v00 + (v01 - v00) * ax
+    bot = v10 + (v11 - v10) * ax
+    val = top + (bot - top) * ay
+    ddx = (v01 - v00) * (1 - ay) + (v11 - v10) * ay
+    ddy = bot - top
+    return val, ddx, ddy
+
+
+def sample_surface(h, scene, px, py):
+    """Surface point, un-normalised normal and its spatial derivatives at world (px, py)."""
+    H, W = h.shape
+    fx = px / scene.texel + (W - 1) / 2.0
+    fy = py / scene.texel + (H - 1) / 2.0
+    N = sobel_normals(h, scene.texel)
+    hv, hdx, hdy = _bilinear(h[None], fx, fy)
+    nv, ndx, ndy = _bilinear(N, fx, fy)
+    return hv[0], nv, ndx / scene.texel, ndy / scene.texel
+
+
+def _dot(a, b):
+    return (a * b).sum(0)
+
+
+def _transfer(D, Dd, t, n, d):
+    """Positional differential carried along direction d for length t onto a plane of normal n
+    (``model/photon_differential.py:69-78``)."""
+    nd = _dot(n, d)
+    return D - _dot(n, D) / nd * d + t * (Dd - _dot(n, Dd) / nd * d)
+
+
+def _refract(d, N, Dd, dN, eta):
+    """Refraction of direction d and its differential Dd at unit normal N (facing the incident
+    side, d.N < 0), ``model/caustics.py:176-189``. Total internal reflection is not handled
+    (it does not occur for the plate geometries here)."""
+    cosi = _dot(d, N).clamp(-1, 1)
+    k = 1 - eta * eta * (1 - cosi * cosi)
+    neg_sq = -torch.sqrt(k.clamp(min=0))
+    coso = eta * cosi - neg_sq
+    out = eta * d - coso * N
+    Dout = eta * Dd - (coso * dN + ((eta - eta * eta * cosi / neg_sq) * (_dot(Dd, N) + _dot(d, dN))) * N)
+    return out, Dout
+
+
+def _unit_normal_and_derivative(Nt, dNt):
+    """n = N~/|N~| and its derivative along a differential (``renderable_object.py:391-401``)."""
+    ndn = _dot(Nt, Nt)
+    n = Nt / torch.sqrt(ndn)
+    dn = (ndn * dNt - _dot(Nt, dNt) * Nt) / ndn ** 1.5
+    return n, dn
+
+
+def trace_to_receiver(h, scene, px, py, Du0, Dv0):
+    """Per-photon receiver position (normalised, ``[2, N]``) and receiver-plane positional
+    differentials ``Du, Dv [3, N]`` (normalised units) for collimated photons entering the
+    plate's top surface at world (px, py) with initial positional differentials Du0, Dv0
+    ``[3, N]`` (in the plane perpendicular to the light)."""
+    dt = h.dtype
+    dev = h.device
+    n_ph = px.shape[0]
+    d = torch.tensor(scene.light_dir, dtype=dt, device=dev)[:, None].expand(3, n_ph)
+    zero = torch.zeros((3, n_ph), dtype=dt, device=dev)
+    hz, Nt, Ntx, Nty = sample_surface(h, scene, px, py)
+    # 1. onto the top surface: the photon crosses the surface at its sample point; carry the
+    #    source plane differentials onto the local tangent plane
+    Ntn = Nt / torch.sqrt(_dot(Nt, Nt))
+    Du1 = _transfer(Du0, zero, 0.0, Ntn, d)
+    Dv1 = _transfer(Dv0, zero, 0.0, Ntn, d)
+    dNu = Ntx * Du1[0] + Nty * Du1[1]
+    dNv = Ntx * Dv1[0] + Nty * Dv1[1]
+    n, dnu = _unit_normal_and_derivative(Nt, dNu)
+    _, dnv = _unit_normal_and_derivative(Nt, dNv)
+    # 2. refraction air -> glass at the top face (normal points up, against the light)
+    eta = 1.0 / scene.ior
+    t1, Ddu = _refract(d, n, zero, dnu, eta)
+    _, Ddv = _refract(d, n, zero, dnv, eta)
+    p1 = torch.stack((px, py, hz))
+    # 3. to the bottom face z = 0
+    s1 = -p1[2] / t1[2]
+    p2 = p1 + s1 * t1
+    nz = torch.zeros_like(zero)
+    nz[2] = 1.0
+    Du2 = _transfer(Du1, Ddu, s1, nz, t1)
+    Dv2 = _transfer(Dv1, Ddv, s1, nz, t1)
+    # 4. refraction glass -> air at the flat bottom face (normal facing the glass side: +z)
+    t2, Ddu2 = _refract(t1, nz, Ddu, zero, scene.ior)
+    _, Ddv2 = _refract(t1, nz, Ddv, zero, scene.ior)
+    # 5. to the receiver plane z = -receiver_distance
+    s2 = (-scene.receiver_distance - p2[2]) / t2[2]
+    p3 = p2 + s2 * t2
+    Du3 = _transfer(Du2, Ddu2, s2, nz, t2)
+    Dv3 = _transfer(Dv2, Ddv2, s2, nz, t2)
+    inv = 1.0 / scene.receiver_half
+    return p3[:2] * inv, Du3 * inv, Dv3 * inv
+
+
+def height_field_bumps(H, W, seed=0, bumps=32, base=1.0, amp=(0.0, 0.05), width=(4.0, 24.0),
+                       dtype=torch.float64, device="cpu"):
+    """Base thickness plus Gaussian bumps (amplitude and width uniform in the given ranges,
+    width in texels, centres uniform); millimetres."""
+    g = torch.Generator(device="cpu").manual_seed(int(seed))
+    cy = torch.rand(bumps, generator=g, dtype=torch.float64) * H
+    cx = torch.rand(bumps, generator=g, dtype=torch.float64) * W
+    a = amp[0] + torch.rand(bumps, generator=g, dtype=torch.float64) * (amp[1] - amp[0])
+    w = width[0] + torch.rand(bumps, generator=g, dtype=torch.float64) * (width[1] - width[0])
+    yy, xx = torch.meshgrid(torch.arange(H, dtype=torch.float64), torch.arange(W, dtype=torch.float64),
+                            indexing="ij")
+    h = torch.full((H, W), base, dtype=torch.float64)
+    for k in range(bumps):
+        h += a[k] * torch.exp(-((yy - cy[k]) ** 2 + (xx - cx[k]) ** 2) / (2 * w[k] ** 2))
+    return h.to(dtype=dtype, device=device)
+
+
+def jittered_photons(H, W, scene, per_texel=4, seed=0, smoothing=4.0, dtype=torch.float64,
+                     device="cpu"):
+    """Collimated photons: ``per_texel`` uniformly jittered entry points per texel, with
+    initial positional differentials ``2 smoothing sqrt(A / (pi N))`` along x and y (the
+    reference scales its light's differentials the same way, ``model/caustics.py:60-61``)
+    and flux 1/N. Returns ``(px, py, Du0, Dv0, flux)``."""
+    g = torch.Generator(device="cpu").manual_seed(int(seed))
+    n = H * W * per_texel
+    iy = torch.arange(H, dtype=torch.float64).repeat_interleave(W * per_texel)
+    ix = torch.arange(W, dtype=torch.float64).repeat_interleave(per_texel).repeat(H)
+    jx = torch.rand(n, generator=g, dtype=torch.float64) - 0.5
+    jy = torch.rand(n, generator=g, dtype=torch.float64) - 0.5
+    px = (ix + jx - (W - 1) / 2.0) * scene.texel
+    py = (iy + jy - (H - 1) / 2.0) * scene.texel
+    area = H * W * scene.texel ** 2
+    scale = 2.0 * smoothing * math.sqrt(area / (math.pi * n))
+    Du0 = torch.zeros((3, n), dtype=torch.float64)
+    Dv0 = torch.zeros((3, n), dtype=torch.float64)
+    Du0[0] = scale
+    Dv0[1] = scale
+    flux = torch.full((n,), 1.0 / n, dtype=torch.float64)
+    cast = dict(dtype=dtype, device=device)
+    return px.to(**cast), py.to(**cast), Du0.to(**cast), Dv0.to(**cast), flux.to(**cast)
+
+
+def receiver_splat_inputs(h, scene, photons, channel=None):
+    """Splat inputs ``(Ep, xp, Mp, cp, radius)`` of the plate for the given photons."""
+    px, py, Du0, Dv0, flux = photons
+    xy, Du, Dv = trace_to_receiver(h, scene, px, py, Du0, Dv0)
+    nrm = torch.zeros_like(Du)
+    nrm[2] = 1.0
+    if channel is None:
+        channel = torch.zeros(px.shape[0], dtype=torch.int64, device=px.device)
+    Ep, Mp, cp, radius = splat_inputs(Du, Dv, nrm, flux, channel)
+    return Ep, xy.contiguous(), Mp, cp, radius

@@ -1,0 +1,86 @@
+"""Refraction-to-receiver step in float64 on the CPU: its height-field gradient (autograd
+through the refraction chain, the FP64 oracle's splat backward at the end) against central
+finite differences of the FP64 forward."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from shapefromcaustics_b200 import refraction as RF
+
+
+class OraclePDS(torch.autograd.Function):
+    """The splat with the FP64 oracle in both directions (test-only)."""
+
+    @staticmethod
+    def forward(ctx, Ep, xp, Mp, cp, radius, shape, mpr):
+        ctx.save_for_backward(Ep, xp, Mp, cp, radius)
+        ctx.mpr = mpr
+        a = [t.detach().numpy() for t in (Ep, xp, Mp, cp, radius)]
+        return torch.from_numpy(O.forward(*a, shape, mpr))
+
+    @staticmethod
+    def backward(ctx, g):
+        a = [t.detach().numpy() for t in ctx.saved_tensors]
+        gE, gX, gM = O.backward(g.detach().numpy(), *a, ctx.mpr)
+        return torch.from_numpy(gE), torch.from_numpy(gX), torch.from_numpy(gM), None, None, None, None
+
+
+def render(h, scene, photons, shape, mpr=20):
+    Ep, xp, Mp, cp, radius = RF.receiver_splat_inputs(h, scene, photons)
+    return OraclePDS.apply(Ep, xp, Mp, cp, radius, shape, mpr)
+
+
+def setup(n=24, img=48):
+    scene = RF.PlateScene(texel=0.4, receiver_distance=30.0, receiver_half=6.0)
+    h = RF.height_field_bumps(n, n, seed=1, bumps=6, amp=(0.0, 0.05), width=(2.0, 5.0))
+    t = RF.height_field_bumps(n, n, seed=2, bumps=6, amp=(0.0, 0.05), width=(2.0, 5.0))
+    photons = RF.jittered_photons(n, n, scene, per_texel=4, seed=3, smoothing=2.0)
+    shape = (1, img, img)
+    target = render(t, scene, photons, shape).detach()
+    return scene, h, photons, shape, target
+
+
+def test_photons_land_on_the_receiver_and_energy_is_kept():
+    scene, h, photons, shape, target = setup()
+    Ep, xp, Mp, cp, radius = RF.receiver_splat_inputs(h, scene, photons)
+    assert (xp.abs() < 1).float().mean() > 0.95
+    img = render(h, scene, photons, shape)
+    # each photon deposits ~ flux * (W/2)(H/2) pixel units when untruncated
+    total = float(photons[4].sum()) * shape[1] * shape[2] / 4
+    assert 0.5 * total < float(img.sum()) < 1.5 * total
+
+
+def test_flat_plate_is_a_uniform_splat():
+    scene = RF.PlateScene(texel=0.4, receiver_distance=30.0, receiver_half=6.0)
+    h = torch.full((24, 24), 1.0, dtype=torch.float64)
+    photons = RF.jittered_photons(24, 24, scene, seed=0, smoothing=2.0)
+    xy, Du, Dv = RF.trace_to_receiver(h, scene, *photons[:4])
+    # normal incidence through parallel faces: straight through, differentials unchanged
+    assert torch.allclose(xy[0] * scene.receiver_half, photons[0], atol=1e-12)
+    assert torch.allclose(Du[:2] * scene.receiver_half, photons[2][:2], atol=1e-12)
+
+
+def test_height_gradient_matches_central_differences():
+    scene, h, photons, shape, target = setup()
+    hv = h.clone().requires_grad_(True)
+    img = render(hv, scene, photons, shape)
+    loss = 0.5 * ((img - target) ** 2).sum()
+    loss.backward()
+    grad = hv.grad.detach()
+    rng = np.random.default_rng(0)
+    idx = [tuple(rng.integers(2, 22, 2)) for _ in range(12)]
+    eps = 1e-6
+
+    def L(hh):
+        with torch.no_grad():
+            return float(0.5 * ((render(hh, scene, photons, shape) - target) ** 2).sum())
+
+    fd, an = [], []
+    for (i, j) in idx:
+        hp = h.clone(); hp[i, j] += eps
+        hm = h.clone(); hm[i, j] -= eps
+        fd.append((L(hp) - L(hm)) / (2 * eps))
+        an.append(float(grad[i, j]))
+    fd, an = np.array(fd), np.array(an)
+    assert np.linalg.norm(fd - an) / np.linalg.norm(an) < 1e-4, (fd, an)
