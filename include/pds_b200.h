@@ -49,6 +49,10 @@ typedef struct pds_config {
     int32_t class_bits; /* footprint-size bits appended to the sort key, 0..4 (default 0) */
     int32_t apron_max;  /* largest footprint radius (px) the tile path holds (default 32);
                            larger footprints take the direct path */
+    int32_t walk;       /* pixels visited per photon: 1 = the reference's whole box,
+                           2 = only the rows / row spans that can hold the kernel's support
+                           (same result: pixels outside the support add exactly zero);
+                           default 2 */
 } pds_config;
 
 /* One simulation of a batch. The caller fills photon_begin, n_photons, image_offset,
@@ -146,6 +150,61 @@ int pds_batch_backward_planned_f32(const float* grad, const float* Ep, const flo
                                    float* grad_Ep, float* grad_xp, float* grad_Mp,
                                    void* workspace, size_t workspace_bytes,
                                    const pds_config* cfg, void* stream);
+
+/* ---- refraction to the receiver for a height-field glass plate --------------------- */
+/* Replaces, for a plate whose top face is a height field lit by collimated light, the
+ * reference's refraction chain from the traced hit to the splat inputs:
+ * Sobel normals (model/caustics.py:215-221), differential transfer
+ * (model/photon_differential.py:69-78), Snell + Igehy differentials (model/caustics.py:152-212),
+ * normal derivatives (model/renderable_object.py:391-401) and the splat inputs
+ * (model/caustics.py:224-239). The OptiX trace that finds the hits (PyOptix/RayTrace.cpp:233-291)
+ * is replaced by the analytic plate: entry at (px, py, h(px, py)), exit through the flat face
+ * z = 0, receiver plane z = -receiver_distance. */
+typedef struct pds_plate {
+    float texel;             /* height-field texel edge (world units); the field is centred */
+    float ior;               /* refractive index of the plate */
+    float receiver_distance; /* from the flat bottom face (z = 0) down to the receiver */
+    float receiver_half;     /* receiver half-extent; receiver coordinates are divided by it */
+    float light_dir[3];      /* unit propagation direction of the collimated light */
+    float du0;               /* length of each photon's initial positional differentials (x, y) */
+} pds_plate;
+
+/* Splat inputs of n photons entering at (px[i], py[i]) with flux[i] (channel[i], or 0 when
+ * channel is NULL): Ep[N], xp[2][N], Mp[2][3][N], cp[1][N] (-1 for degenerate photons),
+ * radius[N]. height: [rows][cols] row-major. */
+int pds_refract_forward_f32(const float* height, int32_t rows, int32_t cols, const pds_plate* plate,
+                            const float* px, const float* py, const float* flux,
+                            const int64_t* channel, int64_t n_photons, float* Ep, float* xp,
+                            float* Mp, int64_t* cp, float* radius, void* stream);
+
+/* Adds d L / d height to grad_height[rows][cols] given the splat-input gradients
+ * (grad_Ep[N], grad_xp[2][N], grad_Mp[2][3][N], e.g. from pds_backward_f32). The chain is
+ * recomputed from the height field; nothing from the forward is needed. */
+int pds_refract_backward_f32(const float* height, int32_t rows, int32_t cols,
+                             const pds_plate* plate, const float* px, const float* py,
+                             const float* flux, int64_t n_photons, const float* grad_Ep,
+                             const float* grad_xp, const float* grad_Mp, float* grad_height,
+                             void* stream);
+
+/* ---- projected Landweber update of the height field ------------------------------- */
+/* One update of the reference's pixel-basis Landweber loop (shape_from_caustics.py:386-398):
+ * d <- VconsHeur(mask * extShrink(d - tau * grad, shrink, lower, upper)), with extShrink
+ * (:184-189) and the volume heuristic VconsHeur (:228-241). */
+typedef struct pds_landweber {
+    float tau;          /* gradient step (the reference's tau_pixel) */
+    float shrink;       /* soft-shrinkage threshold (tau_pixel * alpha_pixel) */
+    float lower, upper; /* clamp of the extended shrinkage */
+    float d1, d2;       /* volume window, in units of the summed offsets */
+    float gamma;        /* volume heuristic step */
+    int32_t radius;     /* volume heuristic box radius (pixels) */
+} pds_landweber;
+
+size_t pds_landweber_workspace_bytes(int64_t rows, int64_t cols);
+
+/* d[rows][cols] updated in place; grad, mask (0/1 floats) same shape. */
+int pds_landweber_update_f32(float* d, const float* grad, const float* mask, int64_t rows,
+                             int64_t cols, const pds_landweber* params, void* workspace,
+                             size_t workspace_bytes, void* stream);
 
 /* ---- device radix sort (exposed for its bit-exactness tests) ----------------------- */
 /* Stable ascending sort of keys[n] (only the low key_bits bits are compared) carrying the

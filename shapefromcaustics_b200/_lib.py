@@ -20,7 +20,8 @@ PDS_ERR_UNSUPPORTED = 4
 class PdsConfig(ctypes.Structure):
     """Mirror of ``pds_config``."""
     _fields_ = [("tile", ctypes.c_int32), ("chunk", ctypes.c_int32),
-                ("class_bits", ctypes.c_int32), ("apron_max", ctypes.c_int32)]
+                ("class_bits", ctypes.c_int32), ("apron_max", ctypes.c_int32),
+                ("walk", ctypes.c_int32)]
 
 
 class PdsSim(ctypes.Structure):
@@ -33,6 +34,20 @@ class PdsSim(ctypes.Structure):
 
 
 assert ctypes.sizeof(PdsSim) == 56
+
+
+class PdsPlate(ctypes.Structure):
+    """Mirror of ``pds_plate``."""
+    _fields_ = [("texel", ctypes.c_float), ("ior", ctypes.c_float),
+                ("receiver_distance", ctypes.c_float), ("receiver_half", ctypes.c_float),
+                ("light_dir", ctypes.c_float * 3), ("du0", ctypes.c_float)]
+
+class PdsLandweber(ctypes.Structure):
+    """Mirror of ``pds_landweber``."""
+    _fields_ = [("tau", ctypes.c_float), ("shrink", ctypes.c_float), ("lower", ctypes.c_float),
+                ("upper", ctypes.c_float), ("d1", ctypes.c_float), ("d2", ctypes.c_float),
+                ("gamma", ctypes.c_float), ("radius", ctypes.c_int32)]
+
 
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
@@ -64,6 +79,13 @@ SIGNATURES = {
                                                      _I64, _I32, _P, _P, _SZ, _CFG, _P]),
     "pds_batch_backward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _P, _I32,
                                                       _I64, _I32, _P, _P, _P, _P, _SZ, _CFG, _P]),
+    "pds_refract_forward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate), _P, _P,
+                                               _P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "pds_refract_backward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate), _P, _P,
+                                                _P, _I64, _P, _P, _P, _P, _P]),
+    "pds_landweber_workspace_bytes": (_SZ, [_I64, _I64]),
+    "pds_landweber_update_f32": (ctypes.c_int, [_P, _P, _P, _I64, _I64,
+                                                ctypes.POINTER(PdsLandweber), _P, _SZ, _P]),
     "pds_sort_workspace_bytes": (_SZ, [_I64]),
     "pds_sort_u32": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P, _SZ, _P]),
 }
@@ -105,5 +127,5 @@ def check(rc):
         raise PdsError(rc, msg)
 
 
-def config(tile=0, chunk=0, class_bits=0, apron_max=0):
-    return PdsConfig(int(tile), int(chunk), int(class_bits), int(apron_max))
+def config(tile=0, chunk=0, class_bits=0, apron_max=0, walk=0):
+    return PdsConfig(int(tile), int(chunk), int(class_bits), int(apron_max), int(walk))

@@ -50,6 +50,9 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
     out.chunk = (in && in->chunk) ? in->chunk : 2048;
     out.class_bits = in ? in->class_bits : 0;
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
+    out.walk = (in && in->walk) ? in->walk : 2;
+    if (out.walk != 1 && out.walk != 2)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.walk must be 1 (box) or 2 (spans)");
     if (out.tile != 16 && out.tile != 32 && out.tile != 64)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.tile must be 16, 32 or 64");
     if (out.chunk < 256 || out.chunk > (1 << 20) || out.chunk % 256 != 0)
@@ -77,6 +80,7 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     r.cfg.class_bits = c.class_bits;
     r.cfg.apron = mpr < 0 ? 0 : (mpr < c.apron_max ? mpr : c.apron_max);
     r.cfg.sw = c.tile + 2 * r.cfg.apron;
+    r.cfg.spans = c.walk == 2 ? 1 : 0;
     r.key_big = uint32_t(uint64_t(n_tiles) << c.class_bits);
     r.key_invalid = uint32_t(inv);
     r.key_bits = bit_length(inv);
@@ -440,6 +444,74 @@ int pds_batch_backward_planned_f32(const float* G, const float* E, const float* 
     return backward_impl(G, photons(E, X, M, cp, R, n_total), table_dev(sims_dev, n_sims),
                          n_tiles, mpr, gE, gX, gM, cfg, ws, ws_bytes,
                          static_cast<cudaStream_t>(stream));
+}
+
+static int check_plate(const float* h, int32_t rows, int32_t cols, const pds_plate* plate,
+                       const float* px, const float* py, const float* flux, int64_t n) {
+    if (!plate) return fail(PDS_ERR_INVALID_ARGUMENT, "null plate");
+    if (rows < 1 || cols < 1 || !h) return fail(PDS_ERR_INVALID_ARGUMENT, "empty height field");
+    if (n < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative photon count");
+    if (n > 0 && (!px || !py || !flux)) return fail(PDS_ERR_INVALID_ARGUMENT, "null photon array");
+    if (!(plate->texel > 0.f) || !(plate->ior > 0.f) || !(plate->receiver_half > 0.f) ||
+        !(plate->receiver_distance >= 0.f))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "plate parameters must be positive");
+    return PDS_OK;
+}
+
+int pds_refract_forward_f32(const float* h, int32_t rows, int32_t cols, const pds_plate* plate,
+                            const float* px, const float* py, const float* flux,
+                            const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
+                            int64_t* cp, float* radius, void* stream) {
+    int rc = check_plate(h, rows, cols, plate, px, py, flux, n);
+    if (rc) return rc;
+    if (n > 0 && (!Ep || !xp || !Mp || !cp || !radius))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
+    cudaError_t e = pds::launch_refract(false, h, rows, cols, *plate, px, py, flux, channel, n, Ep,
+                                        xp, Mp, cp, radius, nullptr, nullptr, nullptr, nullptr,
+                                        static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "refract_fwd_kernel");
+    return PDS_OK;
+}
+
+int pds_refract_backward_f32(const float* h, int32_t rows, int32_t cols, const pds_plate* plate,
+                             const float* px, const float* py, const float* flux, int64_t n,
+                             const float* gE, const float* gX, const float* gM, float* gh,
+                             void* stream) {
+    int rc = check_plate(h, rows, cols, plate, px, py, flux, n);
+    if (rc) return rc;
+    if (n > 0 && (!gE || !gX || !gM || !gh))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
+    cudaError_t e = pds::launch_refract(true, h, rows, cols, *plate, px, py, flux, nullptr, n,
+                                        nullptr, nullptr, nullptr, nullptr, nullptr, gE, gX, gM,
+                                        gh, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel");
+    return PDS_OK;
+}
+
+size_t pds_landweber_workspace_bytes(int64_t rows, int64_t cols) {
+    return pds::landweber_scratch_bytes(rows * cols);
+}
+
+int pds_landweber_update_f32(float* d, const float* grad, const float* mask, int64_t rows,
+                             int64_t cols, const pds_landweber* p, void* ws, size_t ws_bytes,
+                             void* stream) {
+    if (!p) return fail(PDS_ERR_INVALID_ARGUMENT, "null Landweber parameters");
+    if (rows < 1 || cols < 1) return fail(PDS_ERR_INVALID_ARGUMENT, "empty height field");
+    if (!d || !grad || !mask) return fail(PDS_ERR_INVALID_ARGUMENT, "null height-field array");
+    if (p->radius < 0 || p->radius > 64)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "volume radius outside [0, 64]");
+    if (!(p->d1 != 0.f) || !(p->d2 != 0.f))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "volume bounds d1, d2 must be nonzero");
+    const int64_t n = rows * cols;
+    int rc = check_ws(ws, ws_bytes, pds::landweber_scratch_bytes(n));
+    if (rc) return rc;
+    float* t = static_cast<float*>(ws);
+    float* partial = reinterpret_cast<float*>(static_cast<char*>(ws) +
+                                              pds::align_up(size_t(n) * sizeof(float), 256));
+    cudaError_t e = pds::launch_landweber(d, grad, mask, rows, cols, *p, t, partial,
+                                          static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "landweber kernels");
+    return PDS_OK;
 }
 
 size_t pds_sort_workspace_bytes(int64_t n) {

@@ -57,6 +57,7 @@ struct Cfg {
     int32_t class_bits;
     int32_t apron;       // min(max_pixel_radius, apron_max), >= 0
     int32_t sw;          // tile + 2 * apron: edge of the shared accumulator
+    int32_t spans;       // 1: walk only the support's rows / row spans; 0: the whole box
 };
 
 // Simulation table: either a device array or one inline descriptor.
@@ -134,6 +135,60 @@ __device__ __forceinline__ bool clip_box(const Footprint& f, int32_t H, int32_t 
     if (a > b || c > d) return false;
     x0 = int32_t(a); x1 = int32_t(b); y0 = int32_t(c); y1 = int32_t(d);
     return true;
+}
+
+// Rows and per-row column spans of the support |M d| < 1 (d the normalised offset from the
+// photon), in pixel offsets from the centre pixel, one pixel wider on each side than the
+// float solution so that every pixel whose float s is below 1 is inside. With
+// a = |M e_x|^2, b = (M e_x . M e_y) dy, c = |M e_y|^2 dy^2 - 1 the row's support is
+// a dx^2 + 2 b dx + c < 0, and the support's half-height is sqrt(a) / |det M|.
+// Degenerate, near-singular or non-finite M falls back to the whole box.
+struct Support {
+    bool on;
+    float a, inv_a, bco, cco, ey;
+};
+
+__device__ __forceinline__ Support make_support(float m00, float m01, float m10, float m11,
+                                                bool enabled) {
+    Support g;
+    g.on = false;
+    if (!enabled) return g;
+    const float a = fmaf(m00, m00, m10 * m10);
+    const float det = fmaf(m00, m11, -m01 * m10);
+    const float ey = sqrtf(a) / fabsf(det);
+    if (!(a > 0.f) || !isfinite(a) || !isfinite(ey)) return g;
+    // near-singular M: the float determinant has cancelled, so its support size is unreliable
+    if (!(fabsf(det) > 1e-3f * (fabsf(m00 * m11) + fabsf(m01 * m10)))) return g;
+    g.on = true;
+    g.a = a;
+    g.inv_a = 1.f / a;
+    g.bco = fmaf(m00, m01, m10 * m11);
+    g.cco = fmaf(m01, m01, m11 * m11);
+    g.ey = ey;
+    return g;
+}
+
+// Narrows the row range [ky0, ky1] (offsets from the centre pixel) to the support.
+__device__ __forceinline__ void support_rows(const Support& g, float dy0, float inv_sy, int& ky0,
+                                             int& ky1) {
+    if (!g.on) return;
+    ky0 = max(ky0, __float2int_ru((-g.ey - dy0) * inv_sy) - 1);
+    ky1 = min(ky1, __float2int_rd((g.ey - dy0) * inv_sy) + 1);
+}
+
+// Narrows the column range [kx0, kx1] of the row at normalised offset dy; false if empty.
+__device__ __forceinline__ bool support_cols(const Support& g, float dy, float dx0, float inv_sx,
+                                             int& kx0, int& kx1) {
+    if (!g.on) return true;
+    const float b = g.bco * dy;
+    const float c = fmaf(g.cco * dy, dy, -1.f);
+    const float disc = fmaf(b, b, -g.a * c);
+    if (!(disc >= 0.f)) return false;
+    const float r = sqrtf(disc);
+    const float lo = (-b - r) * g.inv_a, hi = (r - b) * g.inv_a;
+    kx0 = max(kx0, __float2int_ru((lo - dx0) * inv_sx) - 1);
+    kx1 = min(kx1, __float2int_rd((hi - dx0) * inv_sx) + 1);
+    return kx0 <= kx1;
 }
 
 // delta = (2 p_c / w - 1) - x in double, rounded once to float.

@@ -19,4 +19,17 @@ cudaError_t radix_sort(const uint32_t* keys_in, uint32_t* k0, uint32_t* k1, uint
                        uint32_t** keys_out, uint32_t** vals_out);
 void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st);
 
+// refraction to the receiver (pds_refract.cu)
+cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
+                           const float* px, const float* py, const float* flux,
+                           const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
+                           int64_t* cp, float* radius, const float* gE, const float* gX,
+                           const float* gM, float* gh, cudaStream_t st);
+
+// Landweber update (pds_landweber.cu)
+size_t landweber_scratch_bytes(int64_t n);
+cudaError_t launch_landweber(float* d, const float* g, const float* mask, int64_t rows,
+                             int64_t cols, const pds_landweber& p, float* t, float* partial,
+                             cudaStream_t st);
+
 }  // namespace pds

@@ -1,0 +1,440 @@
+// Fused refraction-to-receiver for a glass plate with a height-field top face (sm_100a).
+//
+// Per photon, from the height field h and the photon's entry point (px, py):
+//   surface sample      bilinear h and bilinear Sobel normal N~ = (-dh/dx, -dh/dy, 1) with its
+//                       x/y derivatives (model/caustics.py:215-221: replicate padding, kernel
+//                       scaled by -1/(8 texel))
+//   transfer            positional differentials onto the tangent plane
+//                       (model/photon_differential.py:69-78)
+//   refraction x2       Snell + Igehy direction differentials (model/caustics.py:176-189),
+//                       normal derivative of the normalised normal along the positional
+//                       differential (model/renderable_object.py:391-401); flat bottom face
+//   receiver            propagation to the receiver plane, normalised coordinates
+//   splat inputs        Mp = 2 [Du Dv]^-1, radius = |D|max / 2, Ep = 4 flux / |Du x Dv|
+//                       (model/caustics.py:224-239); degenerate photons get channel -1
+// and writes the splat inputs (Ep, xp, Mp, cp, radius) in the reference's layouts.
+//
+// The backward recomputes the chain from h (nothing is stored between the passes) in
+// forward-mode dual numbers over the seven height-dependent scalars of the photon (height,
+// N~x, N~y and their x/y derivatives), contracts with the splat-input gradients, and maps
+// the result back onto the photon's 4x4 texel patch through the transposed bilinear and
+// Sobel stencils. Patches are accumulated with global float adds.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pds_b200.h"
+#include "pds_internal.h"
+
+namespace pds {
+namespace {
+
+constexpr int K = 7;  // height-dependent scalars of one photon
+
+struct Dual {
+    float v;
+    float d[K];
+};
+
+__device__ __forceinline__ Dual dconst(float v) {
+    Dual r;
+    r.v = v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = 0.f;
+    return r;
+}
+__device__ __forceinline__ Dual operator+(const Dual& a, const Dual& b) {
+    Dual r; r.v = a.v + b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual operator-(const Dual& a, const Dual& b) {
+    Dual r; r.v = a.v - b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual operator-(const Dual& a) {
+    Dual r; r.v = -a.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = -a.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual operator*(const Dual& a, const Dual& b) {
+    Dual r; r.v = a.v * b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = fmaf(a.d[k], b.v, a.v * b.d[k]);
+    return r;
+}
+__device__ __forceinline__ Dual operator*(float s, const Dual& a) {
+    Dual r; r.v = s * a.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = s * a.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual operator+(const Dual& a, float s) {
+    Dual r = a; r.v += s; return r;
+}
+__device__ __forceinline__ Dual operator/(const Dual& a, const Dual& b) {
+    const float inv = 1.f / b.v;
+    Dual r; r.v = a.v * inv;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * inv;
+    return r;
+}
+__device__ __forceinline__ Dual dsqrt(const Dual& a) {
+    Dual r; r.v = sqrtf(a.v);
+    const float h = 0.5f / r.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * h;
+    return r;
+}
+__device__ __forceinline__ Dual dabs(const Dual& a) { return a.v < 0.f ? -a : a; }
+__device__ __forceinline__ Dual dmax(const Dual& a, const Dual& b) { return a.v >= b.v ? a : b; }
+
+__device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ float dabs(float a) { return fabsf(a); }
+__device__ __forceinline__ float dmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float dconstf(float v) { return v; }
+
+template <class T>
+struct V3 {
+    T x, y, z;
+};
+template <class T>
+__device__ __forceinline__ V3<T> vadd(const V3<T>& a, const V3<T>& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T>
+__device__ __forceinline__ V3<T> vsub(const V3<T>& a, const V3<T>& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T, class S>
+__device__ __forceinline__ V3<T> vscale(const S& s, const V3<T>& a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T>
+__device__ __forceinline__ T vdot(const V3<T>& a, const V3<T>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+template <class T>
+__device__ __forceinline__ T cst(float v);
+template <>
+__device__ __forceinline__ float cst<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ Dual cst<Dual>(float v) { return dconst(v); }
+
+struct PlateParams {
+    float texel, ior, dist, inv_half, du0;
+    float lx, ly, lz;  // light direction
+};
+
+// Snell refraction of direction d and its differential Dd at unit normal n facing the
+// incident side (d.n < 0), with normal derivative dn (model/caustics.py:176-189).
+template <class T>
+__device__ __forceinline__ void refract(const V3<T>& d, const V3<T>& n, const V3<T>& Dd,
+                                        const V3<T>& dn, float eta, V3<T>& out, V3<T>& Dout) {
+    T cosi = vdot(d, n);
+    const T k = cst<T>(1.f) - eta * eta * (cst<T>(1.f) - cosi * cosi);
+    const T neg_sq = -dsqrt(k);
+    const T coso = eta * cosi - neg_sq;
+    out = vsub(vscale(eta, d), vscale(coso, n));
+    const T f = cst<T>(eta) - (eta * eta) * cosi / neg_sq;
+    const T q = f * (vdot(Dd, n) + vdot(d, dn));
+    Dout = vsub(vscale(eta, Dd), vadd(vscale(coso, dn), vscale(q, n)));
+}
+
+// D carried along direction t for length s onto the plane z = const
+// (model/photon_differential.py:69-78 with n = e_z).
+template <class T>
+__device__ __forceinline__ V3<T> transfer_z(const V3<T>& D, const V3<T>& Dd, const T& s,
+                                            const V3<T>& t) {
+    const T a = D.z / t.z;
+    const T b = Dd.z / t.z;
+    return vadd(vsub(D, vscale(a, t)), vscale(s, vsub(Dd, vscale(b, t))));
+}
+
+// The refraction chain for one photon. Inputs: the seven height-dependent scalars.
+// Outputs: receiver position (normalised) and the receiver-plane differentials (x, y parts).
+template <class T>
+__device__ __forceinline__ void plate_chain(const T& hz, const T& Nx, const T& Ny, const T& Nxx,
+                                            const T& Nyx, const T& Nxy, const T& Nyy, float px,
+                                            float py, const PlateParams& P, T& xr, T& yr,
+                                            T& Dux, T& Duy, T& Dvx, T& Dvy) {
+    const V3<T> d = {cst<T>(P.lx), cst<T>(P.ly), cst<T>(P.lz)};
+    const V3<T> Nt = {Nx, Ny, cst<T>(1.f)};
+    const T nn = vdot(Nt, Nt);
+    const T nlen = dsqrt(nn);
+    const V3<T> n = vscale(cst<T>(1.f) / nlen, Nt);
+    const T nd = vdot(n, d);
+    // source-plane differentials (du0, 0, 0) and (0, du0, 0) onto the tangent plane
+    const V3<T> Du1 = vsub(V3<T>{cst<T>(P.du0), cst<T>(0.f), cst<T>(0.f)}, vscale((P.du0 * n.x) / nd, d));
+    const V3<T> Dv1 = vsub(V3<T>{cst<T>(0.f), cst<T>(P.du0), cst<T>(0.f)}, vscale((P.du0 * n.y) / nd, d));
+    // derivative of the normalised normal along each positional differential
+    const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
+    const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
+    const T nl3 = nn * nlen;
+    const V3<T> dnu = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
+    const V3<T> dnv = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
+    // air -> glass at the top face
+    const V3<T> zero = {cst<T>(0.f), cst<T>(0.f), cst<T>(0.f)};
+    V3<T> t1, Ddu, Ddv, tmp;
+    refract(d, n, zero, dnu, 1.f / P.ior, t1, Ddu);
+    refract(d, n, zero, dnv, 1.f / P.ior, tmp, Ddv);
+    // to the bottom face z = 0
+    const T s1 = -hz / t1.z;
+    const V3<T> p2 = {cst<T>(px) + s1 * t1.x, cst<T>(py) + s1 * t1.y, cst<T>(0.f)};
+    const V3<T> Du2 = transfer_z(Du1, Ddu, s1, t1);
+    const V3<T> Dv2 = transfer_z(Dv1, Ddv, s1, t1);
+    // glass -> air at the flat bottom face (normal +z faces the glass side)
+    const V3<T> ez = {cst<T>(0.f), cst<T>(0.f), cst<T>(1.f)};
+    V3<T> t2, Ddu2, Ddv2;
+    refract(t1, ez, Ddu, zero, P.ior, t2, Ddu2);
+    refract(t1, ez, Ddv, zero, P.ior, tmp, Ddv2);
+    // to the receiver plane z = -dist
+    const T s2 = cst<T>(-P.dist) / t2.z;
+    const V3<T> Du3 = transfer_z(Du2, Ddu2, s2, t2);
+    const V3<T> Dv3 = transfer_z(Dv2, Ddv2, s2, t2);
+    xr = P.inv_half * (p2.x + s2 * t2.x);
+    yr = P.inv_half * (p2.y + s2 * t2.y);
+    Dux = P.inv_half * Du3.x;
+    Duy = P.inv_half * Du3.y;
+    Dvx = P.inv_half * Dv3.x;
+    Dvy = P.inv_half * Dv3.y;
+}
+
+// Bilinear footprint of a world position on the height-field grid (texel centres at
+// integers, clamped to the border).
+struct Bilin {
+    int x0, y0;
+    float ax, ay;
+};
+
+__device__ __forceinline__ Bilin bilin(float px, float py, float texel, int H, int W) {
+    float fx = px / texel + 0.5f * float(W - 1);
+    float fy = py / texel + 0.5f * float(H - 1);
+    fx = fminf(fmaxf(fx, 0.f), float(W - 1));
+    fy = fminf(fmaxf(fy, 0.f), float(H - 1));
+    Bilin b;
+    b.x0 = min(int(floorf(fx)), max(W - 2, 0));
+    b.y0 = min(int(floorf(fy)), max(H - 2, 0));
+    b.ax = fx - float(b.x0);
+    b.ay = fy - float(b.y0);
+    return b;
+}
+
+__device__ __forceinline__ float hat(const float* h, int H, int W, int i, int j) {
+    i = min(max(i, 0), H - 1);
+    j = min(max(j, 0), W - 1);
+    return __ldg(h + int64_t(i) * W + j);
+}
+
+// The seven scalars of one photon: height, Sobel normal (x, y) and their x/y derivatives.
+__device__ __forceinline__ void surface_scalars(const float* h, int H, int W, float texel,
+                                                const Bilin& b, float s[K]) {
+    const float c = -1.f / (8.f * texel);
+    float hv[2][2], nx[2][2], ny[2][2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int i = b.y0 + r, j = min(b.x0 + q, W - 1);
+            hv[r][q] = hat(h, H, W, i, j);
+            nx[r][q] = c * (hat(h, H, W, i - 1, j + 1) - hat(h, H, W, i - 1, j - 1) +
+                            2.f * (hat(h, H, W, i, j + 1) - hat(h, H, W, i, j - 1)) +
+                            hat(h, H, W, i + 1, j + 1) - hat(h, H, W, i + 1, j - 1));
+            ny[r][q] = c * (hat(h, H, W, i + 1, j - 1) - hat(h, H, W, i - 1, j - 1) +
+                            2.f * (hat(h, H, W, i + 1, j) - hat(h, H, W, i - 1, j)) +
+                            hat(h, H, W, i + 1, j + 1) - hat(h, H, W, i - 1, j + 1));
+        }
+    }
+    auto val = [&](float v[2][2]) {
+        const float top = v[0][0] + (v[0][1] - v[0][0]) * b.ax;
+        const float bot = v[1][0] + (v[1][1] - v[1][0]) * b.ax;
+        return top + (bot - top) * b.ay;
+    };
+    auto ddx = [&](float v[2][2]) {
+        return ((v[0][1] - v[0][0]) * (1.f - b.ay) + (v[1][1] - v[1][0]) * b.ay) / texel;
+    };
+    auto ddy = [&](float v[2][2]) {
+        const float top = v[0][0] + (v[0][1] - v[0][0]) * b.ax;
+        const float bot = v[1][0] + (v[1][1] - v[1][0]) * b.ax;
+        return (bot - top) / texel;
+    };
+    s[0] = val(hv);
+    s[1] = val(nx);
+    s[2] = val(ny);
+    s[3] = ddx(nx);  // dNx/dx
+    s[4] = ddx(ny);  // dNy/dx
+    s[5] = ddy(nx);  // dNx/dy
+    s[6] = ddy(ny);  // dNy/dy
+}
+
+struct RefractArgs {
+    const float* h;
+    int H, W;
+    PlateParams P;
+    const float* px;
+    const float* py;
+    const float* flux;
+    const int64_t* channel;
+    int64_t n;
+    // forward outputs
+    float* Ep;
+    float* xp;
+    float* Mp;
+    int64_t* cp;
+    float* radius;
+    // backward inputs / output
+    const float* gE;
+    const float* gX;
+    const float* gM;
+    float* gh;
+};
+
+__global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
+    const int64_t n = a.n;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const float px = a.px[i], py = a.py[i];
+        const Bilin b = bilin(px, py, a.P.texel, a.H, a.W);
+        float s[K];
+        surface_scalars(a.h, a.H, a.W, a.P.texel, b, s);
+        float xr, yr, Dux, Duy, Dvx, Dvy;
+        plate_chain<float>(s[0], s[1], s[2], s[3], s[4], s[5], s[6], px, py, a.P, xr, yr, Dux,
+                           Duy, Dvx, Dvy);
+        const float den = Dux * Dvy - Duy * Dvx;
+        const bool good = den != 0.f;
+        const float f = 2.f / (good ? den : 1.f);
+        a.Mp[i] = f * Dvy;
+        a.Mp[n + i] = -f * Dvx;
+        a.Mp[2 * n + i] = 0.f;
+        a.Mp[3 * n + i] = -f * Duy;
+        a.Mp[4 * n + i] = f * Dux;
+        a.Mp[5 * n + i] = 0.f;
+        a.xp[i] = xr;
+        a.xp[n + i] = yr;
+        a.radius[i] = 0.5f * fmaxf(sqrtf(Dux * Dux + Duy * Duy), sqrtf(Dvx * Dvx + Dvy * Dvy));
+        a.Ep[i] = 4.f * a.flux[i] / (good ? fabsf(den) : 1.f);
+        const int64_t ch = a.channel ? a.channel[i] : 0;
+        a.cp[i] = good ? ch : -1;
+    }
+}
+
+__global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
+    const int64_t n = a.n;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const float px = a.px[i], py = a.py[i];
+        const Bilin b = bilin(px, py, a.P.texel, a.H, a.W);
+        float s[K];
+        surface_scalars(a.h, a.H, a.W, a.P.texel, b, s);
+        Dual v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            v[k] = dconst(s[k]);
+            v[k].d[k] = 1.f;
+        }
+        Dual xr, yr, Dux, Duy, Dvx, Dvy;
+        plate_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], px, py, a.P, xr, yr, Dux,
+                          Duy, Dvx, Dvy);
+        const Dual den = Dux * Dvy - Duy * Dvx;
+        if (den.v == 0.f) continue;  // degenerate photon: skipped by the splat, no gradient
+        const Dual f = dconst(2.f) / den;
+        const float gE = a.gE[i];
+        const float g0 = a.gM[i], g1 = a.gM[n + i], g3 = a.gM[3 * n + i], g4 = a.gM[4 * n + i];
+        // L = gE Ep + gx xr + gy yr + sum gM Mp, as a dual over the seven scalars
+        Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
+        L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
+        L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
+        // map d L / d scalars onto the 4x4 texel patch (x0-1..x0+2, y0-1..y0+2)
+        float patch[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) patch[r][q] = 0.f;
+        const float c = -1.f / (8.f * a.P.texel);
+        const float it = 1.f / a.P.texel;
+        const float wv[2][2] = {{(1.f - b.ay) * (1.f - b.ax), (1.f - b.ay) * b.ax},
+                                {b.ay * (1.f - b.ax), b.ay * b.ax}};
+        const float wx[2][2] = {{-(1.f - b.ay) * it, (1.f - b.ay) * it}, {-b.ay * it, b.ay * it}};
+        const float wy[2][2] = {{-(1.f - b.ax) * it, -b.ax * it}, {(1.f - b.ax) * it, b.ax * it}};
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                patch[r + 1][q + 1] += L.d[0] * wv[r][q];
+                const float gnx = c * (L.d[1] * wv[r][q] + L.d[3] * wx[r][q] + L.d[5] * wy[r][q]);
+                const float gny = c * (L.d[2] * wv[r][q] + L.d[4] * wx[r][q] + L.d[6] * wy[r][q]);
+                // Sobel x at (r, q): +(r-1,q+1) -(r-1,q-1) +2(r,q+1) -2(r,q-1) +(r+1,q+1) -(r+1,q-1)
+                patch[r][q + 2] += gnx;
+                patch[r][q] -= gnx;
+                patch[r + 1][q + 2] += 2.f * gnx;
+                patch[r + 1][q] -= 2.f * gnx;
+                patch[r + 2][q + 2] += gnx;
+                patch[r + 2][q] -= gnx;
+                // Sobel y: +(r+1,q-1) -(r-1,q-1) +2(r+1,q) -2(r-1,q) +(r+1,q+1) -(r-1,q+1)
+                patch[r + 2][q] += gny;
+                patch[r][q] -= gny;
+                patch[r + 2][q + 1] += 2.f * gny;
+                patch[r][q + 1] -= 2.f * gny;
+                patch[r + 2][q + 2] += gny;
+                patch[r][q + 2] -= gny;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int ii = min(max(b.y0 - 1 + r, 0), a.H - 1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int jj = min(max(b.x0 - 1 + q, 0), a.W - 1);
+                if (patch[r][q] != 0.f) atomicAdd(a.gh + int64_t(ii) * a.W + jj, patch[r][q]);
+            }
+        }
+    }
+}
+
+int grid_for(int64_t n) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t blocks = (n + 255) / 256;
+    const int64_t cap = int64_t(sms) * 8;
+    return int(blocks < cap ? blocks : cap);
+}
+
+}  // namespace
+
+cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
+                           const float* px, const float* py, const float* flux,
+                           const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
+                           int64_t* cp, float* radius, const float* gE, const float* gX,
+                           const float* gM, float* gh, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    RefractArgs a;
+    a.h = h;
+    a.H = H;
+    a.W = W;
+    a.P.texel = plate.texel;
+    a.P.ior = plate.ior;
+    a.P.dist = plate.receiver_distance;
+    a.P.inv_half = 1.f / plate.receiver_half;
+    a.P.du0 = plate.du0;
+    a.P.lx = plate.light_dir[0];
+    a.P.ly = plate.light_dir[1];
+    a.P.lz = plate.light_dir[2];
+    a.px = px;
+    a.py = py;
+    a.flux = flux;
+    a.channel = channel;
+    a.n = n;
+    a.Ep = Ep;
+    a.xp = xp;
+    a.Mp = Mp;
+    a.cp = cp;
+    a.radius = radius;
+    a.gE = gE;
+    a.gX = gX;
+    a.gM = gM;
+    a.gh = gh;
+    if (backward)
+        refract_bwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+    else
+        refract_fwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace pds

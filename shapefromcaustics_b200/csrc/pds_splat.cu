@@ -105,6 +105,7 @@ struct TileInfo {
     int32_t W, H;
     int32_t ox, oy;   // pixel coordinates of the accumulator's (0, 0)
     float sx, sy;     // 2 / W, 2 / H
+    float isx, isy;   // W / 2, H / 2
     double wd, hd;    // float(W), float(H) in double (the reference's w, h)
 };
 
@@ -124,14 +125,18 @@ __device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t til
     t.oy = ty * cfg.tile - cfg.apron;
     t.sx = float(2.0 / double(sim.width));
     t.sy = float(2.0 / double(sim.height));
+    t.isx = 0.5f * float(sim.width);
+    t.isy = 0.5f * float(sim.height);
     t.wd = double(float(sim.width));
     t.hd = double(float(sim.height));
     return t;
 }
 
 // Forward deposit of one photon into the shared accumulator (photon_differentials.cu:91-110).
-__device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, float* acc,
-                                        int& bx0, int& bx1, int& by0, int& by1) {
+// With spans on, only the support's rows and row spans are visited; the other box pixels
+// add exactly zero in the reference (value > 0 fails, :106).
+__device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
+                                        float* acc, int& bx0, int& bx1, int& by0, int& by1) {
     const uint32_t p = r.packed;
     const uint32_t fl = rec_flags(p);
     if (fl & kFlagFwdSkip) return;
@@ -142,19 +147,22 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
     bx0 = x0; bx1 = x1; by0 = y0; by1 = y1;
     const float e3 = r.e * kThreeOverPi;
     const bool all = fl & kFlagEllipseAll;
-    for (int py = y0; py <= y1; ++py) {
-        const int ky = py - pyc;
+    const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
+    int ky0 = y0 - pyc, ky1 = y1 - pyc;
+    support_rows(sup, r.dy0, ti.isy, ky0, ky1);
+    for (int ky = ky0; ky <= ky1; ++ky) {
         const float dy = fmaf(float(ky), ti.sy, r.dy0);
+        int kx0 = x0 - pxc, kx1 = x1 - pxc;
+        if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
         const float a0 = r.m01 * dy, a1 = r.m11 * dy;
-        float* row = acc + (py - ti.oy) * sw - ti.ox;
-        for (int px = x0; px <= x1; ++px) {
-            const int kx = px - pxc;
+        float* row = acc + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
+        for (int kx = kx0; kx <= kx1; ++kx) {
             const float dx = fmaf(float(kx), ti.sx, r.dx0);
             const float u0 = fmaf(r.m00, dx, a0), u1 = fmaf(r.m10, dx, a1);
             const float s = fmaf(u0, u0, u1 * u1);
             if (s < 1.f && (all || ellipse_ok(kx, ky, ti.wd, ti.hd))) {
                 const float t = 1.f - s;
-                atomicAdd(row + px, t * t * e3);
+                atomicAdd(row + kx, t * t * e3);
             }
         }
     }
@@ -231,7 +239,7 @@ __global__ __launch_bounds__(NT) void fwd_tiles_kernel(TileArgs a) {
             while (true) {
                 const bool mine = have && key == cur;
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-                if (mine) deposit(r, ti, sw, acc, x0, x1, y0, y1);
+                if (mine) deposit(r, ti, sw, cfg.spans, acc, x0, x1, y0, y1);
                 bbox_publish(sb, x0, x1, y0, y1);
                 const int cnt = __syncthreads_count(mine);
                 const int64_t nxt = base + cnt;
@@ -263,7 +271,9 @@ __device__ __forceinline__ void load_region(float* tg, int sw, const TileInfo& t
 }
 
 // Backward gather of one photon (photon_differentials.cu:169-218) from the staged gradient.
-__device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
+// Pixels outside the support contribute 0 * g in the reference; with spans on they are not
+// visited.
+__device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                        const float* tg, uint32_t rid, const TileArgs& a) {
     const uint32_t p = r.packed;
     const uint32_t fl = rec_flags(p);
@@ -272,21 +282,24 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
     const int x0 = max(pxc - rx, 0), x1 = min(pxc + rx, ti.W - 1);
     const int y0 = max(pyc - ry, 0), y1 = min(pyc + ry, ti.H - 1);
     const bool all = fl & kFlagEllipseAll;
+    const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
+    int ky0 = y0 - pyc, ky1 = y1 - pyc;
+    support_rows(sup, r.dy0, ti.isy, ky0, ky1);
     float sE = 0.f, Sx = 0.f, Sy = 0.f, Sxx = 0.f, Sxy = 0.f, Syy = 0.f;
-    for (int py = y0; py <= y1; ++py) {
-        const int ky = py - pyc;
+    for (int ky = ky0; ky <= ky1; ++ky) {
         const float dy = fmaf(float(ky), ti.sy, r.dy0);
+        int kx0 = x0 - pxc, kx1 = x1 - pxc;
+        if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
         const float a0 = r.m01 * dy, a1 = r.m11 * dy;
-        const float* row = tg + (py - ti.oy) * sw - ti.ox;
+        const float* row = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
         float A0 = 0.f, A1 = 0.f, A2 = 0.f;
-        for (int px = x0; px <= x1; ++px) {
-            const int kx = px - pxc;
+        for (int kx = kx0; kx <= kx1; ++kx) {
             if (!all && !ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
             const float dx = fmaf(float(kx), ti.sx, r.dx0);
             const float u0 = fmaf(r.m00, dx, a0), u1 = fmaf(r.m10, dx, a1);
             const float s = fmaf(u0, u0, u1 * u1);
             const float t = s < 1.f ? 1.f - s : 0.f;
-            const float g = row[px];
+            const float g = row[kx];
             const float tgv = t * g;
             sE = fmaf(t, tgv, sE);
             A0 += tgv;
@@ -344,7 +357,7 @@ __global__ __launch_bounds__(NT) void bwd_tiles_kernel(TileArgs a) {
                     loaded = cur;
                 }
                 const bool mine = have && key == cur;
-                if (mine) gather(r, ti, sw, tg, rid, a);
+                if (mine) gather(r, ti, sw, cfg.spans, tg, rid, a);
                 const int cnt = __syncthreads_count(mine);
                 const int64_t nxt = base + cnt;
                 if (nxt >= bend) break;

@@ -1,0 +1,162 @@
+"""Projected Landweber update of the height field and the reconstruction loop around it.
+
+``landweber_update`` is the fused device update (``pds_landweber_update_f32``);
+``landweber_update_reference`` restates the reference's PyTorch ops
+(``shape_from_caustics.py:184-189`` extShrink, ``:228-241`` VconsHeur, ``:386-398`` the
+update) for tests. ``reconstruct`` runs the reference's pixel-basis Landweber loop
+(``optimization_loop_landweber_pixel``, ``:343-420``) for a height-field plate on the
+sm_100a kernels: simulate (refraction + splat), L2 discrepancy against the target image,
+backward to the height field, update.
+"""
+import ctypes
+import math
+from dataclasses import dataclass
+
+import torch
+import torch.nn.functional as F
+
+from . import _lib
+from ._lib import check, lib
+from .splatting import _ptr, _stream
+
+__all__ = ["LandweberParams", "landweber_update", "landweber_update_reference"]
+
+
+@dataclass
+class LandweberParams:
+    tau: float = 1e-1          # tau_pixel
+    alpha: float = 2e-3        # alpha_pixel (shrink threshold = tau * alpha)
+    lower: float = 0.0
+    upper: float = 0.3
+    d1: float = 1.0
+    d2: float = 1.0
+    gamma: float = 0.1
+    radius: int = 2            # volume_radius
+
+    def c_struct(self):
+        p = _lib.PdsLandweber()
+        p.tau = self.tau
+        p.shrink = self.tau * self.alpha
+        p.lower = self.lower
+        p.upper = self.upper
+        p.d1 = self.d1
+        p.d2 = self.d2
+        p.gamma = self.gamma
+        p.radius = int(self.radius)
+        return p
+
+
+def landweber_update(d, grad, mask, params, workspace=None):
+    """In-place fused update of the height-field offset ``d [H, W]`` (float32, device)."""
+    for t, nm in ((d, "d"), (grad, "grad"), (mask, "mask")):
+        if not (t.is_cuda and t.is_contiguous() and t.dtype == torch.float32 and t.shape == d.shape):
+            raise RuntimeError(f"{nm} must be a contiguous float32 CUDA tensor shaped like d")
+    rows, cols = d.shape
+    nbytes = lib().pds_landweber_workspace_bytes(rows, cols)
+    if workspace is None or workspace.numel() < nbytes:
+        workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=d.device)
+    p = params.c_struct()
+    with torch.cuda.device(d.device):
+        check(lib().pds_landweber_update_f32(_ptr(d), _ptr(grad), _ptr(mask), rows, cols,
+                                             ctypes.byref(p), _ptr(workspace), workspace.numel(),
+                                             _stream(d.device)))
+    return d
+
+
+def ext_shrink(x, alpha, a, b):
+    """``shape_from_caustics.py:184-189``."""
+    zeros = torch.zeros_like(x)
+    ones = torch.ones_like(x)
+    return torch.max(torch.min(torch.max(torch.abs(x) - alpha, zeros) * torch.sign(x), b * ones),
+                     a * ones)
+
+
+def vcons_heur(x, d1, d2, mask, gamma, radius):
+    """``shape_from_caustics.py:228-241``."""
+    vx = torch.sum(x)
+    xmean = F.avg_pool2d(x[None, None], 2 * radius + 1, stride=1, padding=radius)[0, 0]
+    if vx <= d1:
+        x = x + mask * xmean * torch.sin(vx / d1 * math.pi) * gamma
+    elif vx >= d2:
+        x = x - mask * xmean * torch.sin((vx / d2 - 1) * math.pi) * gamma
+    return x
+
+
+def landweber_update_reference(d, grad, mask, params):
+    """The reference's update ops (``shape_from_caustics.py:386-398``), out of place."""
+    x = d - params.tau * grad
+    x = mask * ext_shrink(x, params.tau * params.alpha, params.lower, params.upper)
+    return vcons_heur(x, params.d1, params.d2, mask, params.gamma, params.radius)
+
+
+def render_plate(height, scene, px, py, flux, params, shape, max_pixel_radius=20):
+    """Caustic image of the plate (no gradient)."""
+    from .plate import PlateSplat
+    with torch.no_grad():
+        return PlateSplat.apply(height, px, py, flux, params, shape, max_pixel_radius, False)
+
+
+def jitter(H, W, scene, per_texel, generator, device):
+    """Entry points of ``per_texel`` uniformly jittered photons per texel, on the device."""
+    n = H * W * per_texel
+    idx = torch.arange(n, device=device)
+    texel = idx // per_texel
+    iy = (texel // W).float()
+    ix = (texel % W).float()
+    j = torch.rand((2, n), generator=generator, device=device) - 0.5
+    px = (ix + j[0] - (W - 1) / 2.0) * scene.texel
+    py = (iy + j[1] - (H - 1) / 2.0) * scene.texel
+    return px.contiguous(), py.contiguous()
+
+
+def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image=1024,
+                smoothing=4.0, params=None, mask=None, seed=0, keep_plan=False, target=None,
+                log_every=0):
+    """The reference's pixel-basis Landweber loop (``shape_from_caustics.py:343-420``,
+    default options) for a height-field plate, all on the device.
+
+    Each iteration splats ``sims`` simulations of ``per_texel`` freshly jittered photons
+    per texel into one image (the reference's sum over simulations, ``:351-353``), takes the
+    L2 discrepancy ``0.5 |I - T|^2 / |T|^2`` against the target, back-propagates to the
+    height-field offset through the splat and refraction kernels (refracted positions
+    recomputed, not stored) and applies the fused projected update. Returns a dict with the
+    reconstructed offset, the per-iteration discrepancy and height RMSE."""
+    from .plate import PlateSplat, plate_params
+    dev = h_true.device
+    H, W = h_true.shape
+    n = H * W * per_texel * sims
+    du0 = 2.0 * smoothing * math.sqrt(H * W * scene.texel ** 2 / (math.pi * n))
+    pp = plate_params(scene, du0)
+    shape = (1, image, image)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    flux = torch.full((n,), 1.0 / n, device=dev)
+    d_true = h_true - base
+    if target is None:
+        px, py = jitter(H, W, scene, per_texel * sims, g, dev)
+        target = render_plate(h_true, scene, px, py, flux, pp, shape)
+    tnorm2 = float((target * target).sum())
+    if params is None:
+        vol = float(d_true.sum())
+        params = LandweberParams(d1=0.75 * vol, d2=1.25 * vol)
+    if mask is None:
+        mask = torch.ones_like(h_true)
+    d = torch.zeros_like(h_true)
+    ws = None
+    hist = {"discrepancy": [], "rmse": []}
+    for it in range(iterations):
+        px, py = jitter(H, W, scene, per_texel * sims, g, dev)
+        hv = (base + d).requires_grad_(True)
+        img = PlateSplat.apply(hv, px, py, flux, pp, shape, 20, keep_plan)
+        diff = img - target
+        loss = 0.5 * (diff * diff).sum() / tnorm2
+        loss.backward()
+        if ws is None:
+            ws = torch.empty(int(lib().pds_landweber_workspace_bytes(H, W)), dtype=torch.uint8,
+                             device=dev)
+        landweber_update(d, hv.grad, mask, params, ws)
+        if log_every and (it % log_every == 0 or it == iterations - 1):
+            hist["discrepancy"].append((it, float(loss)))
+            hist["rmse"].append((it, float(((d - d_true) ** 2).mean().sqrt())))
+    rmse = float(((d - d_true) ** 2).mean().sqrt())
+    return {"d": d, "rmse": rmse, "history": hist, "target": target, "photons_per_iteration": n}

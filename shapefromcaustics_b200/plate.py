@@ -1,0 +1,120 @@
+"""Height field -> caustic image on the receiver, differentiable in the height field, on the
+fused sm_100a refraction kernels and the splat kernels.
+
+``PlateSplat.apply(height, photons, plate, output_size, max_pixel_radius)`` is the
+refraction-to-receiver step followed by the splat (``model/caustics.py:242-291`` for this
+scene, with ``splat_photons`` ``:233-239`` at its end). The backward runs the splat backward
+and then the refraction backward kernel, which recomputes each photon's path from the height
+field: refracted positions and differentials are never stored, and with
+``keep_plan=False`` neither is the splat's binning, so the memory held between the passes is
+the height field and the photons' entry points (12 bytes per photon).
+
+``photons`` is ``(px, py, flux)`` (``[N]`` each, float32, device) plus an optional channel
+``[N]`` int64; ``plate`` a ``PlateScene`` (``refraction.py``) with ``du0``, the initial
+positional differential length.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check, lib
+from .splatting import SplatPlan, _ptr, _stream
+
+__all__ = ["PlateParams", "plate_params", "refract_forward", "refract_backward", "PlateSplat"]
+
+
+PlateParams = _lib.PdsPlate
+
+
+def plate_params(scene, du0):
+    """``pds_plate`` of a ``PlateScene`` with initial differential length ``du0``."""
+    p = PlateParams()
+    p.texel = scene.texel
+    p.ior = scene.ior
+    p.receiver_distance = scene.receiver_distance
+    p.receiver_half = scene.receiver_half
+    for k in range(3):
+        p.light_dir[k] = scene.light_dir[k]
+    p.du0 = float(du0)
+    return p
+
+
+def _fn(name):
+    return getattr(lib(), name)
+
+
+def _check_f32(t, name):
+    if not (t.is_cuda and t.is_contiguous() and t.dtype == torch.float32):
+        raise RuntimeError(f"{name} must be a contiguous float32 CUDA tensor")
+
+
+def refract_forward(height, px, py, flux, params, channel=None):
+    """Splat inputs ``(Ep, xp, Mp, cp, radius)`` of the photons (``pds_refract_forward_f32``)."""
+    for t, nm in ((height, "height"), (px, "px"), (py, "py"), (flux, "flux")):
+        _check_f32(t, nm)
+    n = px.numel()
+    dev = height.device
+    Ep = torch.empty(n, device=dev)
+    xp = torch.empty((2, n), device=dev)
+    Mp = torch.empty((2, 3, n), device=dev)
+    cp = torch.empty((1, n), dtype=torch.int64, device=dev)
+    radius = torch.empty(n, device=dev)
+    with torch.cuda.device(dev):
+        check(_fn("pds_refract_forward_f32")(
+            _ptr(height), height.shape[0], height.shape[1], ctypes.byref(params), _ptr(px),
+            _ptr(py), _ptr(flux), _ptr(channel) if channel is not None else None, n, _ptr(Ep),
+            _ptr(xp), _ptr(Mp), _ptr(cp), _ptr(radius), _stream(dev)))
+    return Ep, xp, Mp, cp, radius
+
+
+def refract_backward(height, px, py, flux, params, gE, gX, gM, grad_height=None):
+    """Adds d L / d height for splat-input gradients (``pds_refract_backward_f32``)."""
+    n = px.numel()
+    if grad_height is None:
+        grad_height = torch.zeros_like(height)
+    with torch.cuda.device(height.device):
+        check(_fn("pds_refract_backward_f32")(
+            _ptr(height), height.shape[0], height.shape[1], ctypes.byref(params), _ptr(px),
+            _ptr(py), _ptr(flux), n, _ptr(gE.contiguous()), _ptr(gX.contiguous()),
+            _ptr(gM.contiguous()), _ptr(grad_height), _stream(height.device)))
+    return grad_height
+
+
+class PlateSplat(torch.autograd.Function):
+    """Caustic image of a height-field plate; differentiable in the height field."""
+
+    @staticmethod
+    def forward(ctx, height, px, py, flux, params, output_size, max_pixel_radius, keep_plan=True):
+        h = height.detach().contiguous()
+        Ep, xp, Mp, cp, radius = refract_forward(h, px, py, flux, params)
+        plan = SplatPlan(Ep, xp, Mp, cp, radius, output_size, max_pixel_radius)
+        img = plan.forward()
+        ctx.save_for_backward(h, px, py, flux)
+        ctx.params = params
+        ctx.shape = tuple(int(v) for v in output_size)
+        ctx.mpr = int(max_pixel_radius)
+        ctx.plan_ws = plan.ws if keep_plan else None
+        ctx.cfg = plan.cfg
+        return img
+
+    @staticmethod
+    def backward(ctx, grad_img):
+        h, px, py, flux = ctx.saved_tensors
+        # splat inputs are recomputed, not stored
+        Ep, xp, Mp, cp, radius = refract_forward(h, px, py, flux, ctx.params)
+        if ctx.plan_ws is not None:
+            plan = SplatPlan.__new__(SplatPlan)
+            plan.n = Ep.numel()
+            plan.C, plan.H, plan.W = ctx.shape
+            plan.mpr = ctx.mpr
+            plan.cfg = ctx.cfg
+            plan.device = h.device
+            plan.inputs = (Ep, xp, Mp, cp, radius)
+            plan.ws = ctx.plan_ws
+        else:
+            plan = SplatPlan(Ep, xp, Mp, cp, radius, ctx.shape, ctx.mpr, config=ctx.cfg)
+        gE, gX, gM = plan.backward(grad_img.contiguous())
+        gh = refract_backward(h, px, py, flux, ctx.params, gE, gX, gM)
+        ctx.plan_ws = None
+        return gh, None, None, None, None, None, None, None

@@ -1,0 +1,115 @@
+"""Fused refraction-to-receiver kernels (pds_refract_*_f32) against the float64 PyTorch
+refraction chain (itself checked by central finite differences in test_refraction.py), and
+the end-to-end differentiable plate (PlateSplat) against the FP64 chain + FP64 oracle splat.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from shapefromcaustics_b200 import refraction as RF
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def scene_and_photons(n=64, seed=0, smoothing=3.0):
+    scene = RF.PlateScene(texel=0.4, receiver_distance=30.0, receiver_half=14.0)
+    h = RF.height_field_bumps(n, n, seed=seed, bumps=10, base=1.0, amp=(0.0, 0.05),
+                              width=(2.0, 8.0)).float()
+    ph = RF.jittered_photons(n, n, scene, per_texel=4, seed=seed + 1, smoothing=smoothing)
+    du0 = float(ph[2][0, 0])
+    return scene, h, ph, du0
+
+
+def torch_inputs64(h, scene, ph):
+    px, py, Du0, Dv0, flux = (t.double() for t in ph)
+    return RF.receiver_splat_inputs(h.double(), scene, (px.float().double(), py.float().double(),
+                                                        Du0, Dv0, flux.float().double()))
+
+
+def test_refract_forward_matches_float64_chain(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, ph, du0 = scene_and_photons()
+    params = PL.plate_params(scene, du0)
+    px, py, flux = (t.float().cuda() for t in (ph[0], ph[1], ph[4]))
+    Ep, xp, Mp, cp, radius = PL.refract_forward(h.cuda(), px, py, flux, params)
+    rE, rx, rM, rc, rr = torch_inputs64(h, scene, ph)
+    torch.cuda.synchronize()
+    assert rel_l2(xp.cpu(), rx) < 1e-6
+    assert rel_l2(Ep.cpu(), rE) < 1e-4
+    assert rel_l2(Mp.cpu(), rM) < 1e-4
+    assert rel_l2(radius.cpu(), rr) < 1e-4
+    assert torch.equal(cp.cpu(), rc)
+
+
+def test_refract_backward_matches_float64_autograd(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, ph, du0 = scene_and_photons(seed=3)
+    params = PL.plate_params(scene, du0)
+    n = ph[0].numel()
+    g = torch.Generator().manual_seed(0)
+    gE = torch.randn(n, generator=g, dtype=torch.float64)
+    gX = torch.randn((2, n), generator=g, dtype=torch.float64)
+    gM = torch.randn((2, 3, n), generator=g, dtype=torch.float64) * 1e-3
+    gM[:, 2] = 0
+    px, py, flux = (t.float().cuda() for t in (ph[0], ph[1], ph[4]))
+    gh = PL.refract_backward(h.cuda(), px, py, flux, params, gE.float().cuda(), gX.float().cuda(),
+                             gM.float().cuda())
+    hd = h.double().requires_grad_(True)
+    px64, py64, Du0, Dv0, flux64 = (t.double() for t in ph)
+    Ep, xp, Mp, cp, radius = RF.receiver_splat_inputs(hd, scene, (px64, py64, Du0, Dv0, flux64))
+    L = (Ep * gE).sum() + (xp * gX).sum() + (Mp * gM).sum()
+    (ref,) = torch.autograd.grad(L, hd)
+    torch.cuda.synchronize()
+    assert rel_l2(gh.cpu(), ref) < 1e-3
+
+
+def test_plate_splat_end_to_end_gradient(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, ph, du0 = scene_and_photons(seed=5)
+    params = PL.plate_params(scene, du0)
+    shape = (1, 128, 128)
+    G = torch.randn(shape, generator=torch.Generator().manual_seed(1), dtype=torch.float64)
+    px, py, flux = (t.float().cuda() for t in (ph[0], ph[1], ph[4]))
+    for keep in (True, False):
+        hv = h.cuda().requires_grad_(True)
+        img = PL.PlateSplat.apply(hv, px, py, flux, params, shape, 20, keep)
+        (img * G.float().cuda()).sum().backward()
+        # FP64 reference: float64 chain, FP64 oracle splat and backward
+        hd = h.double().requires_grad_(True)
+        Ep, xp, Mp, cp, radius = RF.receiver_splat_inputs(
+            hd, scene, tuple(t.double() for t in ph))
+        a = [t.detach().numpy() for t in (Ep, xp, Mp, cp, radius)]
+        rimg = O.forward(*a, shape, 20)
+        gE, gX, gM = O.backward(G.numpy(), *a, 20)
+        L = (Ep * torch.from_numpy(gE)).sum() + (xp * torch.from_numpy(gX)).sum() + \
+            (Mp * torch.from_numpy(gM)).sum()
+        (ref,) = torch.autograd.grad(L, hd)
+        torch.cuda.synchronize()
+        assert rel_l2(img.detach().cpu(), rimg) < 1e-4
+        assert rel_l2(hv.grad.cpu(), ref) < 1e-3
+
+
+@pytest.mark.parametrize("vol", ["low", "mid", "high"])
+def test_landweber_update_matches_reference_ops(cuda, vol):
+    from shapefromcaustics_b200.landweber import (LandweberParams, landweber_update,
+                                                  landweber_update_reference)
+    g = torch.Generator().manual_seed(3)
+    H, W = 130, 97
+    d = torch.rand((H, W), generator=g) * 0.2
+    grad = torch.randn((H, W), generator=g)
+    mask = (torch.rand((H, W), generator=g) > 0.3).float()
+    s = float((mask * d).sum())
+    d1, d2 = {"low": (2 * s, 3 * s), "mid": (0.5 * s, 3 * s), "high": (0.2 * s, 0.4 * s)}[vol]
+    p = LandweberParams(tau=0.05, alpha=0.1, lower=0.0, upper=0.15, d1=d1, d2=d2, gamma=0.1,
+                        radius=2)
+    ref = landweber_update_reference(d.double(), grad.double(), mask.double(), p)
+    out = landweber_update(d.cuda(), grad.cuda(), mask.cuda(), p)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu(), ref) < 1e-5

@@ -70,7 +70,8 @@ def test_uniform_cluster_512(cuda):
 
 @pytest.mark.parametrize("cfg", [dict(tile=16), dict(tile=64), dict(chunk=256),
                                  dict(class_bits=2), dict(class_bits=4, chunk=4096),
-                                 dict(tile=32, apron_max=3)])
+                                 dict(tile=32, apron_max=3), dict(walk=1),
+                                 dict(walk=1, tile=16, class_bits=3)])
 def test_tuning_variants(cuda, cfg):
     ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
     assert_parity(ph, (1, 256, 256), 20, cfg=cfg)
@@ -219,6 +220,33 @@ def test_batched_uneven_simulations_match_per_simulation_oracle(cuda):
             assert rel_l2(gX[:, sl].cpu().numpy(), rX) <= GRAD_TOL
             assert rel_l2(gM[:, :, sl].cpu().numpy(), rM) <= GRAD_TOL
         off += n
+
+
+def test_simulations_sharing_an_image_are_summed(cuda):
+    # the reference's caller sums its simulations' images (shape_from_caustics.py:351-353)
+    from shapefromcaustics_b200 import _lib
+    from shapefromcaustics_b200.splatting import BatchedSplat
+    specs = [(5000, (1, 96, 96)), (7000, (1, 96, 96)), (3000, (1, 96, 96))]
+    parts = [S.uniform_cluster_photons(n, 96, 96, seed=200 + s) for s, (n, _) in enumerate(specs)]
+    cat = [torch.cat([p[k] for p in parts], dim=-1).contiguous().cuda() for k in range(5)]
+    b = BatchedSplat(specs, 20, "cuda:0")
+    # point every simulation at image 0
+    t = (_lib.PdsSim * 3).from_buffer_copy(bytes(b.table_dev.cpu().numpy()))
+    for k in range(3):
+        t[k].image_offset = 0
+    b.table_dev = torch.frombuffer(bytearray(bytes(t)), dtype=torch.uint8).cuda()
+    b.image_elems = 96 * 96
+    b.plan(*cat)
+    img = b.forward()
+    G = S.upstream_grad((1, 96, 96), seed=9)
+    gE, gX, gM = b.backward(G.reshape(-1).cuda())
+    torch.cuda.synchronize()
+    allp = [torch.cat([p[k] for p in parts], dim=-1) for k in range(5)]
+    rimg, (rE, rX, rM) = run_oracle(allp, (1, 96, 96), 20, G)
+    assert rel_l2(img.view(1, 96, 96).cpu().numpy(), rimg) <= FWD_TOL
+    assert rel_l2(gE.cpu().numpy(), rE) <= GRAD_TOL
+    assert rel_l2(gX.cpu().numpy(), rX) <= GRAD_TOL
+    assert rel_l2(gM.cpu().numpy(), rM) <= GRAD_TOL
 
 
 def test_batched_graph_replay_equals_eager(cuda):
