@@ -100,6 +100,15 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
 
 // ------------------------------------------------------------------ tiles --------------
 
+// Photon counts of the plan, clamped to the photon count so that a workspace without a plan
+// cannot send the kernels outside their arrays.
+__device__ __forceinline__ int64_t tile_count(const TileArgs& a) {
+    return min(int64_t(a.counters[0]), a.ph.n);
+}
+__device__ __forceinline__ int64_t wide_count(const TileArgs& a) {
+    return min(int64_t(a.counters[1]), a.ph.n - tile_count(a));
+}
+
 struct TileInfo {
     int64_t img_off;  // element offset of the (simulation, channel) image plane
     int32_t W, H;
@@ -220,7 +229,7 @@ __global__ __launch_bounds__(NT) void fwd_tiles_kernel(TileArgs a) {
         sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
     }
     __syncthreads();
-    const int64_t n_tile = a.counters[0];
+    const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
@@ -236,13 +245,18 @@ __global__ __launch_bounds__(NT) void fwd_tiles_kernel(TileArgs a) {
                 r = a.recs[a.sidx[i]];
             }
             const int64_t bend = min(base + NT, p1);
-            while (true) {
+            // The batch's keys are sorted, so its segments are consecutive thread ranges;
+            // `done` counts the threads of the segments handled so far. Each pass of the
+            // loop handles one segment (the first pass may find none when the previous
+            // batch's segment does not continue here), so NT + 1 passes always suffice.
+            int done = 0;
+            for (int pass = 0; pass <= NT; ++pass) {
                 const bool mine = have && key == cur;
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
                 if (mine) deposit(r, ti, sw, cfg.spans, acc, x0, x1, y0, y1);
                 bbox_publish(sb, x0, x1, y0, y1);
-                const int cnt = __syncthreads_count(mine);
-                const int64_t nxt = base + cnt;
+                done += __syncthreads_count(mine);
+                const int64_t nxt = base + done;
                 if (nxt >= bend) break;
                 flush_tile(acc, sw, ti, a.out, sb);
                 cur = a.skeys[nxt] >> cb;
@@ -331,7 +345,7 @@ __global__ __launch_bounds__(NT) void bwd_tiles_kernel(TileArgs a) {
     extern __shared__ float tg[];
     const Cfg cfg = a.cfg;
     const int sw = cfg.sw, cb = cfg.class_bits;
-    const int64_t n_tile = a.counters[0];
+    const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
@@ -349,7 +363,9 @@ __global__ __launch_bounds__(NT) void bwd_tiles_kernel(TileArgs a) {
                 r = a.recs[rid];
             }
             const int64_t bend = min(base + NT, p1);
-            while (true) {
+            // consecutive segments of the sorted batch, as in fwd_tiles_kernel
+            int done = 0;
+            for (int pass = 0; pass <= NT; ++pass) {
                 if (cur != loaded) {
                     __syncthreads();
                     load_region(tg, sw, ti, a.grad);
@@ -358,8 +374,8 @@ __global__ __launch_bounds__(NT) void bwd_tiles_kernel(TileArgs a) {
                 }
                 const bool mine = have && key == cur;
                 if (mine) gather(r, ti, sw, cfg.spans, tg, rid, a);
-                const int cnt = __syncthreads_count(mine);
-                const int64_t nxt = base + cnt;
+                done += __syncthreads_count(mine);
+                const int64_t nxt = base + done;
                 if (nxt >= bend) break;
                 cur = a.skeys[nxt] >> cb;
                 ti = decode_tile(a.sims, cur, cfg);
@@ -411,7 +427,7 @@ __device__ __forceinline__ bool direct_setup(const TileArgs& a, uint32_t rid, Di
 }
 
 __global__ __launch_bounds__(256) void tail_fwd_kernel(TileArgs a) {
-    const int64_t n_tile = a.counters[0], n_big = a.counters[1];
+    const int64_t n_tile = tile_count(a), n_big = wide_count(a);
     const int lane = threadIdx.x & 31;
     const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
     for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_big;
@@ -440,7 +456,7 @@ __global__ __launch_bounds__(256) void tail_fwd_kernel(TileArgs a) {
 
 __global__ __launch_bounds__(256) void tail_bwd_kernel(TileArgs a) {
     const int64_t n = a.ph.n;
-    const int64_t n_tile = a.counters[0], n_big = a.counters[1];
+    const int64_t n_tile = tile_count(a), n_big = wide_count(a);
     const int lane = threadIdx.x & 31;
     const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
     for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_big;
