@@ -174,6 +174,10 @@ def workload(name, rank, device):
         specs = [(2 ** 20, (1, 512, 512))]
         photons = S.uniform_cluster_photons(2 ** 20, 512, 512, seed=seed, device=device)
         desc = "2^20 photons, 512^2, uniform+cluster, s ~ logU[0.5,4] px, mpr 20, fp32"
+    elif name == "medium":
+        specs = [(2 ** 23, (1, 1024, 1024))]
+        photons = S.uniform_cluster_photons(2 ** 23, 1024, 1024, seed=seed, device=device)
+        desc = "2^23 photons, 1024^2, uniform+cluster, s ~ logU[0.5,4] px, mpr 20, fp32"
     elif name == "contention":
         specs = [(2 ** 26, (1, 2048, 2048))]
         photons = S.caustic_curve_photons(2 ** 26, 2048, 2048, seed=seed, device=device)
@@ -299,6 +303,12 @@ def run_ours(args, rank, world, device):
             phases["forward"].append(e[1].elapsed_time(e[2]))
             phases["backward"].append(e[2].elapsed_time(e[3]))
     ph_ms = {k: statistics.median(v) for k, v in phases.items()}
+
+    if args.lean:
+        clocks.stop()
+        return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "phase_ms": ph_ms, "lean": True, "clocks": clocks.summary()}
 
     # ---- plain: one plan + forward + backward per simulation, like the reference's loop ----
     per_sim = split_photons(specs, photons)
@@ -553,14 +563,125 @@ def run_reference_gpu(args, rank, world, device):
                        "mode": "plain: pds_forward + pds_backward per simulation"}}
 
 
+# ------------------------------------------------------------------ Landweber workloads --
+
+def plate_setup(n_field, image, per_texel, device, seed=0, texel=0.1, dist=50.0):
+    """Height-field plate of the Landweber workloads: a 1 mm base plus 32 Gaussian bumps
+    (amplitude U[0, 50] um, width U[4, 24] texels), collimated light at normal incidence,
+    n = 1.5, receiver 50 mm below; photons jittered per texel."""
+    from shapefromcaustics_b200 import refraction as RF
+    half = 0.5 * n_field * texel * 1.1
+    scene = RF.PlateScene(texel=texel, ior=1.5, receiver_distance=dist, receiver_half=half)
+    h = RF.height_field_bumps(n_field, n_field, seed=seed, bumps=32, base=1.0,
+                              amp=(0.0, 0.05), width=(4.0, 24.0)).float().to(device)
+    t = RF.height_field_bumps(n_field, n_field, seed=seed + 1, bumps=32, base=1.0,
+                              amp=(0.0, 0.05), width=(4.0, 24.0)).float().to(device)
+    return scene, h, t
+
+
+def run_landweber_step(args, rank, world, device):
+    """One Landweber iteration on a 256^2 field, 4 photons per texel (262,144), 512^2
+    image: refraction + splat forward, L2 discrepancy against a target rendered from a second
+    field, backward through splat and refraction, fused projected update."""
+    from shapefromcaustics_b200.landweber import LandweberParams, jitter, landweber_update
+    from shapefromcaustics_b200.plate import PlateSplat, plate_params
+    torch.cuda.set_device(device)
+    nf, img, pt = 256, 512, 4
+    scene, h_true, h_tgt = plate_setup(nf, img, pt, device)
+    n = nf * nf * pt
+    du0 = 2.0 * 4.0 * math.sqrt(nf * nf * scene.texel ** 2 / (math.pi * n))
+    pp = plate_params(scene, du0)
+    g = torch.Generator(device=device)
+    g.manual_seed(rank)
+    px, py = jitter(nf, nf, scene, pt, g, device)
+    flux = torch.full((n,), 1.0 / n, device=device)
+    shape = (1, img, img)
+    with torch.no_grad():
+        target = PlateSplat.apply(h_tgt, px, py, flux, pp, shape, MPR, False)
+    base = 1.0
+    d = (h_true - base).clone()
+    mask = torch.ones_like(d)
+    vol = float(d.sum())
+    params = LandweberParams(d1=0.75 * vol, d2=1.25 * vol)
+    tn = float((target * target).sum())
+    ws = torch.empty(1 << 22, dtype=torch.uint8, device=device)
+
+    def step():
+        hv = (base + d).requires_grad_(True)
+        im = PlateSplat.apply(hv, px, py, flux, pp, shape, MPR, True)
+        loss = 0.5 * ((im - target) ** 2).sum() / tn
+        loss.backward()
+        landweber_update(d, hv.grad, mask, params, ws)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, device)
+    its = sum_over_ranks(1.0, world, device) / (ms / 1e3)
+    return {"metric": "Landweber it/s", "value": its, "unit": "it/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "landweber256: 256^2 height field (1 mm + 32 bumps), 4 "
+                                   "jittered photons/texel (262144), n=1.5, receiver 50 mm, "
+                                   "512^2 image, L2 vs second field; refraction + splat "
+                                   "fwd/bwd + fused update", "photons": n}}
+
+
+def run_reconstruction(args, rank, world, device):
+    """Full reconstruction: 1024^2 field, 16 simulations x 4 photons per texel (2^22 each,
+    67M per iteration) into a 1024^2 image, Landweber iterations with the refracted photon
+    positions recomputed in the backward; final height RMSE and peak HBM."""
+    from shapefromcaustics_b200.landweber import reconstruct
+    torch.cuda.set_device(device)
+    nf = 1024
+    scene, h_true, _ = plate_setup(nf, nf, 4, device, seed=7)
+    torch.cuda.reset_peak_memory_stats(device)
+    iters = args.steps
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    res = reconstruct(h_true, 1.0, scene, iterations=iters, sims=16, per_texel=4, image=nf,
+                      smoothing=4.0, seed=rank, keep_plan=False, log_every=max(iters // 10, 1))
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    peak = torch.cuda.max_memory_allocated(device)
+    d_true = h_true - 1.0
+    return {"metric": "Landweber it/s", "value": iters / (ms / 1e3), "unit": "it/s",
+            "n_gpus": world, "steps": iters, "warmup": 0, "ms_per_step": ms / iters,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "recon1024: 1024^2 field, 16 sims x 2^22 photons per "
+                                   "iteration into 1024^2, positions recomputed in backward",
+                       "photons_per_iteration": res["photons_per_iteration"]},
+            "final_height_rmse_mm": res["rmse"],
+            "initial_height_rmse_mm": float((d_true ** 2).mean().sqrt()),
+            "rmse_history": res["history"]["rmse"],
+            "discrepancy_history": res["history"]["discrepancy"],
+            "peak_hbm_bytes": peak}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
-    ap.add_argument("--workload", default="batch64", choices=["batch64", "uniform1m", "contention"])
+    ap.add_argument("--workload", default="batch64",
+                    choices=["batch64", "uniform1m", "medium", "contention", "landweber256",
+                             "recon1024"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lean", action="store_true",
+                    help="timed steps and phase timings only (for profiler runs)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-sample", type=float, default=2 ** 21)
     args = ap.parse_args()
@@ -585,6 +706,10 @@ def main():
                                              device_id=device)
     if args.impl == "reference-gpu":
         res = run_reference_gpu(args, rank, world, device)
+    elif args.workload == "landweber256":
+        res = run_landweber_step(args, rank, world, device)
+    elif args.workload == "recon1024":
+        res = run_reconstruction(args, rank, world, device)
     else:
         res = run_ours(args, rank, world, device)
     if world > 1:

@@ -1,0 +1,81 @@
+"""Autotuner for the splat kernels' launch configuration.
+
+Times candidate ``pds_config`` values (screen-tile edge, photons per CTA work item,
+footprint-class sort bits, pixel walk) on the caller's actual workload with CUDA events, and
+keeps the fastest per workload signature (photon count and image sizes, bucketed). The
+reference has a single fixed launch shape (512 threads per photon block,
+``photon_differentials.cu:120``); here the best tile and chunk depend on footprint sizes and
+photon density, so they are measured rather than fixed.
+"""
+import itertools
+import math
+
+import torch
+
+from . import _lib
+
+__all__ = ["CANDIDATES", "signature", "tune_batch", "cached"]
+
+CANDIDATES = [dict(tile=t, chunk=c, class_bits=b, walk=w)
+              for t, c, b, w in itertools.product((16, 32, 64), (1024, 2048, 4096), (0, 2), (2,))]
+
+_cache = {}
+
+
+def signature(specs, max_pixel_radius):
+    """Bucketed description of a workload: log2 of the photon count, the image sizes."""
+    n = sum(n for n, _ in specs)
+    sizes = tuple(sorted({tuple(int(v) for v in shape) for _, shape in specs}))
+    return (int(math.log2(max(n, 1))), sizes, int(max_pixel_radius), len(specs) > 1)
+
+
+def cached(specs, max_pixel_radius):
+    return _cache.get(signature(specs, max_pixel_radius))
+
+
+def _time_step(batch, photons, out, gflat, grads, reps, stream):
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        batch.plan(*photons)
+        batch.forward(out)
+        batch.backward(gflat, grads)
+        ev0.record(stream)
+        for _ in range(reps):
+            batch.plan(*photons)
+            batch.forward(out)
+            batch.backward(gflat, grads)
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / reps
+
+
+def tune_batch(specs, photons, gflat, max_pixel_radius, device, candidates=None, reps=3,
+               verbose=False):
+    """Times every candidate on ``BatchedSplat(specs)`` with the given photons and upstream
+    gradient; returns ``(best_config_dict, {config_key: ms})`` and caches the winner."""
+    from .splatting import BatchedSplat
+    candidates = candidates or CANDIDATES
+    stream = torch.cuda.Stream(device)
+    results = {}
+    best, best_ms = None, float("inf")
+    grads = tuple(torch.empty_like(t) for t in photons[:3])
+    out = None
+    for c in candidates:
+        cfg = _lib.config(**c)
+        try:
+            batch = BatchedSplat(specs, max_pixel_radius, device, config=cfg)
+        except _lib.PdsError:
+            continue
+        if out is None:
+            out = torch.empty(batch.image_elems, device=device)
+        ms = _time_step(batch, photons, out, gflat, grads, reps, stream)
+        key = tuple(sorted(c.items()))
+        results[key] = ms
+        if verbose:
+            print(f"autotune {c}: {ms:.3f} ms")
+        if ms < best_ms:
+            best, best_ms = c, ms
+        del batch
+    _cache[signature(specs, max_pixel_radius)] = best
+    return best, results
