@@ -206,6 +206,22 @@ int pds_landweber_update_f32(float* d, const float* grad, const float* mask, int
                              int64_t cols, const pds_landweber* params, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of pds_landweber_update_f32. It has no counterpart in the
+ * reference. It is for callers that cannot allocate device memory: code whose device memory
+ * is owned by another allocator (a framework's caching allocator that must not be bypassed),
+ * or a fixed-memory loop that may not allocate after start-up. It takes no workspace: its
+ * scratch is a static device array of this library, 4 MiB + 4 KiB, present on every GPU that
+ * loads the library until the process exits, so fields are limited to rows * cols <=
+ * 1048576 (1024 x 1024); larger fields return PDS_ERR_UNSUPPORTED. The first call on a
+ * device looks up that device's scratch address (a CUDA runtime query, no allocation); make
+ * that first call before any stream capture. All calls share the one scratch array, which
+ * keeps the previous call's contents (every byte this update reads there is written first in
+ * the same call), so calls that overlap on the GPU, from several streams or threads at once,
+ * race and give wrong results: serialise them. */
+int pds_landweber_update_noalloc_f32(float* d, const float* grad, const float* mask,
+                                     int64_t rows, int64_t cols, const pds_landweber* params,
+                                     void* stream);
+
 /* ---- device radix sort (exposed for its bit-exactness tests) ----------------------- */
 /* Stable ascending sort of keys[n] (only the low key_bits bits are compared) carrying the
  * original index: perm_out[k] = index of the k-th smallest key, keys_out the sorted keys. */

@@ -514,6 +514,34 @@ int pds_landweber_update_f32(float* d, const float* grad, const float* mask, int
     return PDS_OK;
 }
 
+int pds_landweber_update_noalloc_f32(float* d, const float* grad, const float* mask,
+                                     int64_t rows, int64_t cols, const pds_landweber* p,
+                                     void* stream) {
+    if (!p) return fail(PDS_ERR_INVALID_ARGUMENT, "null Landweber parameters");
+    if (rows < 1 || cols < 1) return fail(PDS_ERR_INVALID_ARGUMENT, "empty height field");
+    if (!d || !grad || !mask) return fail(PDS_ERR_INVALID_ARGUMENT, "null height-field array");
+    if (p->radius < 0 || p->radius > 64)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "volume radius outside [0, 64]");
+    if (!(p->d1 != 0.f) || !(p->d2 != 0.f))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "volume bounds d1, d2 must be nonzero");
+    const int64_t maxpx = pds::landweber_noalloc_max_pixels();
+    if (rows > maxpx || cols > maxpx || rows * cols > maxpx)
+        return fail(PDS_ERR_UNSUPPORTED,
+                    "pds_landweber_update_noalloc_f32: field of " + std::to_string(rows) + " x " +
+                        std::to_string(cols) + " exceeds its static scratch of " +
+                        std::to_string(maxpx) + " pixels; use pds_landweber_update_f32");
+    void* scratch = nullptr;
+    cudaError_t e = pds::landweber_noalloc_scratch(&scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "noalloc scratch address (cudaGetSymbolAddress)");
+    float* t = static_cast<float*>(scratch);
+    float* partial = reinterpret_cast<float*>(static_cast<char*>(scratch) +
+                                              size_t(maxpx) * sizeof(float));
+    e = pds::launch_landweber(d, grad, mask, rows, cols, *p, t, partial,
+                              static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "landweber kernels (noalloc)");
+    return PDS_OK;
+}
+
 size_t pds_sort_workspace_bytes(int64_t n) {
     const size_t nn = size_t(n > 0 ? n : 1);
     return 2 * pds::align_up(nn * 4, 256) + pds::sort_aux_bytes(n);

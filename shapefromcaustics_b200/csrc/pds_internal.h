@@ -31,5 +31,7 @@ size_t landweber_scratch_bytes(int64_t n);
 cudaError_t launch_landweber(float* d, const float* g, const float* mask, int64_t rows,
                              int64_t cols, const pds_landweber& p, float* t, float* partial,
                              cudaStream_t st);
+int64_t landweber_noalloc_max_pixels();
+cudaError_t landweber_noalloc_scratch(void** out);
 
 }  // namespace pds

@@ -12,6 +12,7 @@
 // the volume heuristic with the box mean of the scratch image. The reference's volume test
 // is a host-side branch on a device scalar; here it stays on the device.
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "../../include/pds_b200.h"
@@ -128,6 +129,39 @@ cudaError_t launch_landweber(float* d, const float* g, const float* mask, int64_
     if (e != cudaSuccess) return e;
     lw_volume_kernel<<<nb, kThreads, 0, st>>>(t, mask, rows, cols, p, partial, nb, d);
     return cudaGetLastError();
+}
+
+// ---- the allocation-free variant -------------------------------------------------------
+// Scratch of pds_landweber_update_noalloc_f32: the shrunk image (up to kNoAllocMaxPixels
+// floats) followed by the per-block partial sums (at most 1024 floats, see lw_blocks).
+// Every GPU that loads this library holds it (4 MiB + 4 KiB) until the process exits.
+constexpr int64_t kNoAllocMaxPixels = int64_t(1) << 20;  // 1024 x 1024
+constexpr size_t kNoAllocImageBytes = size_t(kNoAllocMaxPixels) * sizeof(float);
+constexpr size_t kNoAllocBytes = kNoAllocImageBytes + 1024 * sizeof(float);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+int64_t landweber_noalloc_max_pixels() { return kNoAllocMaxPixels; }
+
+// Device address of the scratch on the current device. In host code the symbol is only a
+// host-side stand-in, so the address is looked up once per device (with that device
+// current) and cached.
+cudaError_t landweber_noalloc_scratch(void** out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return cudaSuccess;
 }
 
 }  // namespace pds
