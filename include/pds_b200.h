@@ -44,15 +44,19 @@ extern "C" {
 
 /* Kernel tuning. A NULL pointer or a zero field selects the default. */
 typedef struct pds_config {
-    int32_t tile;       /* screen-tile edge in pixels: 16, 32 or 64 (default 32) */
+    int32_t tile;       /* screen-tile edge in pixels: 16, 32 or 64 (default 64) */
     int32_t chunk;      /* sorted photons per CTA work item, multiple of 256 (default 2048) */
-    int32_t class_bits; /* footprint-size bits appended to the sort key, 0..4 (default 0) */
+    int32_t class_bits; /* footprint-size bits appended to the sort key (photons of a tile
+                           are then grouped by footprint size): 1..4, or -1 for none
+                           (default 3) */
     int32_t apron_max;  /* largest footprint radius (px) the tile path holds (default 32);
                            larger footprints take the direct path */
     int32_t walk;       /* pixels visited per photon: 1 = the reference's whole box,
                            2 = only the rows / row spans that can hold the kernel's support
                            (same result: pixels outside the support add exactly zero);
-                           default 2 */
+                           default 1 */
+    int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2 (more
+                           registers per thread) or 3 (more warps); default 3 */
 } pds_config;
 
 /* One simulation of a batch. The caller fills photon_begin, n_photons, image_offset,

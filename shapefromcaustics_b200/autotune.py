@@ -16,8 +16,9 @@ from . import _lib
 
 __all__ = ["CANDIDATES", "signature", "tune_batch", "cached"]
 
-CANDIDATES = [dict(tile=t, chunk=c, class_bits=b, walk=w)
-              for t, c, b, w in itertools.product((16, 32, 64), (1024, 2048, 4096), (0, 2), (2,))]
+CANDIDATES = [dict(tile=t, chunk=c, class_bits=b, walk=w, min_blocks=m)
+              for t, c, b, w, m in itertools.product((32, 64), (1024, 4096), (-1, 3), (1, 2),
+                                                     (2, 3))]
 
 _cache = {}
 

@@ -5,7 +5,7 @@
 // 2x3 matrices, one channel row), lays the workspace out, and enqueues
 //   plan:     counters reset, plan_kernel, radix sort
 //   forward:  output reset, fwd_tiles_kernel, tail_fwd_kernel
-//   backward: grad_Mp column-2 reset, bwd_tiles_kernel, tail_bwd_kernel
+//   backward: bwd_tiles_kernel, tail_bwd_kernel, grad_scatter_kernel
 // on the caller's stream. It allocates nothing and never synchronises. Failures return a
 // PDS_ERR_* code and leave a message for pds_last_error() (the reference raises through
 // TORCH_CHECK and does not check its launches, photon_differentials.cu:125, :234).
@@ -46,11 +46,15 @@ struct Resolved {
 };
 
 int resolve_cfg(const pds_config* in, pds_config& out) {
-    out.tile = (in && in->tile) ? in->tile : 32;
+    out.tile = (in && in->tile) ? in->tile : 64;
     out.chunk = (in && in->chunk) ? in->chunk : 2048;
-    out.class_bits = in ? in->class_bits : 0;
+    out.class_bits = (in && in->class_bits) ? in->class_bits : 3;
+    if (out.class_bits == -1) out.class_bits = 0;
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
-    out.walk = (in && in->walk) ? in->walk : 2;
+    out.walk = (in && in->walk) ? in->walk : 1;
+    out.min_blocks = (in && in->min_blocks) ? in->min_blocks : 3;
+    if (out.min_blocks != 2 && out.min_blocks != 3)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.min_blocks must be 2 or 3");
     if (out.walk != 1 && out.walk != 2)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.walk must be 1 (box) or 2 (spans)");
     if (out.tile != 16 && out.tile != 32 && out.tile != 64)
@@ -59,7 +63,7 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.chunk must be a multiple of 256 in [256, 1048576]");
     if (out.class_bits < 0 || out.class_bits > 4)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be in [0, 4]");
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be -1 or in [1, 4]");
     if (out.apron_max < 1 || out.apron_max > 63 || out.tile + 2 * out.apron_max > 255)
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.apron_max must be in [1, 63] with tile + 2*apron_max <= 255");
@@ -81,6 +85,7 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     r.cfg.apron = mpr < 0 ? 0 : (mpr < c.apron_max ? mpr : c.apron_max);
     r.cfg.sw = c.tile + 2 * r.cfg.apron;
     r.cfg.spans = c.walk == 2 ? 1 : 0;
+    r.cfg.min_blocks = c.min_blocks;
     r.key_big = uint32_t(uint64_t(n_tiles) << c.class_bits);
     r.key_invalid = uint32_t(inv);
     r.key_bits = bit_length(inv);
@@ -88,7 +93,7 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
 }
 
 struct Layout {
-    size_t counters, k0, k1, v0, v1, recs, aux, total;
+    size_t counters, k0, k1, v0, v1, recs, stage, aux, total;
 };
 
 Layout make_layout(int64_t n) {
@@ -101,6 +106,7 @@ Layout make_layout(int64_t n) {
     L.v0 = off; off += pds::align_up(nn * 4, 256);
     L.v1 = off; off += pds::align_up(nn * 4, 256);
     L.recs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
+    L.stage = off; off += pds::align_up(nn * sizeof(pds::GradRec), 256);
     L.aux = off; off += pds::sort_aux_bytes(n);
     L.total = off;
     return L;
@@ -110,6 +116,7 @@ struct Bufs {
     uint32_t* counters;
     uint32_t *k0, *k1, *v0, *v1;
     pds::Rec* recs;
+    pds::GradRec* stage;
     void* aux;
 };
 
@@ -122,6 +129,7 @@ Bufs bufs(void* ws, const Layout& L) {
     r.v0 = reinterpret_cast<uint32_t*>(b + L.v0);
     r.v1 = reinterpret_cast<uint32_t*>(b + L.v1);
     r.recs = reinterpret_cast<pds::Rec*>(b + L.recs);
+    r.stage = reinterpret_cast<pds::GradRec*>(b + L.stage);
     r.aux = b + L.aux;
     return r;
 }
@@ -242,6 +250,7 @@ int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.cfg = r.cfg;
     sorted_bufs(b, r.key_bits, &a.skeys, &a.sidx);
     a.recs = b.recs;
+    a.stage = b.stage;
     a.counters = b.counters;
     return PDS_OK;
 }
@@ -275,11 +284,7 @@ int backward_impl(const float* grad, const pds::Photons& ph, const pds::SimTable
     a.gE = gE;
     a.gX = gX;
     a.gM = gM;
-    // grad_Mp[0][2] and grad_Mp[1][2] multiply a zero in the reference (:198-205, :215, :218)
-    cudaError_t e = cudaMemsetAsync(gM + 2 * ph.n, 0, size_t(ph.n) * sizeof(float), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(gM + 5 * ph.n, 0, size_t(ph.n) * sizeof(float), s);
-    if (e != cudaSuccess) return cuda_fail(e, "backward: grad_Mp column-2 reset");
-    e = pds::launch_backward(a, s);
+    cudaError_t e = pds::launch_backward(a, s);
     if (e != cudaSuccess) return cuda_fail(e, "bwd_tiles_kernel");
     return PDS_OK;
 }

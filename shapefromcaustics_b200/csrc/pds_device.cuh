@@ -50,6 +50,13 @@ __device__ __forceinline__ int rec_rx(uint32_t p) { return int((p >> 10) & 0x3Fu
 __device__ __forceinline__ int rec_ry(uint32_t p) { return int((p >> 4) & 0x3Fu); }
 __device__ __forceinline__ uint32_t rec_flags(uint32_t p) { return p & 0xFu; }
 
+// Per-photon gradient record of the backward, written in photon order as one 32-byte sector
+// (a whole-sector store, no read-for-ownership) and spread into the reference's SoA outputs
+// by a coalesced pass.
+struct __align__(16) GradRec {
+    float gE, gx0, gx1, g00, g01, g10, g11, pad;
+};
+
 // Resolved launch configuration (host fills it from pds_config).
 struct Cfg {
     int32_t tile;
@@ -58,6 +65,7 @@ struct Cfg {
     int32_t apron;       // min(max_pixel_radius, apron_max), >= 0
     int32_t sw;          // tile + 2 * apron: edge of the shared accumulator
     int32_t spans;       // 1: walk only the support's rows / row spans; 0: the whole box
+    int32_t min_blocks;  // resident CTAs per SM the tile kernels' register budget targets
 };
 
 // Simulation table: either a device array or one inline descriptor.
@@ -120,7 +128,14 @@ __device__ __forceinline__ Footprint make_footprint(float x, float y, float r, i
     f.ry = min(ry, mpr);
     f.px_c = __double2int_rz((0.5 * double(x) + 0.5) * w);
     f.py_c = __double2int_rz((0.5 * double(y) + 0.5) * h);
-    f.ellipse_all = (f.rx < 0 || f.ry < 0) ? true : ellipse_ok(f.rx, f.ry, w, h);
+    // The corner test sums two terms of at most (2 rx / w)^2 and (2 ry / h)^2; with
+    // 4 rx <= w and 4 ry <= h it is at most 1/2 and passes without evaluating it.
+    if (f.rx < 0 || f.ry < 0)
+        f.ellipse_all = true;
+    else if (int64_t(f.rx) * 4 <= int64_t(W) && int64_t(f.ry) * 4 <= int64_t(H))
+        f.ellipse_all = true;
+    else
+        f.ellipse_all = ellipse_ok(f.rx, f.ry, w, h);
     return f;
 }
 
@@ -193,7 +208,16 @@ __device__ __forceinline__ bool support_cols(const Support& g, float dy, float d
 
 // delta = (2 p_c / w - 1) - x in double, rounded once to float.
 __device__ __forceinline__ float corner_offset(int32_t p_c, int32_t W, float x) {
-    return float(2.0 * double(p_c) / double(W) - 1.0 - double(x));
+    return float(double(p_c) * (2.0 / double(W)) - 1.0 - double(x));
+}
+
+// Predicated shared-memory add without a branch (the compiler otherwise branches around
+// the atomic per pixel).
+__device__ __forceinline__ void red_shared_add_if(bool p, const float* addr, float v) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(addr));
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q red.shared.add.f32 [%0], %1;\n\t}"
+        :: "r"(a), "f"(v), "r"(int(p)) : "memory");
 }
 
 }  // namespace pds

@@ -7,7 +7,9 @@
 //              coalesced kernels (group partials, one-CTA top scan with digit bases, group
 //              down-sweep), yielding each block's first output slot per digit
 //   downsweep  stable rank inside the block (warp-striped order: warp w owns a contiguous
-//              512-key range, ranked per 32-key step with __match_any_sync), then scatter
+//              512-key range, ranked per 32-key step with __match_any_sync), the block's
+//              keys staged in shared memory in digit order, then each digit's run written
+//              contiguously (coalesced stores instead of one scattered store per key)
 // Digits are at most 8 bits; the number of passes is ceil(key_bits / 8) with the bits spread
 // evenly, so a 9-bit key space costs two 5/4-bit passes and a 16-bit one two 8-bit passes.
 #include <cstdint>
@@ -113,6 +115,9 @@ __global__ __launch_bounds__(kThreads) void sort_downsweep(
     uint32_t* __restrict__ vals_out) {
     __shared__ uint32_t wcnt[kWarps][256];
     __shared__ uint32_t boff[256];
+    __shared__ uint32_t dstart[256];
+    __shared__ uint32_t skey[kTileKeys];
+    __shared__ uint32_t sval[kTileKeys];
     const int radix = 1 << bits;
     const uint32_t mask = uint32_t(radix - 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -121,7 +126,8 @@ __global__ __launch_bounds__(kThreads) void sort_downsweep(
         boff[d] = hist[int64_t(blockIdx.x) * radix + d];
     __syncthreads();
 
-    const int64_t base = int64_t(blockIdx.x) * kTileKeys + int64_t(warp) * (32 * kIpt);
+    const int64_t block0 = int64_t(blockIdx.x) * kTileKeys;
+    const int64_t base = block0 + int64_t(warp) * (32 * kIpt);
     const uint32_t lt = lanemask_lt();
     uint32_t k[kIpt], v[kIpt], rank[kIpt];
 #pragma unroll
@@ -140,25 +146,48 @@ __global__ __launch_bounds__(kThreads) void sort_downsweep(
         __syncwarp();
     }
     __syncthreads();
+    // per digit: exclusive offsets of the warps, and the block's total
+    uint32_t total = 0;
     if (threadIdx.x < radix) {
-        uint32_t run = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
             const uint32_t t = wcnt[w][threadIdx.x];
-            wcnt[w][threadIdx.x] = run;
-            run += t;
+            wcnt[w][threadIdx.x] = total;
+            total += t;
         }
     }
+    // exclusive scan of the block's digit totals (Hillis-Steele over 256 entries)
+    dstart[threadIdx.x] = total;
     __syncthreads();
+    for (int off = 1; off < kThreads; off <<= 1) {
+        const uint32_t add = threadIdx.x >= off ? dstart[threadIdx.x - off] : 0u;
+        __syncthreads();
+        dstart[threadIdx.x] += add;
+        __syncthreads();
+    }
+    const uint32_t incl = dstart[threadIdx.x];
+    __syncthreads();
+    dstart[threadIdx.x] = incl - total;
+    __syncthreads();
+    // stage the block's keys in digit order, then write each digit's run contiguously
 #pragma unroll
     for (int j = 0; j < kIpt; ++j) {
         const int64_t i = base + j * 32 + lane;
         if (i < n) {
             const uint32_t d = (k[j] >> shift) & mask;
-            const uint32_t pos = boff[d] + wcnt[warp][d] + rank[j];
-            keys_out[pos] = k[j];
-            vals_out[pos] = v[j];
+            const uint32_t spos = dstart[d] + wcnt[warp][d] + rank[j];
+            skey[spos] = k[j];
+            sval[spos] = v[j];
         }
+    }
+    __syncthreads();
+    const int count = int(min(int64_t(kTileKeys), n - block0));
+    for (int t = threadIdx.x; t < count; t += kThreads) {
+        const uint32_t key = skey[t];
+        const uint32_t d = (key >> shift) & mask;
+        const uint32_t pos = boff[d] + (uint32_t(t) - dstart[d]);
+        keys_out[pos] = key;
+        vals_out[pos] = sval[t];
     }
 }
 

@@ -142,8 +142,12 @@ __device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t til
 }
 
 // Forward deposit of one photon into the shared accumulator (photon_differentials.cu:91-110).
-// With spans on, only the support's rows and row spans are visited; the other box pixels
-// add exactly zero in the reference (value > 0 fails, :106).
+// Per pixel of a row: u = (kx * M00 sx + c0, kx * M10 sx + c1) with the row constants
+// c = M (dx0, dy), s = |u|^2, and a predicated shared add of E 3/pi (1 - s)^2 where s < 1 (the
+// reference's value > 0, :106). With spans on, only the support's rows and row spans are
+// visited; the other box pixels add exactly zero in the reference. Photons that fail the
+// reference's image-half-size ellipse test somewhere in their box (tiny images only) take
+// the per-pixel test path.
 __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                         float* acc, int& bx0, int& bx1, int& by0, int& by1) {
     const uint32_t p = r.packed;
@@ -157,21 +161,40 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
     const float e3 = r.e * kThreeOverPi;
     const bool all = fl & kFlagEllipseAll;
     const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
     int ky0 = y0 - pyc, ky1 = y1 - pyc;
     support_rows(sup, r.dy0, ti.isy, ky0, ky1);
-    for (int ky = ky0; ky <= ky1; ++ky) {
-        const float dy = fmaf(float(ky), ti.sy, r.dy0);
-        int kx0 = x0 - pxc, kx1 = x1 - pxc;
-        if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
-        const float a0 = r.m01 * dy, a1 = r.m11 * dy;
-        float* row = acc + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
-        for (int kx = kx0; kx <= kx1; ++kx) {
-            const float dx = fmaf(float(kx), ti.sx, r.dx0);
-            const float u0 = fmaf(r.m00, dx, a0), u1 = fmaf(r.m10, dx, a1);
-            const float s = fmaf(u0, u0, u1 * u1);
-            if (s < 1.f && (all || ellipse_ok(kx, ky, ti.wd, ti.hd))) {
+    if (all) {
+        for (int ky = ky0; ky <= ky1; ++ky) {
+            const float dy = fmaf(float(ky), ti.sy, r.dy0);
+            int kx0 = x0 - pxc, kx1 = x1 - pxc;
+            if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
+            const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
+            const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
+            const float* q = acc + (pyc + ky - ti.oy) * sw + (pxc - ti.ox) + kx0;
+            float kf = float(kx0);
+            const int n = kx1 - kx0 + 1;
+#pragma unroll 2
+            for (int k = 0; k < n; ++k) {
+                const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
+                const float s = fmaf(u0, u0, u1 * u1);
                 const float t = 1.f - s;
-                atomicAdd(row + kx, t * t * e3);
+                red_shared_add_if(s < 1.f, q + k, (t * e3) * t);
+                kf += 1.f;
+            }
+        }
+    } else {
+        for (int ky = ky0; ky <= ky1; ++ky) {
+            const float dy = fmaf(float(ky), ti.sy, r.dy0);
+            const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
+            const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
+            float* row = acc + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
+            for (int kx = x0 - pxc; kx <= x1 - pxc; ++kx) {
+                if (!ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
+                const float u0 = fmaf(float(kx), a00, c0), u1 = fmaf(float(kx), a10, c1);
+                const float s = fmaf(u0, u0, u1 * u1);
+                const float t = 1.f - s;
+                red_shared_add_if(s < 1.f, row + kx, (t * e3) * t);
             }
         }
     }
@@ -190,7 +213,8 @@ __device__ __forceinline__ void bbox_publish(int* sb, int x0, int x1, int y0, in
     }
 }
 
-// Adds the touched box of the accumulator into the image and clears it.
+// Adds the touched box of the accumulator into the image and clears it: warps take rows,
+// lanes take consecutive columns (coalesced global adds; zeros are skipped).
 __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& ti, float* out,
                                            int* sb) {
     __syncthreads();
@@ -200,26 +224,26 @@ __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& t
         sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
     }
     if (x0 <= x1) {
-        const int bw = x1 - x0 + 1;
-        const int total = bw * (y1 - y0 + 1);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int nw = blockDim.x >> 5;
         float* img = out + ti.img_off;
-        for (int k = threadIdx.x; k < total; k += blockDim.x) {
-            const int rr = k / bw;
-            const int cc = k - rr * bw;
-            const int gx = x0 + cc, gy = y0 + rr;
-            float* a = acc + (gy - ti.oy) * sw + (gx - ti.ox);
-            const float v = *a;
-            if (v != 0.f) {
-                atomicAdd(img + int64_t(gy) * ti.W + gx, v);
-                *a = 0.f;
+        for (int gy = y0 + warp; gy <= y1; gy += nw) {
+            float* arow = acc + (gy - ti.oy) * sw - ti.ox;
+            float* grow = img + int64_t(gy) * ti.W;
+            for (int gx = x0 + lane; gx <= x1; gx += 32) {
+                const float v = arow[gx];
+                if (v != 0.f) {
+                    atomicAdd(grow + gx, v);
+                    arow[gx] = 0.f;
+                }
             }
         }
     }
     __syncthreads();
 }
 
-template <int NT>
-__global__ __launch_bounds__(NT) void fwd_tiles_kernel(TileArgs a) {
+template <int NT, int MINB>
+__global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     extern __shared__ float acc[];
     __shared__ int sb[4];
     const Cfg cfg = a.cfg;
@@ -267,21 +291,45 @@ __global__ __launch_bounds__(NT) void fwd_tiles_kernel(TileArgs a) {
     }
 }
 
-// Stages the tile+apron of the upstream gradient (clipped to the image).
+// Stages the tile+apron of the upstream gradient (clipped to the image): warps take rows,
+// lanes take consecutive columns.
 __device__ __forceinline__ void load_region(float* tg, int sw, const TileInfo& ti,
                                             const float* grad) {
     const int gx0 = max(ti.ox, 0), gx1 = min(ti.ox + sw, ti.W);
     const int gy0 = max(ti.oy, 0), gy1 = min(ti.oy + sw, ti.H);
-    const int bw = gx1 - gx0;
-    if (bw <= 0 || gy1 <= gy0) return;
-    const int total = bw * (gy1 - gy0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
     const float* img = grad + ti.img_off;
-    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        const int rr = k / bw;
-        const int cc = k - rr * bw;
-        const int gy = gy0 + rr, gx = gx0 + cc;
-        tg[(gy - ti.oy) * sw + (gx - ti.ox)] = __ldg(img + int64_t(gy) * ti.W + gx);
+    for (int gy = gy0 + warp; gy < gy1; gy += nw) {
+        float* trow = tg + (gy - ti.oy) * sw - ti.ox;
+        const float* grow = img + int64_t(gy) * ti.W;
+        for (int gx = gx0 + lane; gx < gx1; gx += 32) trow[gx] = __ldg(grow + gx);
     }
+}
+
+__device__ __forceinline__ void store_grad(GradRec* stage, uint32_t rid, float gE, float gx0,
+                                           float gx1, float g00, float g01, float g10,
+                                           float g11) {
+    float4* d = reinterpret_cast<float4*>(stage + rid);
+    d[0] = make_float4(gE, gx0, gx1, g00);
+    d[1] = make_float4(g01, g10, g11, 0.f);
+}
+
+// The moments of one photon turned into its gradients. With a = -12/pi E t g (the
+// reference's d_silverman(r) E g / r, :193), sums over the support of
+//   S  = sum t^2 g,  Sd = sum t g d,  Sdd = sum t g d d^T  (d the normalised offset)
+// give  dL/dE = 3/pi S,  dL/dx = -M^T (c M Sd),  dL/dM = c M Sdd  with c = -12/pi E
+// (:195-205 summed over the pixels; u = M d).
+__device__ __forceinline__ void finish_grad(GradRec* stage, uint32_t rid, float e, float m00,
+                                            float m01, float m10, float m11, float sE, float Sx,
+                                            float Sy, float Sxx, float Sxy, float Syy) {
+    const float c = -kTwelveOverPi * e;
+    const float v0 = c * fmaf(m00, Sx, m01 * Sy);
+    const float v1 = c * fmaf(m10, Sx, m11 * Sy);
+    store_grad(stage, rid, kThreeOverPi * sE, -fmaf(m00, v0, m10 * v1),
+               -fmaf(m01, v0, m11 * v1), c * fmaf(m00, Sxx, m01 * Sxy),
+               c * fmaf(m00, Sxy, m01 * Syy), c * fmaf(m10, Sxx, m11 * Sxy),
+               c * fmaf(m10, Sxy, m11 * Syy));
 }
 
 // Backward gather of one photon (photon_differentials.cu:169-218) from the staged gradient.
@@ -297,6 +345,7 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
     const int y0 = max(pyc - ry, 0), y1 = min(pyc + ry, ti.H - 1);
     const bool all = fl & kFlagEllipseAll;
     const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
     int ky0 = y0 - pyc, ky1 = y1 - pyc;
     support_rows(sup, r.dy0, ti.isy, ky0, ky1);
     float sE = 0.f, Sx = 0.f, Sy = 0.f, Sxx = 0.f, Sxy = 0.f, Syy = 0.f;
@@ -304,22 +353,42 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
         const float dy = fmaf(float(ky), ti.sy, r.dy0);
         int kx0 = x0 - pxc, kx1 = x1 - pxc;
         if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
-        const float a0 = r.m01 * dy, a1 = r.m11 * dy;
-        const float* row = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
+        const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
+        const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
+        const float* q = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
         float A0 = 0.f, A1 = 0.f, A2 = 0.f;
-        for (int kx = kx0; kx <= kx1; ++kx) {
-            if (!all && !ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
-            const float dx = fmaf(float(kx), ti.sx, r.dx0);
-            const float u0 = fmaf(r.m00, dx, a0), u1 = fmaf(r.m10, dx, a1);
-            const float s = fmaf(u0, u0, u1 * u1);
-            const float t = s < 1.f ? 1.f - s : 0.f;
-            const float g = row[kx];
-            const float tgv = t * g;
-            sE = fmaf(t, tgv, sE);
-            A0 += tgv;
-            const float adx = tgv * dx;
-            A1 += adx;
-            A2 = fmaf(adx, dx, A2);
+        if (all) {
+            float kf = float(kx0);
+            const int n = kx1 - kx0 + 1;
+#pragma unroll 2
+            for (int k = 0; k < n; ++k) {
+                const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
+                const float s = fmaf(u0, u0, u1 * u1);
+                const float t = s < 1.f ? 1.f - s : 0.f;
+                const float tgv = t * q[kx0 + k];
+                const float dx = fmaf(kf, ti.sx, r.dx0);
+                sE = fmaf(t, tgv, sE);
+                A0 += tgv;
+                const float adx = tgv * dx;
+                A1 += adx;
+                A2 = fmaf(adx, dx, A2);
+                kf += 1.f;
+            }
+        } else {
+            for (int kx = kx0; kx <= kx1; ++kx) {
+                if (!ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
+                const float kf = float(kx);
+                const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
+                const float s = fmaf(u0, u0, u1 * u1);
+                const float t = s < 1.f ? 1.f - s : 0.f;
+                const float tgv = t * q[kx];
+                const float dx = fmaf(kf, ti.sx, r.dx0);
+                sE = fmaf(t, tgv, sE);
+                A0 += tgv;
+                const float adx = tgv * dx;
+                A1 += adx;
+                A2 = fmaf(adx, dx, A2);
+            }
         }
         Sx += A1;
         Sy = fmaf(dy, A0, Sy);
@@ -327,21 +396,11 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
         Sxy = fmaf(dy, A1, Sxy);
         Syy = fmaf(dy * dy, A0, Syy);
     }
-    const float c = -kTwelveOverPi * r.e;
-    const float v0 = c * fmaf(r.m00, Sx, r.m01 * Sy);
-    const float v1 = c * fmaf(r.m10, Sx, r.m11 * Sy);
-    const int64_t n = a.ph.n;
-    a.gE[rid] = kThreeOverPi * sE;
-    a.gX[rid] = -fmaf(r.m00, v0, r.m10 * v1);
-    a.gX[n + rid] = -fmaf(r.m01, v0, r.m11 * v1);
-    a.gM[rid] = c * fmaf(r.m00, Sxx, r.m01 * Sxy);
-    a.gM[n + rid] = c * fmaf(r.m00, Sxy, r.m01 * Syy);
-    a.gM[3 * n + rid] = c * fmaf(r.m10, Sxx, r.m11 * Sxy);
-    a.gM[4 * n + rid] = c * fmaf(r.m10, Sxy, r.m11 * Syy);
+    finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
 }
 
-template <int NT>
-__global__ __launch_bounds__(NT) void bwd_tiles_kernel(TileArgs a) {
+template <int NT, int MINB>
+__global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
     extern __shared__ float tg[];
     const Cfg cfg = a.cfg;
     const int sw = cfg.sw, cb = cfg.class_bits;
@@ -499,30 +558,34 @@ __global__ __launch_bounds__(256) void tail_bwd_kernel(TileArgs a) {
             if (!any) {
                 d.m00 = d.m01 = d.m10 = d.m11 = d.e = 0.f;
             }
-            const float c = -kTwelveOverPi * d.e;
-            const float v0 = c * fmaf(d.m00, Sx, d.m01 * Sy);
-            const float v1 = c * fmaf(d.m10, Sx, d.m11 * Sy);
-            a.gE[rid] = kThreeOverPi * sE;
-            a.gX[rid] = -fmaf(d.m00, v0, d.m10 * v1);
-            a.gX[n + rid] = -fmaf(d.m01, v0, d.m11 * v1);
-            a.gM[rid] = c * fmaf(d.m00, Sxx, d.m01 * Sxy);
-            a.gM[n + rid] = c * fmaf(d.m00, Sxy, d.m01 * Syy);
-            a.gM[3 * n + rid] = c * fmaf(d.m10, Sxx, d.m11 * Sxy);
-            a.gM[4 * n + rid] = c * fmaf(d.m10, Sxy, d.m11 * Syy);
+            finish_grad(a.stage, rid, d.e, d.m00, d.m01, d.m10, d.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
         }
     }
     // photons that touch no pixel: zero gradients
     const int64_t inv0 = n_tile + n_big;
     const int64_t threads = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t p = inv0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += threads) {
-        const uint32_t rid = a.sidx[p];
-        a.gE[rid] = 0.f;
-        a.gX[rid] = 0.f;
-        a.gX[n + rid] = 0.f;
-        a.gM[rid] = 0.f;
-        a.gM[n + rid] = 0.f;
-        a.gM[3 * n + rid] = 0.f;
-        a.gM[4 * n + rid] = 0.f;
+    for (int64_t p = inv0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += threads)
+        store_grad(a.stage, a.sidx[p], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f);
+}
+
+// Spreads the per-photon gradient records (photon order) into the reference's outputs
+// grad_Ep[N], grad_xp[2][N], grad_Mp[2][3][N] (column 2 of grad_Mp is zero, :212, :218);
+// reads and writes are coalesced.
+__global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
+    const int64_t n = a.ph.n;
+    const float4* st = reinterpret_cast<const float4*>(a.stage);
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const float4 lo = st[2 * i], hi = st[2 * i + 1];
+        a.gE[i] = lo.x;
+        a.gX[i] = lo.y;
+        a.gX[n + i] = lo.z;
+        a.gM[i] = lo.w;
+        a.gM[n + i] = hi.x;
+        a.gM[2 * n + i] = 0.f;
+        a.gM[3 * n + i] = hi.y;
+        a.gM[4 * n + i] = hi.z;
+        a.gM[5 * n + i] = 0.f;
     }
 }
 
@@ -574,14 +637,16 @@ cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
+template <int MINB>
+cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
     const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
-    cudaError_t e = set_smem(fwd_tiles_kernel<kTileThreads>, smem);
+    auto kern = fwd_tiles_kernel<kTileThreads, MINB>;
+    cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
     if (chunks > 0) {
-        const int grid = persistent_grid(fwd_tiles_kernel<kTileThreads>, smem, chunks);
-        fwd_tiles_kernel<kTileThreads><<<grid, kTileThreads, smem, st>>>(a);
+        const int grid = persistent_grid(kern, smem, chunks);
+        kern<<<grid, kTileThreads, smem, st>>>(a);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         const int tgrid = num_sms() * 2;
@@ -591,21 +656,36 @@ cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
     return e;
 }
 
-cudaError_t launch_backward(const TileArgs& a, cudaStream_t st) {
+template <int MINB>
+cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
     const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
-    cudaError_t e = set_smem(bwd_tiles_kernel<kTileThreads>, smem);
+    auto kern = bwd_tiles_kernel<kTileThreads, MINB>;
+    cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
     if (chunks > 0) {
-        const int grid = persistent_grid(bwd_tiles_kernel<kTileThreads>, smem, chunks);
-        bwd_tiles_kernel<kTileThreads><<<grid, kTileThreads, smem, st>>>(a);
+        const int grid = persistent_grid(kern, smem, chunks);
+        kern<<<grid, kTileThreads, smem, st>>>(a);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         const int tgrid = num_sms() * 2;
         tail_bwd_kernel<<<tgrid, 256, 0, st>>>(a);
         e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        const int64_t sblocks = (a.ph.n + 255) / 256;
+        const int64_t scap = int64_t(num_sms()) * 16;
+        grad_scatter_kernel<<<unsigned(sblocks < scap ? sblocks : scap), 256, 0, st>>>(a);
+        e = cudaGetLastError();
     }
     return e;
+}
+
+cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
+    return a.cfg.min_blocks >= 3 ? launch_forward_t<3>(a, st) : launch_forward_t<2>(a, st);
+}
+
+cudaError_t launch_backward(const TileArgs& a, cudaStream_t st) {
+    return a.cfg.min_blocks >= 3 ? launch_backward_t<3>(a, st) : launch_backward_t<2>(a, st);
 }
 
 }  // namespace pds

@@ -43,6 +43,7 @@ struct TileArgs {
     float* gE;                 // backward outputs
     float* gX;
     float* gM;
+    GradRec* stage;            // backward: per-photon gradient records (workspace)
 };
 
 cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st);

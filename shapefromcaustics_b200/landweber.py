@@ -110,7 +110,7 @@ def jitter(H, W, scene, per_texel, generator, device):
 
 
 def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image=1024,
-                smoothing=4.0, params=None, mask=None, seed=0, keep_plan=False, target=None,
+                footprint_px=3.0, params=None, mask=None, seed=0, keep_plan=False, target=None,
                 log_every=0):
     """The reference's pixel-basis Landweber loop (``shape_from_caustics.py:343-420``,
     default options) for a height-field plate, all on the device.
@@ -119,13 +119,15 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
     per texel into one image (the reference's sum over simulations, ``:351-353``), takes the
     L2 discrepancy ``0.5 |I - T|^2 / |T|^2`` against the target, back-propagates to the
     height-field offset through the splat and refraction kernels (refracted positions
-    recomputed, not stored) and applies the fused projected update. Returns a dict with the
-    reconstructed offset, the per-iteration discrepancy and height RMSE."""
+    recomputed, not stored) and applies the fused projected update. ``footprint_px`` sets the
+    photons' initial positional differentials to that many receiver pixels (the reference's
+    splat smoothing, ``model/caustics.py:60-61``). Returns a dict with the reconstructed
+    offset, the per-iteration discrepancy and height RMSE."""
     from .plate import PlateSplat, plate_params
     dev = h_true.device
     H, W = h_true.shape
     n = H * W * per_texel * sims
-    du0 = 2.0 * smoothing * math.sqrt(H * W * scene.texel ** 2 / (math.pi * n))
+    du0 = footprint_px * 2.0 * scene.receiver_half / image
     pp = plate_params(scene, du0)
     shape = (1, image, image)
     g = torch.Generator(device=dev)
@@ -156,7 +158,7 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
                              device=dev)
         landweber_update(d, hv.grad, mask, params, ws)
         if log_every and (it % log_every == 0 or it == iterations - 1):
-            hist["discrepancy"].append((it, float(loss)))
+            hist["discrepancy"].append((it, float(loss.detach())))
             hist["rmse"].append((it, float(((d - d_true) ** 2).mean().sqrt())))
     rmse = float(((d - d_true) ** 2).mean().sqrt())
     return {"d": d, "rmse": rmse, "history": hist, "target": target, "photons_per_iteration": n}

@@ -72,9 +72,12 @@ def test_batch_layout_on_host():
         t[k].channels, t[k].height, t[k].width = c, h, w
         b += 10 + k
     nt = ctypes.c_int64()
-    _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))
+    cfg = _lib.config(tile=32)
+    _lib.check(lib.pds_batch_layout(t, 3, ctypes.byref(cfg), ctypes.byref(nt)))
     assert [t[k].tile_base for k in range(3)] == [0, 256, 256 + 2 * 4 * 3]
     assert nt.value == 256 + 24 + 1
+    _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))  # default 64-pixel tiles
+    assert [t[k].tile_base for k in range(3)] == [0, 64, 64 + 2 * 2 * 2]
     t[1].photon_begin = 3  # not contiguous
     with pytest.raises(_lib.PdsError):
         _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))

@@ -68,10 +68,10 @@ def test_uniform_cluster_512(cuda):
     assert_parity(ph, (1, 512, 512), 20)
 
 
-@pytest.mark.parametrize("cfg", [dict(tile=16), dict(tile=64), dict(chunk=256),
-                                 dict(class_bits=2), dict(class_bits=4, chunk=4096),
-                                 dict(tile=32, apron_max=3), dict(walk=1),
-                                 dict(walk=1, tile=16, class_bits=3)])
+@pytest.mark.parametrize("cfg", [dict(tile=16), dict(tile=32), dict(chunk=256),
+                                 dict(class_bits=-1), dict(class_bits=4, chunk=4096),
+                                 dict(tile=32, apron_max=3), dict(walk=2),
+                                 dict(walk=2, tile=16, class_bits=1), dict(min_blocks=2)])
 def test_tuning_variants(cuda, cfg):
     ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
     assert_parity(ph, (1, 256, 256), 20, cfg=cfg)
