@@ -3,7 +3,7 @@
 // This layer validates arguments the way the reference's binding does
 // (PyOptix/PhotonDifferentialSplattig.cpp:14-22: matching photon counts, 2-row positions,
 // 2x3 matrices, one channel row), lays the workspace out, and enqueues
-//   plan:     counters reset, plan_kernel, radix sort
+//   plan:     counters reset, plan_kernel, radix sort, sort_records_kernel
 //   forward:  output reset, fwd_tiles_kernel, tail_fwd_kernel
 //   backward: bwd_tiles_kernel, tail_bwd_kernel, grad_scatter_kernel
 // on the caller's stream. It allocates nothing and never synchronises. Failures return a
@@ -92,8 +92,10 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     return PDS_OK;
 }
 
+// recs holds the plan's records in photon order until they are copied into srecs in sorted
+// order; it is then free, and the backward reuses it for its per-photon gradient records.
 struct Layout {
-    size_t counters, k0, k1, v0, v1, recs, stage, aux, total;
+    size_t counters, k0, k1, v0, v1, recs, srecs, aux, total;
 };
 
 Layout make_layout(int64_t n) {
@@ -106,7 +108,7 @@ Layout make_layout(int64_t n) {
     L.v0 = off; off += pds::align_up(nn * 4, 256);
     L.v1 = off; off += pds::align_up(nn * 4, 256);
     L.recs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
-    L.stage = off; off += pds::align_up(nn * sizeof(pds::GradRec), 256);
+    L.srecs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
     L.aux = off; off += pds::sort_aux_bytes(n);
     L.total = off;
     return L;
@@ -116,6 +118,7 @@ struct Bufs {
     uint32_t* counters;
     uint32_t *k0, *k1, *v0, *v1;
     pds::Rec* recs;
+    pds::Rec* srecs;
     pds::GradRec* stage;
     void* aux;
 };
@@ -129,7 +132,9 @@ Bufs bufs(void* ws, const Layout& L) {
     r.v0 = reinterpret_cast<uint32_t*>(b + L.v0);
     r.v1 = reinterpret_cast<uint32_t*>(b + L.v1);
     r.recs = reinterpret_cast<pds::Rec*>(b + L.recs);
-    r.stage = reinterpret_cast<pds::GradRec*>(b + L.stage);
+    r.srecs = reinterpret_cast<pds::Rec*>(b + L.srecs);
+    r.stage = reinterpret_cast<pds::GradRec*>(b + L.recs);
+    static_assert(sizeof(pds::GradRec) == sizeof(pds::Rec), "gradient records reuse recs");
     r.aux = b + L.aux;
     return r;
 }
@@ -231,6 +236,8 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     uint32_t *ko, *vo;
     e = pds::radix_sort(b.k1, b.k0, b.k1, b.v0, b.v1, ph.n, r.key_bits, b.aux, s, &ko, &vo);
     if (e != cudaSuccess) return cuda_fail(e, "radix sort");
+    e = pds::launch_sort_records(b.recs, vo, b.counters, ph.n, b.srecs, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sort_records_kernel");
     return PDS_OK;
 }
 
@@ -249,7 +256,7 @@ int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.mpr = mpr;
     a.cfg = r.cfg;
     sorted_bufs(b, r.key_bits, &a.skeys, &a.sidx);
-    a.recs = b.recs;
+    a.srecs = b.srecs;
     a.stage = b.stage;
     a.counters = b.counters;
     return PDS_OK;

@@ -214,7 +214,9 @@ __device__ __forceinline__ void bbox_publish(int* sb, int x0, int x1, int y0, in
 }
 
 // Adds the touched box of the accumulator into the image and clears it: warps take rows,
-// lanes take consecutive columns (coalesced global adds; zeros are skipped).
+// lanes take consecutive columns. When image rows are 16-byte aligned the adds are 4-wide
+// vector reductions (red.global.add.v4.f32) over 4-aligned column groups; columns of a group
+// outside the touched box add zero. All-zero groups are skipped.
 __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& ti, float* out,
                                            int* sb) {
     __syncthreads();
@@ -227,14 +229,39 @@ __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& t
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int nw = blockDim.x >> 5;
         float* img = out + ti.img_off;
-        for (int gy = y0 + warp; gy <= y1; gy += nw) {
-            float* arow = acc + (gy - ti.oy) * sw - ti.ox;
-            float* grow = img + int64_t(gy) * ti.W;
-            for (int gx = x0 + lane; gx <= x1; gx += 32) {
-                const float v = arow[gx];
-                if (v != 0.f) {
-                    atomicAdd(grow + gx, v);
-                    arow[gx] = 0.f;
+        const bool vec = (ti.W & 3) == 0 && (reinterpret_cast<uintptr_t>(img) & 15) == 0;
+        if (vec) {
+            const int g0 = x0 >> 2, g1 = x1 >> 2;
+            for (int gy = y0 + warp; gy <= y1; gy += nw) {
+                float* arow = acc + (gy - ti.oy) * sw - ti.ox;
+                float* grow = img + int64_t(gy) * ti.W;
+                for (int g = g0 + lane; g <= g1; g += 32) {
+                    const int gx = g << 2;
+                    float v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int c = gx + j;
+                        v[j] = 0.f;
+                        if (c >= x0 && c <= x1) {
+                            v[j] = arow[c];
+                            arow[c] = 0.f;
+                        }
+                    }
+                    if (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f)
+                        atomicAdd(reinterpret_cast<float4*>(grow + gx),
+                                  make_float4(v[0], v[1], v[2], v[3]));
+                }
+            }
+        } else {
+            for (int gy = y0 + warp; gy <= y1; gy += nw) {
+                float* arow = acc + (gy - ti.oy) * sw - ti.ox;
+                float* grow = img + int64_t(gy) * ti.W;
+                for (int gx = x0 + lane; gx <= x1; gx += 32) {
+                    const float v = arow[gx];
+                    if (v != 0.f) {
+                        atomicAdd(grow + gx, v);
+                        arow[gx] = 0.f;
+                    }
                 }
             }
         }
@@ -266,7 +293,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
             Rec r;
             if (have) {
                 key = a.skeys[i] >> cb;
-                r = a.recs[a.sidx[i]];
+                r = a.srecs[i];
             }
             const int64_t bend = min(base + NT, p1);
             // The batch's keys are sorted, so its segments are consecutive thread ranges;
@@ -419,7 +446,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
             if (have) {
                 key = a.skeys[i] >> cb;
                 rid = a.sidx[i];
-                r = a.recs[rid];
+                r = a.srecs[i];
             }
             const int64_t bend = min(base + NT, p1);
             // consecutive segments of the sorted batch, as in fwd_tiles_kernel
@@ -589,6 +616,18 @@ __global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
     }
 }
 
+// Records of the tile-path photons in sorted order, so that the tile kernels read them with
+// coalesced loads; this one random gather replaces one per tile kernel.
+__global__ __launch_bounds__(256) void sort_records_kernel(const Rec* __restrict__ recs,
+                                                           const uint32_t* __restrict__ sidx,
+                                                           const uint32_t* __restrict__ counters,
+                                                           int64_t n, Rec* __restrict__ srecs) {
+    const int64_t n_tile = min(int64_t(counters[0]), n);
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n_tile;
+         p += int64_t(gridDim.x) * blockDim.x)
+        srecs[p] = recs[__ldg(sidx + p)];
+}
+
 __global__ void iota_kernel(uint32_t* dst, int64_t n) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x)
@@ -627,6 +666,16 @@ void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st) {
     if (n <= 0) return;
     const int64_t blocks = (n + 255) / 256;
     iota_kernel<<<unsigned(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(dst, n);
+}
+
+cudaError_t launch_sort_records(const Rec* recs, const uint32_t* sidx, const uint32_t* counters,
+                                int64_t n, Rec* srecs, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t blocks = (n + 255) / 256;
+    const int64_t cap = int64_t(num_sms()) * 16;
+    sort_records_kernel<<<unsigned(blocks < cap ? blocks : cap), 256, 0, st>>>(recs, sidx, counters,
+                                                                              n, srecs);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st) {

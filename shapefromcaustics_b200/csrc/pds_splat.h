@@ -36,7 +36,7 @@ struct TileArgs {
     Cfg cfg;
     const uint32_t* skeys;     // sorted keys
     const uint32_t* sidx;      // sorted photon indices
-    const Rec* recs;
+    const Rec* srecs;          // records in sorted order
     const uint32_t* counters;
     float* out;                // forward: flat image buffer (zeroed by caller)
     const float* grad;         // backward: flat upstream gradient buffer
@@ -47,6 +47,8 @@ struct TileArgs {
 };
 
 cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st);
+cudaError_t launch_sort_records(const Rec* recs, const uint32_t* sidx, const uint32_t* counters,
+                                int64_t n, Rec* srecs, cudaStream_t st);
 cudaError_t launch_forward(const TileArgs& a, cudaStream_t st);
 cudaError_t launch_backward(const TileArgs& a, cudaStream_t st);
 
