@@ -178,10 +178,11 @@ def workload(name, rank, device):
         specs = [(2 ** 23, (1, 1024, 1024))]
         photons = S.uniform_cluster_photons(2 ** 23, 1024, 1024, seed=seed, device=device)
         desc = "2^23 photons, 1024^2, uniform+cluster, s ~ logU[0.5,4] px, mpr 20, fp32"
-    elif name == "contention":
-        specs = [(2 ** 26, (1, 2048, 2048))]
-        photons = S.caustic_curve_photons(2 ** 26, 2048, 2048, seed=seed, device=device)
-        desc = ("2^26 photons, 2048^2, 80% on 4 caustic curves (1.5 px), "
+    elif name in ("contention", "contention24"):
+        n = 2 ** 26 if name == "contention" else 2 ** 24
+        specs = [(n, (1, 2048, 2048))]
+        photons = S.caustic_curve_photons(n, 2048, 2048, seed=seed, device=device)
+        desc = (f"2^{n.bit_length() - 1} photons, 2048^2, 80% on 4 caustic curves (1.5 px), "
                 "s ~ logU[0.25,16] px, mpr 20, fp32")
     else:
         raise SystemExit(f"unknown workload {name}")
@@ -701,8 +702,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--workload", default="batch64",
-                    choices=["batch64", "uniform1m", "medium", "contention", "landweber256",
-                             "recon1024"])
+                    choices=["batch64", "uniform1m", "medium", "contention", "contention24",
+                             "landweber256", "recon1024"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lean", action="store_true",
                     help="timed steps and phase timings only (for profiler runs)")

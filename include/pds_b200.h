@@ -57,6 +57,8 @@ typedef struct pds_config {
                            default 1 */
     int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2 (more
                            registers per thread) or 3 (more warps); default 3 */
+    int32_t coop_radius; /* footprints with a radius (px) of at least this are splatted by a
+                           whole warp instead of one thread; -1 never; default 5 */
 } pds_config;
 
 /* One simulation of a batch. The caller fills photon_begin, n_photons, image_offset,

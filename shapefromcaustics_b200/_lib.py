@@ -21,7 +21,8 @@ class PdsConfig(ctypes.Structure):
     """Mirror of ``pds_config``."""
     _fields_ = [("tile", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("class_bits", ctypes.c_int32), ("apron_max", ctypes.c_int32),
-                ("walk", ctypes.c_int32), ("min_blocks", ctypes.c_int32)]
+                ("walk", ctypes.c_int32), ("min_blocks", ctypes.c_int32),
+                ("coop_radius", ctypes.c_int32)]
 
 
 class PdsSim(ctypes.Structure):
@@ -129,6 +130,6 @@ def check(rc):
         raise PdsError(rc, msg)
 
 
-def config(tile=0, chunk=0, class_bits=0, apron_max=0, walk=0, min_blocks=0):
+def config(tile=0, chunk=0, class_bits=0, apron_max=0, walk=0, min_blocks=0, coop_radius=0):
     return PdsConfig(int(tile), int(chunk), int(class_bits), int(apron_max), int(walk),
-                     int(min_blocks))
+                     int(min_blocks), int(coop_radius))

@@ -53,6 +53,9 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
     out.walk = (in && in->walk) ? in->walk : 1;
     out.min_blocks = (in && in->min_blocks) ? in->min_blocks : 3;
+    out.coop_radius = (in && in->coop_radius) ? in->coop_radius : 5;
+    if (out.coop_radius < -1 || out.coop_radius > 63)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.coop_radius must be -1 or in [1, 63]");
     if (out.min_blocks != 2 && out.min_blocks != 3)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.min_blocks must be 2 or 3");
     if (out.walk != 1 && out.walk != 2)
@@ -83,9 +86,11 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     r.cfg.chunk = c.chunk;
     r.cfg.class_bits = c.class_bits;
     r.cfg.apron = mpr < 0 ? 0 : (mpr < c.apron_max ? mpr : c.apron_max);
-    r.cfg.sw = c.tile + 2 * r.cfg.apron;
+    // odd pitch: the rows of one column of the accumulator fall in different banks
+    r.cfg.sw = (c.tile + 2 * r.cfg.apron) | 1;
     r.cfg.spans = c.walk == 2 ? 1 : 0;
     r.cfg.min_blocks = c.min_blocks;
+    r.cfg.coop_r = c.coop_radius > 0 ? c.coop_radius : 0;
     r.key_big = uint32_t(uint64_t(n_tiles) << c.class_bits);
     r.key_invalid = uint32_t(inv);
     r.key_bits = bit_length(inv);

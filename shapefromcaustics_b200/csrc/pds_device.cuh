@@ -66,6 +66,7 @@ struct Cfg {
     int32_t sw;          // tile + 2 * apron: edge of the shared accumulator
     int32_t spans;       // 1: walk only the support's rows / row spans; 0: the whole box
     int32_t min_blocks;  // resident CTAs per SM the tile kernels' register budget targets
+    int32_t coop_r;      // footprint radius from which a photon is splatted by a whole warp
 };
 
 // Simulation table: either a device array or one inline descriptor.
@@ -218,6 +219,15 @@ __device__ __forceinline__ void red_shared_add_if(bool p, const float* addr, flo
     asm volatile(
         "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q red.shared.add.f32 [%0], %1;\n\t}"
         :: "r"(a), "f"(v), "r"(int(p)) : "memory");
+}
+
+// Shared add of v at shared byte address a + OFF when s < 1 (the kernel's support), as one
+// predicated reduction: no branch per pixel.
+template <int OFF>
+__device__ __forceinline__ void red_shared_inside(uint32_t a, float s, float v) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.lt.f32 q, %1, 0f3F800000;\n\t@q red.shared.add.f32 [%0+%3], %2;\n\t}"
+        :: "r"(a), "f"(s), "f"(v), "n"(OFF) : "memory");
 }
 
 }  // namespace pds

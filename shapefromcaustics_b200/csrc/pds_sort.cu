@@ -2,12 +2,12 @@
 //
 // The splatting plan sorts photons by (simulation, channel, screen tile, footprint class);
 // the permutation must equal a CPU stable sort bit for bit, so every pass is stable:
-//   upsweep    per 4096-key block digit counts (warp-aggregated shared atomics), block-major
+//   upsweep    per 2048-key block digit counts (warp-aggregated shared atomics), block-major
 //   col scan   column-wise exclusive scan of the [blocks][radix] count matrix in three
 //              coalesced kernels (group partials, one-CTA top scan with digit bases, group
 //              down-sweep), yielding each block's first output slot per digit
 //   downsweep  stable rank inside the block (warp-striped order: warp w owns a contiguous
-//              512-key range, ranked per 32-key step with __match_any_sync), the block's
+//              256-key range, ranked per 32-key step with __match_any_sync), the block's
 //              keys staged in shared memory in digit order, then each digit's run written
 //              contiguously (coalesced stores instead of one scattered store per key)
 // Digits are at most 8 bits; the number of passes is ceil(key_bits / 8) with the bits spread
@@ -23,7 +23,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kIpt = 16;                       // keys per thread
+constexpr int kIpt = 8;                        // keys per thread
 constexpr int kTileKeys = kThreads * kIpt;     // keys per sort block
 constexpr int kGroup = 64;                     // sort blocks per column-scan group
 

@@ -39,15 +39,23 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
     uint32_t c_tile = 0, c_big = 0, c_inv = 0;
     const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
     const uint32_t cls_max = (1u << cb) - 1u;
+    const int64_t* __restrict__ cp = a.ph.cp;
+    const float* __restrict__ X = a.ph.X;
+    const float* __restrict__ R = a.ph.R;
+    const float* __restrict__ E = a.ph.E;
+    const float* __restrict__ M = a.ph.M;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        // all of the photon's inputs are loaded up front (coalesced, one latency round)
+        const int64_t ch = __ldg(cp + i);
+        const float x = __ldg(X + i), y = __ldg(X + n + i), rad = __ldg(R + i);
+        const float e = __ldg(E + i);
+        const float m00 = __ldg(M + i), m01 = __ldg(M + n + i);
+        const float m10 = __ldg(M + 3 * n + i), m11 = __ldg(M + 4 * n + i);
         const int s = find_sim_of_photon(a.sims, i);
         const pds_sim sim = load_sim(a.sims, s);
-        const int64_t ch = __ldg(a.ph.cp + i);
         uint32_t key = a.key_invalid;
         if (ch >= 0 && ch < sim.channels) {
-            const float x = __ldg(a.ph.X + i), y = __ldg(a.ph.X + n + i);
-            const Footprint f = make_footprint(x, y, __ldg(a.ph.R + i), sim.height, sim.width,
-                                               a.mpr);
+            const Footprint f = make_footprint(x, y, rad, sim.height, sim.width, a.mpr);
             int32_t x0, x1, y0, y1;
             if (clip_box(f, sim.height, sim.width, x0, x1, y0, y1)) {
                 if (f.rx > A || f.ry > A) {
@@ -60,16 +68,15 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
                                           uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
                     const uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
                     key = (tile << cb) | cls;
-                    const float e = __ldg(a.ph.E + i);
                     const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) |
                                            (e > 0.f ? 0u : kFlagFwdSkip);
                     Rec r;
                     r.dx0 = corner_offset(f.px_c, sim.width, x);
                     r.dy0 = corner_offset(f.py_c, sim.height, y);
-                    r.m00 = __ldg(a.ph.M + i);
-                    r.m01 = __ldg(a.ph.M + n + i);
-                    r.m10 = __ldg(a.ph.M + 3 * n + i);
-                    r.m11 = __ldg(a.ph.M + 4 * n + i);
+                    r.m00 = m00;
+                    r.m01 = m01;
+                    r.m10 = m10;
+                    r.m11 = m11;
                     r.e = e;
                     r.packed = pack_rec(f.px_c - (tx * T - A), f.py_c - (ty * T - A), f.rx, f.ry,
                                         flags);
@@ -141,11 +148,36 @@ __device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t til
     return t;
 }
 
+// One row of a forward deposit: n pixels from shared byte address a, with
+// u = (k M00 sx + b0, k M10 sx + b1) at the k-th pixel, s = |u|^2, and a predicated shared add
+// of E 3/pi (1 - s)^2 where s < 1 (the reference's value > 0, photon_differentials.cu:105-106).
+// Lanes of a warp hold photons of one footprint class, so n is nearly always warp-uniform and
+// the loop stays converged; it is unrolled by two.
+__device__ __forceinline__ void fwd_row(int n, uint32_t a, float b0, float b1, float a00,
+                                        float a10, float e3) {
+    float kf = 0.f;
+    int k = 0;
+    for (; k + 1 < n; k += 2) {
+        const float u0 = fmaf(kf, a00, b0), u1 = fmaf(kf, a10, b1);
+        const float v0 = u0 + a00, v1 = u1 + a10;
+        const float s = fmaf(u0, u0, u1 * u1), s2 = fmaf(v0, v0, v1 * v1);
+        const float t = 1.f - s, t2 = 1.f - s2;
+        red_shared_inside<0>(a, s, (t * e3) * t);
+        red_shared_inside<4>(a, s2, (t2 * e3) * t2);
+        a += 8u;
+        kf += 2.f;
+    }
+    if (k < n) {
+        const float u0 = fmaf(kf, a00, b0), u1 = fmaf(kf, a10, b1);
+        const float s = fmaf(u0, u0, u1 * u1);
+        const float t = 1.f - s;
+        red_shared_inside<0>(a, s, (t * e3) * t);
+    }
+}
+
 // Forward deposit of one photon into the shared accumulator (photon_differentials.cu:91-110).
-// Per pixel of a row: u = (kx * M00 sx + c0, kx * M10 sx + c1) with the row constants
-// c = M (dx0, dy), s = |u|^2, and a predicated shared add of E 3/pi (1 - s)^2 where s < 1 (the
-// reference's value > 0, :106). With spans on, only the support's rows and row spans are
-// visited; the other box pixels add exactly zero in the reference. Photons that fail the
+// With spans on, only the support's rows and row spans are visited; the other box pixels
+// add exactly zero in the reference (value > 0 fails, :106). Photons that fail the
 // reference's image-half-size ellipse test somewhere in their box (tiny images only) take
 // the per-pixel test path.
 __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
@@ -162,41 +194,106 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
     const bool all = fl & kFlagEllipseAll;
     const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
     const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
+    const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
+    // u at the centre pixel's corner: M (dx0, dy0)
+    const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
+    const uint32_t acc_base = static_cast<uint32_t>(__cvta_generic_to_shared(acc));
     int ky0 = y0 - pyc, ky1 = y1 - pyc;
     support_rows(sup, r.dy0, ti.isy, ky0, ky1);
     if (all) {
-        for (int ky = ky0; ky <= ky1; ++ky) {
+        // Each lane starts its row walk at a different row: co-located photons in one warp
+        // (focused caustics) then add into different rows at the same time instead of
+        // serialising on one shared address.
+        const int nrows = ky1 - ky0 + 1;
+        int ky = nrows > 0 ? ky0 + int(threadIdx.x & 31) % nrows : ky0;
+        for (int j = 0; j < nrows; ++j, ky = (ky == ky1) ? ky0 : ky + 1) {
             const float dy = fmaf(float(ky), ti.sy, r.dy0);
             int kx0 = x0 - pxc, kx1 = x1 - pxc;
             if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
-            const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
-            const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
-            const float* q = acc + (pyc + ky - ti.oy) * sw + (pxc - ti.ox) + kx0;
-            float kf = float(kx0);
-            const int n = kx1 - kx0 + 1;
-#pragma unroll 2
-            for (int k = 0; k < n; ++k) {
-                const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
-                const float s = fmaf(u0, u0, u1 * u1);
-                const float t = 1.f - s;
-                red_shared_add_if(s < 1.f, q + k, (t * e3) * t);
-                kf += 1.f;
-            }
+            const float kf = float(kx0);
+            const float b0 = fmaf(kf, a00, fmaf(float(ky), m01sy, c00));
+            const float b1 = fmaf(kf, a10, fmaf(float(ky), m11sy, c10));
+            const uint32_t a = acc_base +
+                               4u * uint32_t((pyc + ky - ti.oy) * sw + (pxc + kx0 - ti.ox));
+            fwd_row(kx1 - kx0 + 1, a, b0, b1, a00, a10, e3);
         }
     } else {
         for (int ky = ky0; ky <= ky1; ++ky) {
             const float dy = fmaf(float(ky), ti.sy, r.dy0);
             const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
             const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
-            float* row = acc + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
+            const uint32_t arow = acc_base + 4u * uint32_t((pyc + ky - ti.oy) * sw + (pxc - ti.ox));
             for (int kx = x0 - pxc; kx <= x1 - pxc; ++kx) {
                 if (!ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
                 const float u0 = fmaf(float(kx), a00, c0), u1 = fmaf(float(kx), a10, c1);
                 const float s = fmaf(u0, u0, u1 * u1);
                 const float t = 1.f - s;
-                red_shared_add_if(s < 1.f, row + kx, (t * e3) * t);
+                red_shared_inside<0>(arow + 4u * uint32_t(kx), s, (t * e3) * t);
             }
         }
+    }
+}
+
+// Photons with a footprint radius of at least cfg.coop_r are splatted by their whole warp:
+// lane j takes rows j, j + 32, ... of the photon and walks each row's span of the support
+// (|M d| < 1 solved per row, one pixel of margin) rather than the whole box row. Large and
+// thin footprints then cost about their support area, co-located photons of a caustic no
+// longer make a warp's lanes add into one shared address at once, and with an odd
+// accumulator pitch the 32 rows of one column fall in 32 different banks.
+__device__ __forceinline__ bool use_coop(const Rec& r, int coop_r) {
+    const uint32_t p = r.packed;
+    const uint32_t fl = rec_flags(p);
+    return coop_r > 0 && (fl & kFlagEllipseAll) && !(fl & kFlagFwdSkip) &&
+           (rec_rx(p) >= coop_r || rec_ry(p) >= coop_r);
+}
+
+__device__ __forceinline__ Rec shfl_rec(const Rec& r, int src) {
+    Rec o;
+    o.dx0 = __shfl_sync(0xFFFFFFFFu, r.dx0, src);
+    o.dy0 = __shfl_sync(0xFFFFFFFFu, r.dy0, src);
+    o.m00 = __shfl_sync(0xFFFFFFFFu, r.m00, src);
+    o.m01 = __shfl_sync(0xFFFFFFFFu, r.m01, src);
+    o.m10 = __shfl_sync(0xFFFFFFFFu, r.m10, src);
+    o.m11 = __shfl_sync(0xFFFFFFFFu, r.m11, src);
+    o.e = __shfl_sync(0xFFFFFFFFu, r.e, src);
+    o.packed = __shfl_sync(0xFFFFFFFFu, r.packed, src);
+    return o;
+}
+
+// Clipped box of a record in pixel coordinates.
+__device__ __forceinline__ void rec_box(const Rec& r, const TileInfo& ti, int& pxc, int& pyc,
+                                        int& x0, int& x1, int& y0, int& y1) {
+    const uint32_t p = r.packed;
+    pxc = ti.ox + rec_lx(p);
+    pyc = ti.oy + rec_ly(p);
+    const int rx = rec_rx(p), ry = rec_ry(p);
+    x0 = max(pxc - rx, 0);
+    x1 = min(pxc + rx, ti.W - 1);
+    y0 = max(pyc - ry, 0);
+    y1 = min(pyc + ry, ti.H - 1);
+}
+
+// Forward deposit of one photon by the whole warp (see use_coop).
+__device__ __forceinline__ void deposit_coop(const Rec& r, const TileInfo& ti, int sw,
+                                             uint32_t acc_base, int lane) {
+    int pxc, pyc, x0, x1, y0, y1;
+    rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
+    const float e3 = r.e * kThreeOverPi;
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
+    const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
+    const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
+    const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, true);
+    int ky0 = y0 - pyc, ky1 = y1 - pyc;
+    support_rows(sup, r.dy0, ti.isy, ky0, ky1);
+    for (int ky = ky0 + lane; ky <= ky1; ky += 32) {
+        const float dy = fmaf(float(ky), ti.sy, r.dy0);
+        int kx0 = x0 - pxc, kx1 = x1 - pxc;
+        if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
+        const float kf = float(kx0);
+        const float b0 = fmaf(kf, a00, fmaf(float(ky), m01sy, c00));
+        const float b1 = fmaf(kf, a10, fmaf(float(ky), m11sy, c10));
+        const uint32_t a = acc_base + 4u * uint32_t((pyc + ky - ti.oy) * sw + (pxc + kx0 - ti.ox));
+        fwd_row(kx1 - kx0 + 1, a, b0, b1, a00, a10, e3);
     }
 }
 
@@ -280,6 +377,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
         sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
     }
     __syncthreads();
+    const uint32_t acc_base = static_cast<uint32_t>(__cvta_generic_to_shared(acc));
     const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
@@ -290,7 +388,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
             const int64_t i = base + threadIdx.x;
             const bool have = i < p1;
             uint32_t key = 0xFFFFFFFFu;
-            Rec r;
+            Rec r = {};
             if (have) {
                 key = a.skeys[i] >> cb;
                 r = a.srecs[i];
@@ -303,8 +401,17 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
             int done = 0;
             for (int pass = 0; pass <= NT; ++pass) {
                 const bool mine = have && key == cur;
+                const bool coop = mine && use_coop(r, cfg.coop_r);
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-                if (mine) deposit(r, ti, sw, cfg.spans, acc, x0, x1, y0, y1);
+                if (mine && !coop) deposit(r, ti, sw, cfg.spans, acc, x0, x1, y0, y1);
+                if (coop) {
+                    int pxc, pyc;
+                    rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
+                }
+                for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
+                    const Rec rb = shfl_rec(r, __ffs(cm) - 1);
+                    deposit_coop(rb, ti, sw, acc_base, threadIdx.x & 31);
+                }
                 bbox_publish(sb, x0, x1, y0, y1);
                 done += __syncthreads_count(mine);
                 const int64_t nxt = base + done;
@@ -359,9 +466,49 @@ __device__ __forceinline__ void finish_grad(GradRec* stage, uint32_t rid, float 
                c * fmaf(m10, Sxy, m11 * Syy));
 }
 
+// One row of a backward gather: n pixels from q, the first at pixel offset k0 (relative to
+// the centre pixel). With t = max(1 - s, 0) and g the upstream gradient it accumulates
+// sum t^2 g, and over the row sum t g and sum t g k (k the pixel offset); the caller folds
+// those into the photon's moments. Unrolled by two; n is nearly always warp-uniform.
+__device__ __forceinline__ void bwd_row(int n, const float* q, float k0, float b0, float b1,
+                                        float a00, float a10, float& sE, float& A0, float& B1,
+                                        float& B2) {
+    float kf = 0.f;
+    int k = 0;
+    for (; k + 1 < n; k += 2) {
+        const float u0 = fmaf(kf, a00, b0), u1 = fmaf(kf, a10, b1);
+        const float v0 = u0 + a00, v1 = u1 + a10;
+        const float s = fmaf(u0, u0, u1 * u1), s2 = fmaf(v0, v0, v1 * v1);
+        const float t = fmaxf(1.f - s, 0.f), t2 = fmaxf(1.f - s2, 0.f);
+        const float g = t * q[k], g2 = t2 * q[k + 1];
+        const float kk = k0 + kf;
+        sE = fmaf(t, g, sE);
+        sE = fmaf(t2, g2, sE);
+        A0 += g + g2;
+        const float tk = g * kk, tk2 = g2 * (kk + 1.f);
+        B1 += tk + tk2;
+        B2 = fmaf(tk, kk, B2);
+        B2 = fmaf(tk2, kk + 1.f, B2);
+        kf += 2.f;
+    }
+    if (k < n) {
+        const float u0 = fmaf(kf, a00, b0), u1 = fmaf(kf, a10, b1);
+        const float s = fmaf(u0, u0, u1 * u1);
+        const float t = fmaxf(1.f - s, 0.f);
+        const float g = t * q[k];
+        const float kk = k0 + kf;
+        sE = fmaf(t, g, sE);
+        A0 += g;
+        const float tk = g * kk;
+        B1 += tk;
+        B2 = fmaf(tk, kk, B2);
+    }
+}
+
 // Backward gather of one photon (photon_differentials.cu:169-218) from the staged gradient.
 // Pixels outside the support contribute 0 * g in the reference; with spans on they are not
-// visited.
+// visited. The offset d of pixel (kx, ky) is (kx sx + dx0, ky sy + dy0); moments in x are
+// kept in the integer offset kx and converted once per photon.
 __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                        const float* tg, uint32_t rid, const TileArgs& a) {
     const uint32_t p = r.packed;
@@ -375,7 +522,7 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
     const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
     int ky0 = y0 - pyc, ky1 = y1 - pyc;
     support_rows(sup, r.dy0, ti.isy, ky0, ky1);
-    float sE = 0.f, Sx = 0.f, Sy = 0.f, Sxx = 0.f, Sxy = 0.f, Syy = 0.f;
+    float sE = 0.f, A0t = 0.f, B1t = 0.f, B2 = 0.f, Sy = 0.f, Sxy = 0.f, Syy = 0.f;
     for (int ky = ky0; ky <= ky1; ++ky) {
         const float dy = fmaf(float(ky), ti.sy, r.dy0);
         int kx0 = x0 - pxc, kx1 = x1 - pxc;
@@ -383,47 +530,84 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
         const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
         const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
         const float* q = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
-        float A0 = 0.f, A1 = 0.f, A2 = 0.f;
+        float A0 = 0.f, B1 = 0.f;
         if (all) {
-            float kf = float(kx0);
-            const int n = kx1 - kx0 + 1;
-#pragma unroll 2
-            for (int k = 0; k < n; ++k) {
-                const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
-                const float s = fmaf(u0, u0, u1 * u1);
-                const float t = s < 1.f ? 1.f - s : 0.f;
-                const float tgv = t * q[kx0 + k];
-                const float dx = fmaf(kf, ti.sx, r.dx0);
-                sE = fmaf(t, tgv, sE);
-                A0 += tgv;
-                const float adx = tgv * dx;
-                A1 += adx;
-                A2 = fmaf(adx, dx, A2);
-                kf += 1.f;
-            }
+            const float kf = float(kx0);
+            bwd_row(kx1 - kx0 + 1, q + kx0, kf, fmaf(kf, a00, c0), fmaf(kf, a10, c1), a00, a10,
+                    sE, A0, B1, B2);
         } else {
             for (int kx = kx0; kx <= kx1; ++kx) {
                 if (!ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
                 const float kf = float(kx);
                 const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
                 const float s = fmaf(u0, u0, u1 * u1);
-                const float t = s < 1.f ? 1.f - s : 0.f;
+                const float t = fmaxf(1.f - s, 0.f);
                 const float tgv = t * q[kx];
-                const float dx = fmaf(kf, ti.sx, r.dx0);
                 sE = fmaf(t, tgv, sE);
                 A0 += tgv;
-                const float adx = tgv * dx;
-                A1 += adx;
-                A2 = fmaf(adx, dx, A2);
+                const float tk = tgv * kf;
+                B1 += tk;
+                B2 = fmaf(tk, kf, B2);
             }
         }
-        Sx += A1;
+        A0t += A0;
+        B1t += B1;
+        const float sdx = fmaf(ti.sx, B1, r.dx0 * A0);  // sum t g dx over the row
         Sy = fmaf(dy, A0, Sy);
-        Sxx += A2;
-        Sxy = fmaf(dy, A1, Sxy);
+        Sxy = fmaf(dy, sdx, Sxy);
         Syy = fmaf(dy * dy, A0, Syy);
     }
+    const float Sx = fmaf(ti.sx, B1t, r.dx0 * A0t);
+    const float Sxx = fmaf(ti.sx * ti.sx, B2, fmaf(2.f * ti.sx * r.dx0, B1t, r.dx0 * r.dx0 * A0t));
     finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+}
+
+// Backward gather of one photon by the whole warp (see use_coop): lanes take rows and walk
+// their support spans, and a warp reduction hands the moments to the owning lane.
+__device__ __forceinline__ void gather_coop(const Rec& r, const TileInfo& ti, int sw,
+                                            const float* tg, uint32_t rid, int owner,
+                                            const TileArgs& a) {
+    const int lane = threadIdx.x & 31;
+    int pxc, pyc, x0, x1, y0, y1;
+    rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
+    const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, true);
+    int ky0 = y0 - pyc, ky1 = y1 - pyc;
+    support_rows(sup, r.dy0, ti.isy, ky0, ky1);
+    float sE = 0.f, A0t = 0.f, B1t = 0.f, B2 = 0.f, Sy = 0.f, Sxy = 0.f, Syy = 0.f;
+    for (int ky = ky0 + lane; ky <= ky1; ky += 32) {
+        const float dy = fmaf(float(ky), ti.sy, r.dy0);
+        int kx0 = x0 - pxc, kx1 = x1 - pxc;
+        if (!support_cols(sup, dy, r.dx0, ti.isx, kx0, kx1)) continue;
+        const float c0 = fmaf(r.m00, r.dx0, r.m01 * dy);
+        const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
+        const float* q = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
+        float A0 = 0.f, B1 = 0.f;
+        const float kf = float(kx0);
+        bwd_row(kx1 - kx0 + 1, q + kx0, kf, fmaf(kf, a00, c0), fmaf(kf, a10, c1), a00, a10, sE,
+                A0, B1, B2);
+        A0t += A0;
+        B1t += B1;
+        const float sdx = fmaf(ti.sx, B1, r.dx0 * A0);
+        Sy = fmaf(dy, A0, Sy);
+        Sxy = fmaf(dy, sdx, Sxy);
+        Syy = fmaf(dy * dy, A0, Syy);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        sE += __shfl_xor_sync(0xFFFFFFFFu, sE, off);
+        A0t += __shfl_xor_sync(0xFFFFFFFFu, A0t, off);
+        B1t += __shfl_xor_sync(0xFFFFFFFFu, B1t, off);
+        B2 += __shfl_xor_sync(0xFFFFFFFFu, B2, off);
+        Sy += __shfl_xor_sync(0xFFFFFFFFu, Sy, off);
+        Sxy += __shfl_xor_sync(0xFFFFFFFFu, Sxy, off);
+        Syy += __shfl_xor_sync(0xFFFFFFFFu, Syy, off);
+    }
+    if (lane == owner) {
+        const float Sx = fmaf(ti.sx, B1t, r.dx0 * A0t);
+        const float Sxx = fmaf(ti.sx * ti.sx, B2, fmaf(2.f * ti.sx * r.dx0, B1t, r.dx0 * r.dx0 * A0t));
+        finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+    }
 }
 
 template <int NT, int MINB>
@@ -442,7 +626,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
             const int64_t i = base + threadIdx.x;
             const bool have = i < p1;
             uint32_t key = 0xFFFFFFFFu, rid = 0;
-            Rec r;
+            Rec r = {};
             if (have) {
                 key = a.skeys[i] >> cb;
                 rid = a.sidx[i];
@@ -459,7 +643,13 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
                     loaded = cur;
                 }
                 const bool mine = have && key == cur;
-                if (mine) gather(r, ti, sw, cfg.spans, tg, rid, a);
+                const bool coop = mine && use_coop(r, cfg.coop_r);
+                if (mine && !coop) gather(r, ti, sw, cfg.spans, tg, rid, a);
+                for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
+                    const int src = __ffs(cm) - 1;
+                    const Rec rb = shfl_rec(r, src);
+                    gather_coop(rb, ti, sw, tg, __shfl_sync(0xFFFFFFFFu, rid, src), src, a);
+                }
                 done += __syncthreads_count(mine);
                 const int64_t nxt = base + done;
                 if (nxt >= bend) break;

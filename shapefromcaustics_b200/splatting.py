@@ -31,10 +31,11 @@ def default_config():
     return _default_cfg
 
 
-def set_default_config(tile=0, chunk=0, class_bits=0, apron_max=0, walk=0, min_blocks=0):
-    """Tuning used by calls that pass no config (zeros select the library defaults)."""
+def set_default_config(**fields):
+    """Tuning used by calls that pass no config (``pds_config`` fields; zeros or absent
+    fields select the library defaults)."""
     global _default_cfg
-    _default_cfg = _lib.config(tile, chunk, class_bits, apron_max, walk, min_blocks)
+    _default_cfg = _lib.config(**fields)
 
 
 def _check_input(t, name):

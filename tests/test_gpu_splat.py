@@ -71,7 +71,9 @@ def test_uniform_cluster_512(cuda):
 @pytest.mark.parametrize("cfg", [dict(tile=16), dict(tile=32), dict(chunk=256),
                                  dict(class_bits=-1), dict(class_bits=4, chunk=4096),
                                  dict(tile=32, apron_max=3), dict(walk=2),
-                                 dict(walk=2, tile=16, class_bits=1), dict(min_blocks=2)])
+                                 dict(walk=2, tile=16, class_bits=1), dict(min_blocks=2),
+                                 dict(coop_radius=1), dict(coop_radius=-1),
+                                 dict(coop_radius=2, min_blocks=2)])
 def test_tuning_variants(cuda, cfg):
     ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
     assert_parity(ph, (1, 256, 256), 20, cfg=cfg)
@@ -89,6 +91,13 @@ def test_wide_footprints_take_the_direct_path(cuda):
     # radii up to 40 px > apron_max (8): direct path; mpr 30 truncates some boxes
     ph = S.uniform_cluster_photons(3000, 128, 128, seed=3, s_range=(0.5, 40.0))
     assert_parity(ph, (1, 128, 128), 30, cfg=dict(apron_max=8))
+
+
+@pytest.mark.parametrize("coop", [3, -1])
+def test_caustic_curves_large_footprints(cuda, coop):
+    # the contention workload's shape at a small size: most photons on thin curves
+    ph = S.caustic_curve_photons(2 ** 16, 256, 256, seed=13, s_range=(0.25, 16.0))
+    assert_parity(ph, (1, 256, 256), 20, cfg=dict(coop_radius=coop))
 
 
 def test_photons_partly_and_fully_off_image(cuda):
