@@ -52,9 +52,10 @@ typedef struct pds_config {
     int32_t apron_max;  /* largest footprint radius (px) the tile path holds (default 32);
                            larger footprints take the direct path */
     int32_t walk;       /* pixels visited per photon: 1 = the reference's whole box,
-                           2 = only the rows / row spans that can hold the kernel's support
-                           (same result: pixels outside the support add exactly zero);
-                           default 1 */
+                           2 = only the rows / row spans that can hold the kernel's support,
+                           3 = a sheared band of equal-width rows around the support
+                           (2 and 3 give the same result: pixels outside the support add
+                           exactly zero); default 1 */
     int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2 (more
                            registers per thread) or 3 (more warps); default 3 */
     int32_t coop_radius; /* footprints with a radius (px) of at least this are splatted by a

@@ -58,8 +58,9 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.coop_radius must be -1 or in [1, 63]");
     if (out.min_blocks != 2 && out.min_blocks != 3)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.min_blocks must be 2 or 3");
-    if (out.walk != 1 && out.walk != 2)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.walk must be 1 (box) or 2 (spans)");
+    if (out.walk < 1 || out.walk > 3)
+        return fail(PDS_ERR_INVALID_ARGUMENT,
+                    "pds_config.walk must be 1 (box), 2 (support spans) or 3 (support band)");
     if (out.tile != 16 && out.tile != 32 && out.tile != 64)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.tile must be 16, 32 or 64");
     if (out.chunk < 256 || out.chunk > (1 << 20) || out.chunk % 256 != 0)
@@ -89,6 +90,7 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     // odd pitch: the rows of one column of the accumulator fall in different banks
     r.cfg.sw = (c.tile + 2 * r.cfg.apron) | 1;
     r.cfg.spans = c.walk == 2 ? 1 : 0;
+    r.cfg.band = c.walk == 3 ? 1 : 0;
     r.cfg.min_blocks = c.min_blocks;
     r.cfg.coop_r = c.coop_radius > 0 ? c.coop_radius : 0;
     r.key_big = uint32_t(uint64_t(n_tiles) << c.class_bits);
@@ -264,6 +266,7 @@ int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.srecs = b.srecs;
     a.stage = b.stage;
     a.counters = b.counters;
+    a.queue = b.counters + 4;  // [0..3) plan counters; [4] the tile kernels' work counter
     return PDS_OK;
 }
 
@@ -276,6 +279,7 @@ int forward_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tile
     if (rc) return rc;
     a.out = out;
     cudaError_t e = cudaMemsetAsync(out, 0, size_t(image_elems) * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "forward: output reset");
     if (ph.n == 0) return PDS_OK;
     e = pds::launch_forward(a, s);
@@ -296,7 +300,9 @@ int backward_impl(const float* grad, const pds::Photons& ph, const pds::SimTable
     a.gE = gE;
     a.gX = gX;
     a.gM = gM;
-    cudaError_t e = pds::launch_backward(a, s);
+    cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "backward: work counter reset");
+    e = pds::launch_backward(a, s);
     if (e != cudaSuccess) return cuda_fail(e, "bwd_tiles_kernel");
     return PDS_OK;
 }

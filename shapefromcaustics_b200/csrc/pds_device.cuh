@@ -65,6 +65,7 @@ struct Cfg {
     int32_t apron;       // min(max_pixel_radius, apron_max), >= 0
     int32_t sw;          // tile + 2 * apron: edge of the shared accumulator
     int32_t spans;       // 1: walk only the support's rows / row spans; 0: the whole box
+    int32_t band;        // 1: walk each footprint's sheared band (see Band)
     int32_t min_blocks;  // resident CTAs per SM the tile kernels' register budget targets
     int32_t coop_r;      // footprint radius from which a photon is splatted by a whole warp
 };
@@ -205,6 +206,48 @@ __device__ __forceinline__ bool support_cols(const Support& g, float dy, float d
     kx0 = max(kx0, __float2int_ru((lo - dx0) * inv_sx) - 1);
     kx1 = min(kx1, __float2int_rd((hi - dx0) * inv_sx) + 1);
     return kx0 <= kx1;
+}
+
+// Band: the support |M d| < 1 covered by a sheared parallelogram whose rows all have the
+// same width. Row ky (pixel offset from the centre pixel) of the support is centred on the
+// column alpha + beta ky and at most hw pixels wide on either side (the half-width of the
+// row quadratic, sqrt(a - det^2 dy^2) / a, is largest on the centre line: 1 / sqrt(a)); its
+// pixels lie in columns xs(ky) .. xs(ky) + bw - 1 with xs = floor(alpha + beta ky - hw) and
+// bw = floor(2 hw) + 2. The band is ~4/pi of the support's area (plus a column), where the
+// reference's box can be 40 times it for thin rotated footprints. Pixels whose float s is
+// below 1 only by rounding at the support's edge may fall outside; they add (1 - s)^2 ~ 0.
+// Degenerate, near-singular or non-finite M: on = false (walk the box).
+struct Band {
+    bool on;
+    int ky0, ky1;  // support rows
+    float alpha, beta, hw;
+    int bw;
+};
+
+__device__ __forceinline__ Band make_band(float m00, float m01, float m10, float m11, float dx0,
+                                          float dy0, float sy, float isx, float isy) {
+    Band b;
+    b.on = false;
+    const float a = fmaf(m00, m00, m10 * m10);
+    const float det = fmaf(m00, m11, -m01 * m10);
+    const float ey = sqrtf(a) / fabsf(det);
+    if (!(a > 0.f) || !isfinite(a) || !isfinite(ey)) return b;
+    if (!(fabsf(det) > 1e-3f * (fabsf(m00 * m11) + fabsf(m01 * m10)))) return b;
+    const float bco = fmaf(m00, m01, m10 * m11);
+    const float ia = 1.f / a;
+    b.hw = isx * sqrtf(ia);
+    if (!(b.hw < 1e6f) || !(ey * isy < 1e6f)) return b;
+    b.on = true;
+    b.ky0 = __float2int_ru((-ey - dy0) * isy);
+    b.ky1 = __float2int_rd((ey - dy0) * isy);
+    b.alpha = (-bco * dy0 * ia - dx0) * isx;
+    b.beta = -bco * sy * isx * ia;
+    b.bw = __float2int_rd(2.f * b.hw) + 2;
+    return b;
+}
+
+__device__ __forceinline__ int band_start(const Band& b, int ky) {
+    return __float2int_rd(fmaf(float(ky), b.beta, b.alpha - b.hw));
 }
 
 // delta = (2 p_c / w - 1) - x in double, rounded once to float.

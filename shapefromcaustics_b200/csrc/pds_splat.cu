@@ -66,7 +66,22 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
                     const int tx = pcx / T, ty = pcy / T;
                     const uint32_t tile = uint32_t(sim.tile_base) +
                                           uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
-                    const uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
+                    uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
+                    if (a.cfg.band) {
+                        // photons of a warp then have similar band areas (trip counts)
+                        const float sx = float(2.0 / double(sim.width)),
+                                    sy = float(2.0 / double(sim.height));
+                        const float dx0 = corner_offset(f.px_c, sim.width, x);
+                        const float dy0 = corner_offset(f.py_c, sim.height, y);
+                        const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy,
+                                                  0.5f * float(sim.width), 0.5f * float(sim.height));
+                        (void)sx;
+                        int area = (2 * f.rx + 1) * (2 * f.ry + 1);
+                        if (bd.on && f.ellipse_all)
+                            area = min(area, (min(bd.ky1, f.ry) - max(bd.ky0, -f.ry) + 1) * bd.bw);
+                        const int lg = 31 - __clz(max(area, 1));
+                        cls = min(uint32_t(max(lg - 1, 0)), cls_max);
+                    }
                     key = (tile << cb) | cls;
                     const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) |
                                            (e > 0.f ? 0u : kFlagFwdSkip);
@@ -175,13 +190,54 @@ __device__ __forceinline__ void fwd_row(int n, uint32_t a, float b0, float b1, f
     }
 }
 
+// Forward deposit of one photon over its band (see Band): one flattened loop over
+// rows x bw pixels, so the trip count depends only on the band's area (photons of a warp
+// share an area class), the row changing every bw steps. Pixels outside the reference's
+// clipped box are masked off (their add is predicated away).
+__device__ __forceinline__ void deposit_band(const Rec& r, const Band& bd, const TileInfo& ti,
+                                             int sw, uint32_t acc_base, int pxc, int pyc, int x0,
+                                             int x1, int y0, int y1) {
+    const int ky0 = max(bd.ky0, y0 - pyc), ky1 = min(bd.ky1, y1 - pyc);
+    if (ky0 > ky1) return;
+    const int kxb0 = x0 - pxc;
+    const uint32_t kxspan = uint32_t(x1 - x0);
+    const float e3 = r.e * kThreeOverPi;
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
+    const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
+    const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
+    const int bw = bd.bw;
+    const int total = (ky1 - ky0 + 1) * bw;
+    int ky = ky0, c = 0;
+    int xs = band_start(bd, ky);
+    float c0 = fmaf(float(ky), m01sy, c00), c1 = fmaf(float(ky), m11sy, c10);
+    uint32_t row = acc_base + 4u * uint32_t((pyc + ky - ti.oy) * sw + (pxc - ti.ox));
+    for (int q = 0; q < total; ++q) {
+        const int kx = xs + c;
+        const bool in = uint32_t(kx - kxb0) <= kxspan;
+        const float kf = float(kx);
+        const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
+        const float s = fmaf(u0, u0, u1 * u1);
+        const float t = 1.f - s;
+        red_shared_inside<0>(row + 4u * uint32_t(kx), in ? s : 2.f, (t * e3) * t);
+        if (++c == bw) {
+            c = 0;
+            ++ky;
+            xs = band_start(bd, ky);
+            c0 += m01sy;
+            c1 += m11sy;
+            row += 4u * uint32_t(sw);
+        }
+    }
+}
+
 // Forward deposit of one photon into the shared accumulator (photon_differentials.cu:91-110).
 // With spans on, only the support's rows and row spans are visited; the other box pixels
 // add exactly zero in the reference (value > 0 fails, :106). Photons that fail the
 // reference's image-half-size ellipse test somewhere in their box (tiny images only) take
 // the per-pixel test path.
 __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
-                                        float* acc, int& bx0, int& bx1, int& by0, int& by1) {
+                                        bool band, float* acc, int& bx0, int& bx1, int& by0,
+                                        int& by1) {
     const uint32_t p = r.packed;
     const uint32_t fl = rec_flags(p);
     if (fl & kFlagFwdSkip) return;
@@ -192,6 +248,14 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
     bx0 = x0; bx1 = x1; by0 = y0; by1 = y1;
     const float e3 = r.e * kThreeOverPi;
     const bool all = fl & kFlagEllipseAll;
+    if (band && all) {
+        const Band bd = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy);
+        if (bd.on) {
+            deposit_band(r, bd, ti, sw, static_cast<uint32_t>(__cvta_generic_to_shared(acc)), pxc,
+                         pyc, x0, x1, y0, y1);
+            return;
+        }
+    }
     const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
     const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
     const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
@@ -366,6 +430,16 @@ __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& t
     __syncthreads();
 }
 
+// Next chunk of sorted photons for this CTA: a shared work counter (reset to zero before the
+// launch) hands chunks out in order as CTAs finish, so CTAs that drew chunks of large
+// footprints do not hold up the others. Nothing waits on it.
+__device__ __forceinline__ int64_t next_chunk(uint32_t* queue, uint32_t* slot) {
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = atomicAdd(queue, 1u);
+    __syncthreads();
+    return int64_t(*slot);
+}
+
 template <int NT, int MINB>
 __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     extern __shared__ float acc[];
@@ -380,7 +454,9 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     const uint32_t acc_base = static_cast<uint32_t>(__cvta_generic_to_shared(acc));
     const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
-    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    __shared__ uint32_t chunk_slot;
+    for (int64_t c = next_chunk(a.queue, &chunk_slot); c < nchunks;
+         c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
         uint32_t cur = a.skeys[p0] >> cb;
         TileInfo ti = decode_tile(a.sims, cur, cfg);
@@ -403,7 +479,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
                 const bool mine = have && key == cur;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-                if (mine && !coop) deposit(r, ti, sw, cfg.spans, acc, x0, x1, y0, y1);
+                if (mine && !coop) deposit(r, ti, sw, cfg.spans, cfg.band, acc, x0, x1, y0, y1);
                 if (coop) {
                     int pxc, pyc;
                     rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
@@ -505,12 +581,70 @@ __device__ __forceinline__ void bwd_row(int n, const float* q, float k0, float b
     }
 }
 
+// Backward gather of one photon over its band (see Band and deposit_band). Per row it keeps
+// sum t g and sum t g kx (kx the integer pixel offset) and folds them at the row change;
+// sum t g kx^2 and sum t^2 g run over the whole band.
+__device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const TileInfo& ti,
+                                            int sw, const float* tg, uint32_t rid, int pxc,
+                                            int pyc, int x0, int x1, int y0, int y1,
+                                            const TileArgs& a) {
+    const int ky0 = max(bd.ky0, y0 - pyc), ky1 = min(bd.ky1, y1 - pyc);
+    const int kxb0 = x0 - pxc;
+    const uint32_t kxspan = uint32_t(x1 - x0);
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
+    const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
+    const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
+    const int bw = bd.bw;
+    const int total = ky0 <= ky1 ? (ky1 - ky0 + 1) * bw : 0;
+    float sE = 0.f, A0t = 0.f, B1t = 0.f, B2 = 0.f, Sy = 0.f, Sxy = 0.f, Syy = 0.f;
+    float A0 = 0.f, B1 = 0.f;
+    int ky = ky0, c = 0;
+    int xs = band_start(bd, ky);
+    float c0 = fmaf(float(ky), m01sy, c00), c1 = fmaf(float(ky), m11sy, c10);
+    const float* row = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
+    for (int q = 0; q < total; ++q) {
+        const int kx = xs + c;
+        const bool in = uint32_t(kx - kxb0) <= kxspan;
+        const float kf = float(kx);
+        const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
+        const float s = fmaf(u0, u0, u1 * u1);
+        const float t = in ? fmaxf(1.f - s, 0.f) : 0.f;
+        const float g = t * (in ? row[kx] : 0.f);
+        sE = fmaf(t, g, sE);
+        A0 += g;
+        const float tk = g * kf;
+        B1 += tk;
+        B2 = fmaf(tk, kf, B2);
+        if (++c == bw) {
+            const float dy = fmaf(float(ky), ti.sy, r.dy0);
+            const float sdx = fmaf(ti.sx, B1, r.dx0 * A0);
+            Sy = fmaf(dy, A0, Sy);
+            Sxy = fmaf(dy, sdx, Sxy);
+            Syy = fmaf(dy * dy, A0, Syy);
+            A0t += A0;
+            B1t += B1;
+            A0 = 0.f;
+            B1 = 0.f;
+            c = 0;
+            ++ky;
+            xs = band_start(bd, ky);
+            c0 += m01sy;
+            c1 += m11sy;
+            row += sw;
+        }
+    }
+    const float Sx = fmaf(ti.sx, B1t, r.dx0 * A0t);
+    const float Sxx = fmaf(ti.sx * ti.sx, B2, fmaf(2.f * ti.sx * r.dx0, B1t, r.dx0 * r.dx0 * A0t));
+    finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+}
+
 // Backward gather of one photon (photon_differentials.cu:169-218) from the staged gradient.
 // Pixels outside the support contribute 0 * g in the reference; with spans on they are not
 // visited. The offset d of pixel (kx, ky) is (kx sx + dx0, ky sy + dy0); moments in x are
 // kept in the integer offset kx and converted once per photon.
 __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
-                                       const float* tg, uint32_t rid, const TileArgs& a) {
+                                       bool band, const float* tg, uint32_t rid,
+                                       const TileArgs& a) {
     const uint32_t p = r.packed;
     const uint32_t fl = rec_flags(p);
     const int pxc = ti.ox + rec_lx(p), pyc = ti.oy + rec_ly(p);
@@ -518,6 +652,13 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
     const int x0 = max(pxc - rx, 0), x1 = min(pxc + rx, ti.W - 1);
     const int y0 = max(pyc - ry, 0), y1 = min(pyc + ry, ti.H - 1);
     const bool all = fl & kFlagEllipseAll;
+    if (band && all) {
+        const Band bd = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy);
+        if (bd.on) {
+            gather_band(r, bd, ti, sw, tg, rid, pxc, pyc, x0, x1, y0, y1, a);
+            return;
+        }
+    }
     const Support sup = make_support(r.m00, r.m01, r.m10, r.m11, spans && all);
     const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
     int ky0 = y0 - pyc, ky1 = y1 - pyc;
@@ -617,7 +758,9 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
     const int sw = cfg.sw, cb = cfg.class_bits;
     const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
-    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    __shared__ uint32_t chunk_slot;
+    for (int64_t c = next_chunk(a.queue, &chunk_slot); c < nchunks;
+         c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
         uint32_t cur = a.skeys[p0] >> cb;
         TileInfo ti = decode_tile(a.sims, cur, cfg);
@@ -644,7 +787,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
                 }
                 const bool mine = have && key == cur;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
-                if (mine && !coop) gather(r, ti, sw, cfg.spans, tg, rid, a);
+                if (mine && !coop) gather(r, ti, sw, cfg.spans, cfg.band, tg, rid, a);
                 for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
                     const int src = __ffs(cm) - 1;
                     const Rec rb = shfl_rec(r, src);

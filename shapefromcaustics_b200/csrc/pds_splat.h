@@ -38,6 +38,7 @@ struct TileArgs {
     const uint32_t* sidx;      // sorted photon indices
     const Rec* srecs;          // records in sorted order
     const uint32_t* counters;
+    uint32_t* queue;           // chunk work counter of the tile kernel (zeroed before launch)
     float* out;                // forward: flat image buffer (zeroed by caller)
     const float* grad;         // backward: flat upstream gradient buffer
     float* gE;                 // backward outputs
