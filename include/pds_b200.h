@@ -55,11 +55,11 @@ typedef struct pds_config {
                            2 = only the rows / row spans that can hold the kernel's support,
                            3 = a sheared band of equal-width rows around the support
                            (2 and 3 give the same result: pixels outside the support add
-                           exactly zero); default 1 */
+                           exactly zero); default 3 */
     int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2 (more
                            registers per thread) or 3 (more warps); default 3 */
     int32_t coop_radius; /* footprints with a radius (px) of at least this are splatted by a
-                           whole warp instead of one thread; -1 never; default 5 */
+                           whole warp instead of one thread; -1 never; default -1 */
 } pds_config;
 
 /* One simulation of a batch. The caller fills photon_begin, n_photons, image_offset,

@@ -51,9 +51,9 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
     out.class_bits = (in && in->class_bits) ? in->class_bits : 3;
     if (out.class_bits == -1) out.class_bits = 0;
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
-    out.walk = (in && in->walk) ? in->walk : 1;
+    out.walk = (in && in->walk) ? in->walk : 3;
     out.min_blocks = (in && in->min_blocks) ? in->min_blocks : 3;
-    out.coop_radius = (in && in->coop_radius) ? in->coop_radius : 5;
+    out.coop_radius = (in && in->coop_radius) ? in->coop_radius : -1;
     if (out.coop_radius < -1 || out.coop_radius > 63)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.coop_radius must be -1 or in [1, 63]");
     if (out.min_blocks != 2 && out.min_blocks != 3)

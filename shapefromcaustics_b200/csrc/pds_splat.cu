@@ -608,8 +608,10 @@ __device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const 
         const float kf = float(kx);
         const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
         const float s = fmaf(u0, u0, u1 * u1);
+        // the load's column is clamped into the box, so it never leaves the staged tile
+        const float gv = row[min(max(kx, kxb0), kxb0 + int(kxspan))];
         const float t = in ? fmaxf(1.f - s, 0.f) : 0.f;
-        const float g = t * (in ? row[kx] : 0.f);
+        const float g = in ? t * gv : 0.f;
         sE = fmaf(t, g, sE);
         A0 += g;
         const float tk = g * kf;
