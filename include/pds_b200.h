@@ -25,6 +25,7 @@
  *   - Photons whose channel lies outside [0, C) contribute nothing and get zero gradients
  *     (the reference checks only c < C, photon_differentials.cu:75, and leaves its
  *     empty_like gradient outputs unwritten for them).
+ *   - A call takes fewer than 2^31 - 1 photons (PDS_ERR_UNSUPPORTED otherwise).
  */
 #ifndef PDS_B200_H
 #define PDS_B200_H

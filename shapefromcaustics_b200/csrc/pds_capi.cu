@@ -3,7 +3,8 @@
 // This layer validates arguments the way the reference's binding does
 // (PyOptix/PhotonDifferentialSplattig.cpp:14-22: matching photon counts, 2-row positions,
 // 2x3 matrices, one channel row), lays the workspace out, and enqueues
-//   plan:     counters reset, plan_kernel, radix sort, sort_records_kernel
+//   plan:     counter and bucket-count reset, plan_kernel, bucket scan, bucket_scatter,
+//             chunk_tile_kernel
 //   forward:  output reset, fwd_tiles_kernel, tail_fwd_kernel
 //   backward: bwd_tiles_kernel, tail_bwd_kernel, grad_scatter_kernel
 // on the caller's stream. It allocates nothing and never synchronises. Failures return a
@@ -30,18 +31,9 @@ int cuda_fail(cudaError_t e, const char* where) {
     return PDS_ERR_CUDA;
 }
 
-int bit_length(uint64_t v) {
-    int b = 0;
-    while (v) {
-        ++b;
-        v >>= 1;
-    }
-    return b;
-}
-
 struct Resolved {
     pds::Cfg cfg;
-    int key_bits;
+    int64_t n_buckets;
     uint32_t key_big, key_invalid;
 };
 
@@ -93,72 +85,81 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     r.cfg.band = c.walk == 3 ? 1 : 0;
     r.cfg.min_blocks = c.min_blocks;
     r.cfg.coop_r = c.coop_radius > 0 ? c.coop_radius : 0;
-    r.key_big = uint32_t(uint64_t(n_tiles) << c.class_bits);
+    r.n_buckets = n_tiles << c.class_bits;
+    r.key_big = uint32_t(r.n_buckets);
     r.key_invalid = uint32_t(inv);
-    r.key_bits = bit_length(inv);
     return PDS_OK;
 }
 
-// recs holds the plan's records in photon order until they are copied into srecs in sorted
-// order; it is then free, and the backward reuses it for its per-photon gradient records.
+// The plan's workspace. recs holds the records in photon order until bucket_scatter has copied
+// them into srecs in sorted order; it is then free, and the backward reuses it for its
+// gradient records.
 struct Layout {
-    size_t counters, k0, k1, v0, v1, recs, srecs, aux, total;
+    size_t counters, keys, inv, wide, recs, srecs, counts, start, cursor, part, chunk_tile,
+        total;
 };
 
-Layout make_layout(int64_t n) {
+// Photon count n, bucket count nb (tiles << class bits).
+Layout make_layout(int64_t n, int64_t nb) {
     Layout L;
     const size_t nn = size_t(n > 0 ? n : 1);
+    const size_t nbb = size_t(nb > 0 ? nb : 1);
     size_t off = 0;
     L.counters = off; off += 256;
-    L.k0 = off; off += pds::align_up(nn * 4, 256);
-    L.k1 = off; off += pds::align_up(nn * 4, 256);
-    L.v0 = off; off += pds::align_up(nn * 4, 256);
-    L.v1 = off; off += pds::align_up(nn * 4, 256);
+    L.keys = off; off += pds::align_up(nn * 4, 256);
+    L.inv = off; off += pds::align_up(nn * 4, 256);
+    L.wide = off; off += pds::align_up(nn * 4, 256);
     L.recs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
     L.srecs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
-    L.aux = off; off += pds::sort_aux_bytes(n);
+    L.counts = off; off += pds::align_up(nbb * 4, 256);
+    L.start = off; off += pds::align_up((nbb + 1) * 4, 256);
+    L.cursor = off; off += pds::align_up(nbb * 4, 256);
+    L.part = off; off += pds::align_up(size_t(pds::bucket_scan_parts(int64_t(nbb))) * 4, 256);
+    L.chunk_tile = off; off += pds::align_up((nn / 256 + 2) * 4, 256);  // chunks >= 256
     L.total = off;
     return L;
 }
 
 struct Bufs {
     uint32_t* counters;
-    uint32_t *k0, *k1, *v0, *v1;
+    uint32_t *keys, *inv, *wide, *counts, *start, *cursor, *part, *chunk_tile;
     pds::Rec* recs;
     pds::Rec* srecs;
     pds::GradRec* stage;
-    void* aux;
 };
 
 Bufs bufs(void* ws, const Layout& L) {
     char* b = static_cast<char*>(ws);
     Bufs r;
     r.counters = reinterpret_cast<uint32_t*>(b + L.counters);
-    r.k0 = reinterpret_cast<uint32_t*>(b + L.k0);
-    r.k1 = reinterpret_cast<uint32_t*>(b + L.k1);
-    r.v0 = reinterpret_cast<uint32_t*>(b + L.v0);
-    r.v1 = reinterpret_cast<uint32_t*>(b + L.v1);
+    r.keys = reinterpret_cast<uint32_t*>(b + L.keys);
+    r.inv = reinterpret_cast<uint32_t*>(b + L.inv);
+    r.wide = reinterpret_cast<uint32_t*>(b + L.wide);
+    r.counts = reinterpret_cast<uint32_t*>(b + L.counts);
+    r.start = reinterpret_cast<uint32_t*>(b + L.start);
+    r.cursor = reinterpret_cast<uint32_t*>(b + L.cursor);
+    r.part = reinterpret_cast<uint32_t*>(b + L.part);
+    r.chunk_tile = reinterpret_cast<uint32_t*>(b + L.chunk_tile);
     r.recs = reinterpret_cast<pds::Rec*>(b + L.recs);
     r.srecs = reinterpret_cast<pds::Rec*>(b + L.srecs);
     r.stage = reinterpret_cast<pds::GradRec*>(b + L.recs);
     static_assert(sizeof(pds::GradRec) == sizeof(pds::Rec), "gradient records reuse recs");
-    r.aux = b + L.aux;
     return r;
 }
 
-// The plan kernel writes raw keys into k1; pass p of the sort writes buffer (p & 1).
-void sorted_bufs(const Bufs& b, int key_bits, const uint32_t** keys, const uint32_t** idx) {
-    const int passes = pds::sort_passes(key_bits);
-    const bool in0 = passes == 0 || ((passes - 1) & 1) == 0;
-    *keys = in0 ? b.k0 : b.k1;
-    *idx = in0 ? b.v0 : b.v1;
+// Bucket count of a configuration over n_tiles tiles (0 when the configuration is invalid;
+// the entry points report that).
+int64_t bucket_count(const pds_config* cfg, int64_t n_tiles) {
+    pds_config c;
+    if (resolve_cfg(cfg, c) != PDS_OK || n_tiles < 1 || n_tiles >= (int64_t(1) << 30)) return 0;
+    return n_tiles << c.class_bits;
 }
 
 int check_photons(const float* E, const float* X, const float* M, const int64_t* cp,
                   const float* R, int64_t n) {
     if (n < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative photon count");
-    if (n >= int64_t(0xFFFFFFFFll))
-        return fail(PDS_ERR_UNSUPPORTED, "photon count must be below 2^32 - 1");
+    if (n >= int64_t(0x7FFFFFFFll))
+        return fail(PDS_ERR_UNSUPPORTED, "photon count must be below 2^31 - 1");
     if (n > 0 && (!E || !X || !M || !cp || !R))
         return fail(PDS_ERR_INVALID_ARGUMENT, "null photon array");
     return PDS_OK;
@@ -221,13 +222,13 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     Resolved r;
     int rc = resolve(cfg, mpr, n_tiles, r);
     if (rc) return rc;
-    const Layout L = make_layout(ph.n);
+    const Layout L = make_layout(ph.n, r.n_buckets);
     rc = check_ws(ws, ws_bytes, L.total);
     if (rc) return rc;
     const Bufs b = bufs(ws, L);
     cudaError_t e = cudaMemsetAsync(b.counters, 0, 16, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.counts, 0, size_t(r.n_buckets) * 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "plan: counter reset");
-    if (ph.n == 0) return PDS_OK;
     pds::PlanArgs a;
     a.ph = ph;
     a.sims = st;
@@ -235,16 +236,36 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.cfg = r.cfg;
     a.key_big = r.key_big;
     a.key_invalid = r.key_invalid;
-    a.keys = b.k1;
+    a.keys = b.keys;
     a.recs = b.recs;
+    a.counts = b.counts;
+    a.inv = b.inv;
+    a.wide = b.wide;
     a.counters = b.counters;
+    a.range = pds::plan_range(ph.n);
     e = pds::launch_plan(a, s);
     if (e != cudaSuccess) return cuda_fail(e, "plan_kernel");
-    uint32_t *ko, *vo;
-    e = pds::radix_sort(b.k1, b.k0, b.k1, b.v0, b.v1, ph.n, r.key_bits, b.aux, s, &ko, &vo);
-    if (e != cudaSuccess) return cuda_fail(e, "radix sort");
-    e = pds::launch_sort_records(b.recs, vo, b.counters, ph.n, b.srecs, s);
-    if (e != cudaSuccess) return cuda_fail(e, "sort_records_kernel");
+    pds::ScatterArgs sa;
+    sa.sims = st;
+    sa.keys = b.keys;
+    sa.recs = b.recs;
+    sa.counts = b.counts;
+    sa.counters = b.counters;
+    sa.part = b.part;
+    sa.start = b.start;
+    sa.cursor = b.cursor;
+    sa.srecs = b.srecs;
+    sa.inv = b.inv;
+    sa.chunk_tile = b.chunk_tile;
+    sa.n = ph.n;
+    sa.nb = r.n_buckets;
+    sa.n_tiles = n_tiles;
+    sa.range = a.range;
+    sa.key_big = r.key_big;
+    sa.chunk = r.cfg.chunk;
+    sa.cb = r.cfg.class_bits;
+    e = pds::launch_bucket_sort(sa, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bucket sort");
     return PDS_OK;
 }
 
@@ -253,7 +274,7 @@ int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     Resolved r;
     int rc = resolve(cfg, mpr, n_tiles, r);
     if (rc) return rc;
-    const Layout L = make_layout(ph.n);
+    const Layout L = make_layout(ph.n, r.n_buckets);
     rc = check_ws(ws, ws_bytes, L.total);
     if (rc) return rc;
     const Bufs b = bufs(ws, L);
@@ -262,8 +283,12 @@ int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.sims = st;
     a.mpr = mpr;
     a.cfg = r.cfg;
-    sorted_bufs(b, r.key_bits, &a.skeys, &a.sidx);
+    a.n_tiles = n_tiles;
     a.srecs = b.srecs;
+    a.start = b.start;
+    a.chunk_tile = b.chunk_tile;
+    a.inv = b.inv;
+    a.wide = b.wide;
     a.stage = b.stage;
     a.counters = b.counters;
     a.queue = b.counters + 4;  // [0..3) plan counters; [4] the tile kernels' work counter
@@ -335,13 +360,14 @@ const char* pds_last_error(void) { return g_err.c_str(); }
 const char* pds_version(void) { return "pds_b200 1.0 (sm_100a)"; }
 
 size_t pds_workspace_bytes(int64_t n, int64_t C, int64_t H, int64_t W, const pds_config* cfg) {
-    (void)C; (void)H; (void)W; (void)cfg;
-    return make_layout(n).total;
+    pds_config c;
+    if (resolve_cfg(cfg, c) != PDS_OK || C < 1 || H < 1 || W < 1) return make_layout(n, 1).total;
+    const int64_t tiles = C * ((H + c.tile - 1) / c.tile) * ((W + c.tile - 1) / c.tile);
+    return make_layout(n, bucket_count(cfg, tiles)).total;
 }
 
 size_t pds_batch_workspace_bytes(int64_t n_total, int64_t n_tiles_total, const pds_config* cfg) {
-    (void)n_tiles_total; (void)cfg;
-    return make_layout(n_total).total;
+    return make_layout(n_total, bucket_count(cfg, n_tiles_total)).total;
 }
 
 int pds_plan_f32(const float* E, const float* X, const float* M, const int64_t* cp,

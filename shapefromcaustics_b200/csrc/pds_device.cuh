@@ -29,6 +29,11 @@ constexpr float kTwelveOverPi = 3.819718634205488f;    // 12 / pi
 constexpr uint32_t kFlagEllipseAll = 1u;  // :93 test passes for the whole box
 constexpr uint32_t kFlagFwdSkip = 2u;     // E <= 0 or NaN: forward deposits nothing (:106)
 
+// Per-photon slot of the plan's inverse map: a sorted position of the tile path, a wide photon
+// (kWideBit | index into the wide list), or a photon that touches no pixel.
+constexpr uint32_t kWideBit = 0x80000000u;
+constexpr uint32_t kInvalidPos = 0xFFFFFFFFu;
+
 // One photon of the tile path, 32 bytes, written once in photon order by the plan kernel
 // and gathered by sorted index by the tile kernels.
 struct __align__(16) Rec {
@@ -224,19 +229,26 @@ struct Band {
     int bw;
 };
 
+// The band's geometry only has to be right to within its margins (a column and the rows'
+// rounding), so it uses the approximate reciprocal and reciprocal square root.
+// max_hw bounds the band's half-width in pixels (the footprint's box radius plus one): an M
+// whose support is wider than the box the radius gives takes the box walk, which the radius
+// bounds.
 __device__ __forceinline__ Band make_band(float m00, float m01, float m10, float m11, float dx0,
-                                          float dy0, float sy, float isx, float isy) {
+                                          float dy0, float sy, float isx, float isy,
+                                          float max_hw) {
     Band b;
     b.on = false;
     const float a = fmaf(m00, m00, m10 * m10);
     const float det = fmaf(m00, m11, -m01 * m10);
-    const float ey = sqrtf(a) / fabsf(det);
-    if (!(a > 0.f) || !isfinite(a) || !isfinite(ey)) return b;
+    if (!(a > 0.f) || !(a < 1e30f)) return b;
     if (!(fabsf(det) > 1e-3f * (fabsf(m00 * m11) + fabsf(m01 * m10)))) return b;
+    const float ra = rsqrtf(a);                                // 1 / sqrt(a)
+    const float ey = a * ra * __fdividef(1.f, fabsf(det));     // sqrt(a) / |det|
+    const float ia = ra * ra;
+    b.hw = isx * ra;
+    if (!(b.hw <= max_hw) || !(ey * isy < 1e6f)) return b;
     const float bco = fmaf(m00, m01, m10 * m11);
-    const float ia = 1.f / a;
-    b.hw = isx * sqrtf(ia);
-    if (!(b.hw < 1e6f) || !(ey * isy < 1e6f)) return b;
     b.on = true;
     b.ky0 = __float2int_ru((-ey - dy0) * isy);
     b.ky1 = __float2int_rd((ey - dy0) * isy);

@@ -1,0 +1,362 @@
+// Photon binning of the splatting plan, for sm_100a.
+//
+// Reference: PyOptix/kernel/photon_differentials.cu:76-89 (the footprint each photon's
+// threads recompute in both kernels). Here every photon is binned once per plan:
+//
+//   plan_kernel      one pass over the photons (coalesced SoA reads): exact integer footprint,
+//                    a bucket (simulation, channel, screen tile of the centre pixel, footprint
+//                    class) and a 32-byte record in photon order. Each CTA takes a contiguous
+//                    photon range (one or two simulations) and counts its buckets in a
+//                    shared-memory histogram over the window of buckets that starts at its
+//                    first photon's simulation; the histogram is added into the global counts
+//                    once per CTA. Photons wider than the apron go to the wide list.
+//   bucket scan      exclusive scan of the bucket counts (three parallel kernels), giving each
+//                    bucket its first sorted position; a copy serves as the scatter's cursors.
+//   bucket_scatter   the same CTA ranges: each CTA recounts its window, reserves its share of
+//                    every bucket with one atomic on the global cursor, then hands positions
+//                    out from shared memory; each record is copied to its position, and the
+//                    position is kept per photon (coalesced) for the backward's gradient spread.
+//   chunk_tile       the tile holding the first photon of every tile-kernel work chunk.
+//
+// This is a counting sort by bucket: two passes over the photons, no sort passes, and global
+// atomics per CTA and bucket rather than per photon (buckets outside a CTA's window, possible
+// for simulations with more buckets than the window, take one global atomic per photon).
+// Photons of one bucket land in an arbitrary order; every photon's result is independent of it
+// (forward sums are reassociated, as the reference's atomics also do).
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pds_device.cuh"
+#include "pds_internal.h"
+#include "pds_splat.h"
+
+namespace pds {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+constexpr int kWindow = 12160;  // buckets of a CTA's shared histogram (47.5 KB)
+
+// First bucket of the simulation owning photon i.
+__device__ __forceinline__ uint32_t window_base(const SimTable& st, int64_t i, int cb) {
+    return uint32_t(load_sim(st, find_sim_of_photon(st, i)).tile_base) << cb;
+}
+
+__device__ __forceinline__ void zero_window(uint32_t* hist) {
+    for (int j = threadIdx.x; j < kWindow; j += blockDim.x) hist[j] = 0u;
+}
+
+__global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
+    __shared__ uint32_t hist[kWindow];
+    const int64_t n = a.ph.n;
+    const int lane = threadIdx.x & 31;
+    const int64_t r0 = int64_t(blockIdx.x) * a.range, r1 = min(r0 + a.range, n);
+    const uint32_t kb0 = window_base(a.sims, r0, a.cfg.class_bits);
+    zero_window(hist);
+    __syncthreads();
+    uint32_t c_tile = 0, c_inv = 0;
+    const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
+    const uint32_t cls_max = (1u << cb) - 1u;
+    const int64_t* __restrict__ cp = a.ph.cp;
+    const float* __restrict__ X = a.ph.X;
+    const float* __restrict__ R = a.ph.R;
+    const float* __restrict__ E = a.ph.E;
+    const float* __restrict__ M = a.ph.M;
+    // whole warps step together (the wide list's ballot needs every lane)
+    for (int64_t base = r0; base < r1; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const bool valid = i < r1;
+        uint32_t key = a.key_invalid;
+        if (valid) {
+            // all of the photon's inputs are loaded up front (coalesced, one latency round)
+            const int64_t ch = __ldg(cp + i);
+            const float x = __ldg(X + i), y = __ldg(X + n + i), rad = __ldg(R + i);
+            const float e = __ldg(E + i);
+            const float m00 = __ldg(M + i), m01 = __ldg(M + n + i);
+            const float m10 = __ldg(M + 3 * n + i), m11 = __ldg(M + 4 * n + i);
+            const int s = find_sim_of_photon(a.sims, i);
+            const pds_sim sim = load_sim(a.sims, s);
+            if (ch >= 0 && ch < sim.channels) {
+                const Footprint f = make_footprint(x, y, rad, sim.height, sim.width, a.mpr);
+                int32_t x0, x1, y0, y1;
+                if (clip_box(f, sim.height, sim.width, x0, x1, y0, y1)) {
+                    if (f.rx > A || f.ry > A) {
+                        key = a.key_big;
+                    } else {
+                        const int pcx = min(max(f.px_c, 0), sim.width - 1);
+                        const int pcy = min(max(f.py_c, 0), sim.height - 1);
+                        const int tx = pcx / T, ty = pcy / T;
+                        const uint32_t tile =
+                            uint32_t(sim.tile_base) +
+                            uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
+                        const float dx0 = corner_offset(f.px_c, sim.width, x);
+                        const float dy0 = corner_offset(f.py_c, sim.height, y);
+                        uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
+                        if (a.cfg.band) {
+                            // photons of a warp then have similar band areas (trip counts)
+                            const float sy = float(2.0 / double(sim.height));
+                            const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy,
+                                                      0.5f * float(sim.width),
+                                                      0.5f * float(sim.height),
+                                                      float(f.rx) + 1.f);
+                            int area = (2 * f.rx + 1) * (2 * f.ry + 1);
+                            if (bd.on && f.ellipse_all)
+                                area = min(area, (min(bd.ky1, f.ry) - max(bd.ky0, -f.ry) + 1) *
+                                                     bd.bw);
+                            const int lg = 31 - __clz(max(area, 1));
+                            cls = min(uint32_t(max(lg - 1, 0)), cls_max);
+                        }
+                        key = (tile << cb) | cls;
+                        const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) |
+                                               (e > 0.f ? 0u : kFlagFwdSkip);
+                        Rec r;
+                        r.dx0 = dx0;
+                        r.dy0 = dy0;
+                        r.m00 = m00;
+                        r.m01 = m01;
+                        r.m10 = m10;
+                        r.m11 = m11;
+                        r.e = e;
+                        r.packed = pack_rec(f.px_c - (tx * T - A), f.py_c - (ty * T - A), f.rx,
+                                            f.ry, flags);
+                        a.recs[i] = r;
+                    }
+                }
+            }
+            a.keys[i] = key;
+            if (key == a.key_invalid) a.inv[i] = kInvalidPos;
+        }
+        const bool tile_path = key < a.key_big;
+        const bool wide = key == a.key_big;
+        c_tile += tile_path;
+        c_inv += valid && key == a.key_invalid;
+        if (tile_path) {
+            const uint32_t j = key - kb0;
+            if (j < uint32_t(kWindow)) atomicAdd(hist + j, 1u);
+            else atomicAdd(a.counts + key, 1u);
+        }
+        // wide photons: appended to the wide list (one atomic per warp)
+        const uint32_t wm = __ballot_sync(0xFFFFFFFFu, wide);
+        if (wm) {
+            uint32_t wbase = 0;
+            if (lane == __ffs(wm) - 1) wbase = atomicAdd(a.counters + 1, uint32_t(__popc(wm)));
+            wbase = __shfl_sync(0xFFFFFFFFu, wbase, __ffs(wm) - 1);
+            if (wide) {
+                const uint32_t k = wbase + __popc(wm & lanemask_lt());
+                a.wide[k] = uint32_t(i);
+                a.inv[i] = kWideBit | k;
+            }
+        }
+    }
+    // block totals -> the tile-path and untouched counters; the window -> the bucket counts
+    __shared__ uint32_t red[2];
+    if (threadIdx.x < 2) red[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t wend = min(int64_t(kWindow), int64_t(a.key_big) - int64_t(kb0));
+    for (int j = threadIdx.x; j < wend; j += blockDim.x)
+        if (hist[j]) atomicAdd(a.counts + kb0 + j, hist[j]);
+    c_tile = __reduce_add_sync(0xFFFFFFFFu, c_tile);
+    c_inv = __reduce_add_sync(0xFFFFFFFFu, c_inv);
+    if (lane == 0) {
+        atomicAdd(&red[0], c_tile);
+        atomicAdd(&red[1], c_inv);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && red[0]) atomicAdd(a.counters + 0, red[0]);
+    if (threadIdx.x == 1 && red[1]) atomicAdd(a.counters + 2, red[1]);
+}
+
+// ------------------------------------------------------------------ bucket scan --------
+// Exclusive scan of counts[0, nb) into start[0, nb] (start[nb] = the total) and cursor[0, nb):
+// per-CTA sums of kScanItems buckets, one CTA scanning those sums, then each CTA's rescan.
+
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 16;
+constexpr int kScanItems = kScanThreads * kScanPer;
+
+// Exclusive scan of one value per thread over the CTA; *total gets the CTA's sum.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t wsum[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kScanThreads / 32 ? wsum[lane] : 0u;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, off);
+            if (lane >= off) w += y;
+        }
+        if (lane < kScanThreads / 32) wsum[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = warp > 0 ? wsum[warp - 1] : 0u;
+    *total = wsum[kScanThreads / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ __launch_bounds__(kScanThreads) void bucket_reduce(const uint32_t* __restrict__ counts,
+                                                              int64_t nb,
+                                                              uint32_t* __restrict__ part) {
+    const int64_t b0 = int64_t(blockIdx.x) * kScanItems;
+    uint32_t s = 0;
+    for (int k = threadIdx.x; k < kScanItems; k += kScanThreads) {
+        const int64_t j = b0 + k;
+        if (j < nb) s += __ldg(counts + j);
+    }
+    uint32_t total;
+    block_exclusive_scan(s, &total);
+    if (threadIdx.x == 0) part[blockIdx.x] = total;
+}
+
+__global__ __launch_bounds__(kScanThreads) void bucket_top(uint32_t* __restrict__ part,
+                                                           int64_t np, uint32_t* __restrict__ start,
+                                                           int64_t nb) {
+    uint32_t carry = 0;
+    for (int64_t b = 0; b < np; b += kScanThreads) {
+        const int64_t j = b + threadIdx.x;
+        const uint32_t v = j < np ? part[j] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(v, &total);
+        if (j < np) part[j] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) start[nb] = carry;
+}
+
+__global__ __launch_bounds__(kScanThreads) void bucket_down(const uint32_t* __restrict__ counts,
+                                                            int64_t nb,
+                                                            const uint32_t* __restrict__ part,
+                                                            uint32_t* __restrict__ start,
+                                                            uint32_t* __restrict__ cursor) {
+    // thread t owns buckets [b0 + t * kScanPer, + kScanPer)
+    const int64_t b0 = int64_t(blockIdx.x) * kScanItems + int64_t(threadIdx.x) * kScanPer;
+    uint32_t v[kScanPer];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = b0 + k < nb ? __ldg(counts + b0 + k) : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t run = part[blockIdx.x] + block_exclusive_scan(s, &total);
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        if (b0 + k < nb) {
+            start[b0 + k] = run;
+            cursor[b0 + k] = run;
+        }
+        run += v[k];
+    }
+}
+
+// ------------------------------------------------------------------ scatter ------------
+
+__global__ __launch_bounds__(256) void bucket_scatter(ScatterArgs a) {
+    __shared__ uint32_t hist[kWindow];
+    const int64_t r0 = int64_t(blockIdx.x) * a.range, r1 = min(r0 + a.range, a.n);
+    const uint32_t kb0 = window_base(a.sims, r0, a.cb);
+    zero_window(hist);
+    __syncthreads();
+    // the CTA's count per window bucket (as plan_kernel counted them)
+    for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const uint32_t j = __ldg(a.keys + i) - kb0;
+        if (j < uint32_t(kWindow) && j + kb0 < a.key_big) atomicAdd(hist + j, 1u);
+    }
+    __syncthreads();
+    // reserve the CTA's share of each bucket: hist[j] becomes its first position
+    const int64_t wend = min(int64_t(kWindow), int64_t(a.key_big) - int64_t(kb0));
+    for (int j = threadIdx.x; j < wend; j += blockDim.x) {
+        const uint32_t c = hist[j];
+        if (c) hist[j] = atomicAdd(a.cursor + kb0 + j, c);
+    }
+    __syncthreads();
+    for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const uint32_t key = __ldg(a.keys + i);
+        if (key < a.key_big) {
+            const uint32_t j = key - kb0;
+            const uint32_t pos = j < uint32_t(kWindow) ? atomicAdd(hist + j, 1u)
+                                                       : atomicAdd(a.cursor + key, 1u);
+            a.srecs[pos] = a.recs[i];
+            a.inv[i] = pos;
+        }
+    }
+}
+
+// Tile of the first photon of every work chunk: the last tile whose bucket range starts at or
+// before the chunk's first position (empty tiles start where their successor does).
+__global__ __launch_bounds__(256) void chunk_tile_kernel(ScatterArgs a) {
+    const int64_t n_tile = min(int64_t(a.counters[0]), a.n);
+    const int64_t nchunks = (n_tile + a.chunk - 1) / a.chunk;
+    for (int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < nchunks;
+         c += int64_t(gridDim.x) * blockDim.x) {
+        const uint32_t p = uint32_t(c * a.chunk);
+        int64_t lo = 0, hi = a.n_tiles - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(a.start + (mid << a.cb)) <= p) lo = mid; else hi = mid - 1;
+        }
+        a.chunk_tile[c] = uint32_t(lo);
+    }
+}
+
+int num_sms() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+unsigned capped_blocks(int64_t items, int per_sm) {
+    const int64_t blocks = (items + 255) / 256;
+    const int64_t cap = int64_t(num_sms()) * per_sm;
+    return unsigned(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
+}
+
+}  // namespace
+
+int64_t bucket_scan_parts(int64_t nb) { return (nb + kScanItems - 1) / kScanItems; }
+
+// Photons per CTA of the plan and scatter kernels: enough CTAs for four per SM, each a
+// multiple of 256 photons and at least 4096 (the window's flush is amortised over them).
+int64_t plan_range(int64_t n) {
+    const int64_t ctas = int64_t(num_sms()) * 4;
+    int64_t r = (n + ctas - 1) / ctas;
+    r = (r + 255) / 256 * 256;
+    return r < 4096 ? 4096 : r;
+}
+
+cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st) {
+    if (a.ph.n <= 0) return cudaSuccess;
+    plan_kernel<<<unsigned((a.ph.n + a.range - 1) / a.range), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bucket_sort(const ScatterArgs& a, cudaStream_t st) {
+    const int64_t np = bucket_scan_parts(a.nb);
+    bucket_reduce<<<unsigned(np), kScanThreads, 0, st>>>(a.counts, a.nb, a.part);
+    bucket_top<<<1, kScanThreads, 0, st>>>(a.part, np, a.start, a.nb);
+    bucket_down<<<unsigned(np), kScanThreads, 0, st>>>(a.counts, a.nb, a.part, a.start,
+                                                       a.cursor);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || a.n <= 0) return e;
+    bucket_scatter<<<unsigned((a.n + a.range - 1) / a.range), 256, 0, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    chunk_tile_kernel<<<capped_blocks((a.n + a.chunk - 1) / a.chunk, 4), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace pds

@@ -2,23 +2,22 @@
 //
 // Reference: PyOptix/kernel/photon_differentials.cu. The reference runs one thread per
 // photon over its whole footprint box with one global atomicAdd per covered pixel (forward,
-// :60-113) and the same walk reading the upstream gradient (backward, :136-221). Here:
+// :60-113) and the same walk reading the upstream gradient (backward, :136-221). Here the
+// photons come binned by the plan (pds_plan.cu: records in (simulation, channel, screen tile,
+// footprint class) order) and
 //
-//   plan_kernel      one pass over the photons (coalesced SoA reads): exact integer
-//                    footprint, a sort key (simulation, channel, screen tile of the centre
-//                    pixel, footprint class) and a 32-byte record in photon order.
-//   radix sort       pds_sort.cu: stable, so the order equals a CPU stable sort.
-//   fwd_tiles_kernel persistent CTAs walk fixed-size chunks of the sorted photons; each
-//                    tile segment is rasterised into a shared-memory accumulator covering
-//                    the tile plus an apron of the largest footprint radius, then flushed
-//                    with one coalesced pass of global adds over the touched box.
+//   fwd_tiles_kernel persistent CTAs take fixed-size chunks of the sorted photons from a work
+//                    counter; each tile segment is rasterised into a shared-memory accumulator
+//                    covering the tile plus an apron of the largest footprint radius, then
+//                    flushed with one coalesced pass of global adds over the touched box.
 //   bwd_tiles_kernel same walk; the segment's tile+apron of the upstream gradient is staged
-//                    in shared memory once, each photon gathers over its box from there and
-//                    writes its gradients (no atomics). The per-pixel work is reduced to the
-//                    moments sum(t g), sum(t^2 g), sum(t g d), sum(t g d d^T) of the offset d,
-//                    from which dL/dE, dL/dx and dL/dM follow by 2x2 algebra per photon.
-//   tail kernels     footprints wider than the apron (direct global path, a warp per photon)
-//                    and zero gradients for photons that touch no pixel.
+//                    in shared memory once, each photon gathers over its footprint from there
+//                    and writes one gradient record (no atomics). The per-pixel work is reduced
+//                    to the moments sum(t g), sum(t^2 g), sum(t g d), sum(t g d d^T) of the
+//                    offset d, from which dL/dE, dL/dx and dL/dM follow by 2x2 algebra.
+//   tail kernels     footprints wider than the apron (direct global path, a warp per photon).
+//   grad_scatter     gradient records into the reference's SoA outputs, zero for photons that
+//                    touch no pixel.
 #include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -30,95 +29,6 @@
 namespace pds {
 
 namespace {
-
-// ------------------------------------------------------------------ plan ---------------
-
-__global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
-    const int64_t n = a.ph.n;
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    uint32_t c_tile = 0, c_big = 0, c_inv = 0;
-    const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
-    const uint32_t cls_max = (1u << cb) - 1u;
-    const int64_t* __restrict__ cp = a.ph.cp;
-    const float* __restrict__ X = a.ph.X;
-    const float* __restrict__ R = a.ph.R;
-    const float* __restrict__ E = a.ph.E;
-    const float* __restrict__ M = a.ph.M;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        // all of the photon's inputs are loaded up front (coalesced, one latency round)
-        const int64_t ch = __ldg(cp + i);
-        const float x = __ldg(X + i), y = __ldg(X + n + i), rad = __ldg(R + i);
-        const float e = __ldg(E + i);
-        const float m00 = __ldg(M + i), m01 = __ldg(M + n + i);
-        const float m10 = __ldg(M + 3 * n + i), m11 = __ldg(M + 4 * n + i);
-        const int s = find_sim_of_photon(a.sims, i);
-        const pds_sim sim = load_sim(a.sims, s);
-        uint32_t key = a.key_invalid;
-        if (ch >= 0 && ch < sim.channels) {
-            const Footprint f = make_footprint(x, y, rad, sim.height, sim.width, a.mpr);
-            int32_t x0, x1, y0, y1;
-            if (clip_box(f, sim.height, sim.width, x0, x1, y0, y1)) {
-                if (f.rx > A || f.ry > A) {
-                    key = a.key_big;
-                } else {
-                    const int pcx = min(max(f.px_c, 0), sim.width - 1);
-                    const int pcy = min(max(f.py_c, 0), sim.height - 1);
-                    const int tx = pcx / T, ty = pcy / T;
-                    const uint32_t tile = uint32_t(sim.tile_base) +
-                                          uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
-                    uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
-                    if (a.cfg.band) {
-                        // photons of a warp then have similar band areas (trip counts)
-                        const float sx = float(2.0 / double(sim.width)),
-                                    sy = float(2.0 / double(sim.height));
-                        const float dx0 = corner_offset(f.px_c, sim.width, x);
-                        const float dy0 = corner_offset(f.py_c, sim.height, y);
-                        const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy,
-                                                  0.5f * float(sim.width), 0.5f * float(sim.height));
-                        (void)sx;
-                        int area = (2 * f.rx + 1) * (2 * f.ry + 1);
-                        if (bd.on && f.ellipse_all)
-                            area = min(area, (min(bd.ky1, f.ry) - max(bd.ky0, -f.ry) + 1) * bd.bw);
-                        const int lg = 31 - __clz(max(area, 1));
-                        cls = min(uint32_t(max(lg - 1, 0)), cls_max);
-                    }
-                    key = (tile << cb) | cls;
-                    const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) |
-                                           (e > 0.f ? 0u : kFlagFwdSkip);
-                    Rec r;
-                    r.dx0 = corner_offset(f.px_c, sim.width, x);
-                    r.dy0 = corner_offset(f.py_c, sim.height, y);
-                    r.m00 = m00;
-                    r.m01 = m01;
-                    r.m10 = m10;
-                    r.m11 = m11;
-                    r.e = e;
-                    r.packed = pack_rec(f.px_c - (tx * T - A), f.py_c - (ty * T - A), f.rx, f.ry,
-                                        flags);
-                    a.recs[i] = r;
-                }
-            }
-        }
-        a.keys[i] = key;
-        c_tile += key < a.key_big;
-        c_big += key == a.key_big;
-        c_inv += key == a.key_invalid;
-    }
-    // block totals -> three global counters
-    __shared__ uint32_t red[3];
-    if (threadIdx.x < 3) red[threadIdx.x] = 0;
-    __syncthreads();
-    c_tile = __reduce_add_sync(0xFFFFFFFFu, c_tile);
-    c_big = __reduce_add_sync(0xFFFFFFFFu, c_big);
-    c_inv = __reduce_add_sync(0xFFFFFFFFu, c_inv);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&red[0], c_tile);
-        atomicAdd(&red[1], c_big);
-        atomicAdd(&red[2], c_inv);
-    }
-    __syncthreads();
-    if (threadIdx.x < 3 && red[threadIdx.x]) atomicAdd(a.counters + threadIdx.x, red[threadIdx.x]);
-}
 
 // ------------------------------------------------------------------ tiles --------------
 
@@ -249,7 +159,8 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
     const float e3 = r.e * kThreeOverPi;
     const bool all = fl & kFlagEllipseAll;
     if (band && all) {
-        const Band bd = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy);
+        const Band bd = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy,
+                                  float(rx) + 1.f);
         if (bd.on) {
             deposit_band(r, bd, ti, sw, static_cast<uint32_t>(__cvta_generic_to_shared(acc)), pxc,
                          pyc, x0, x1, y0, y1);
@@ -430,6 +341,45 @@ __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& t
     __syncthreads();
 }
 
+// A run of sorted positions [begin, end) holding one screen tile's photons.
+struct Segment {
+    uint32_t tile;
+    int64_t begin, end;
+};
+
+// End of tile t's photons: the start of its successor's first bucket.
+__device__ __forceinline__ int64_t tile_end(const TileArgs& a, int64_t t) {
+    return int64_t(__ldg(a.start + ((t + 1) << a.cfg.class_bits)));
+}
+
+__device__ __forceinline__ Segment first_segment(const TileArgs& a, int64_t chunk, int64_t p0) {
+    Segment s;
+    // (clamped, like the counters, so that a workspace without a plan stays in its arrays)
+    s.tile = uint32_t(min(int64_t(__ldg(a.chunk_tile + chunk)), a.n_tiles - 1));
+    s.begin = p0;
+    s.end = tile_end(a, s.tile);
+    return s;
+}
+
+// The segment after sg (sg.end below the tile path's photon count): the first tile after
+// sg.tile whose range is not empty, found by doubling steps then bisection (empty tiles are
+// usually few, so one probe mostly suffices). Every thread computes it from the same loads.
+__device__ __forceinline__ Segment next_segment(const TileArgs& a, const Segment& sg) {
+    const int64_t p = sg.end, t = sg.tile, last = a.n_tiles - 1;
+    int64_t k = 1;
+    while (t + k < last && tile_end(a, t + k) <= p) k <<= 1;
+    int64_t lo = t + (k >> 1) + 1, hi = min(t + k, last);
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (tile_end(a, mid) > p) hi = mid; else lo = mid + 1;
+    }
+    Segment s;
+    s.tile = uint32_t(lo);
+    s.begin = p;
+    s.end = tile_end(a, lo);
+    return s;
+}
+
 // Next chunk of sorted photons for this CTA: a shared work counter (reset to zero before the
 // launch) hands chunks out in order as CTAs finish, so CTAs that drew chunks of large
 // footprints do not hold up the others. Nothing waits on it.
@@ -445,7 +395,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     extern __shared__ float acc[];
     __shared__ int sb[4];
     const Cfg cfg = a.cfg;
-    const int sw = cfg.sw, cb = cfg.class_bits;
+    const int sw = cfg.sw;
     for (int k = threadIdx.x; k < sw * sw; k += NT) acc[k] = 0.f;
     if (threadIdx.x == 0) {
         sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
@@ -458,25 +408,19 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     for (int64_t c = next_chunk(a.queue, &chunk_slot); c < nchunks;
          c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
-        uint32_t cur = a.skeys[p0] >> cb;
-        TileInfo ti = decode_tile(a.sims, cur, cfg);
+        Segment sg = first_segment(a, c, p0);
+        TileInfo ti = decode_tile(a.sims, sg.tile, cfg);
         for (int64_t base = p0; base < p1; base += NT) {
             const int64_t i = base + threadIdx.x;
             const bool have = i < p1;
-            uint32_t key = 0xFFFFFFFFu;
             Rec r = {};
-            if (have) {
-                key = a.skeys[i] >> cb;
-                r = a.srecs[i];
-            }
+            if (have) r = a.srecs[i];
             const int64_t bend = min(base + NT, p1);
-            // The batch's keys are sorted, so its segments are consecutive thread ranges;
-            // `done` counts the threads of the segments handled so far. Each pass of the
-            // loop handles one segment (the first pass may find none when the previous
-            // batch's segment does not continue here), so NT + 1 passes always suffice.
-            int done = 0;
+            // The batch's segments (runs of one tile) are consecutive thread ranges; each
+            // pass handles one and flushes the tile's accumulator when the next one starts.
+            // Every pass but the first covers at least one photon, so NT + 1 passes suffice.
             for (int pass = 0; pass <= NT; ++pass) {
-                const bool mine = have && key == cur;
+                const bool mine = have && i >= sg.begin && i < sg.end;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
                 if (mine && !coop) deposit(r, ti, sw, cfg.spans, cfg.band, acc, x0, x1, y0, y1);
@@ -489,12 +433,10 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
                     deposit_coop(rb, ti, sw, acc_base, threadIdx.x & 31);
                 }
                 bbox_publish(sb, x0, x1, y0, y1);
-                done += __syncthreads_count(mine);
-                const int64_t nxt = base + done;
-                if (nxt >= bend) break;
+                if (sg.end >= bend) break;
                 flush_tile(acc, sw, ti, a.out, sb);
-                cur = a.skeys[nxt] >> cb;
-                ti = decode_tile(a.sims, cur, cfg);
+                sg = next_segment(a, sg);
+                ti = decode_tile(a.sims, sg.tile, cfg);
             }
         }
         flush_tile(acc, sw, ti, a.out, sb);
@@ -581,63 +523,113 @@ __device__ __forceinline__ void bwd_row(int n, const float* q, float k0, float b
     }
 }
 
-// Backward gather of one photon over its band (see Band and deposit_band). Per row it keeps
-// sum t g and sum t g kx (kx the integer pixel offset) and folds them at the row change;
-// sum t g kx^2 and sum t^2 g run over the whole band.
-__device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const TileInfo& ti,
-                                            int sw, const float* tg, uint32_t rid, int pxc,
-                                            int pyc, int x0, int x1, int y0, int y1,
-                                            const TileArgs& a) {
-    const int ky0 = max(bd.ky0, y0 - pyc), ky1 = min(bd.ky1, y1 - pyc);
-    const int kxb0 = x0 - pxc;
-    const uint32_t kxspan = uint32_t(x1 - x0);
-    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
-    const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
-    const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
-    const int bw = bd.bw;
-    const int total = ky0 <= ky1 ? (ky1 - ky0 + 1) * bw : 0;
-    float sE = 0.f, A0t = 0.f, B1t = 0.f, B2 = 0.f, Sy = 0.f, Sxy = 0.f, Syy = 0.f;
+// The backward walks the band inside the clipped box. A row is w = min(bw rounded up to
+// even, box width) pixels wide and starts at the band's start clamped into
+// [kxb0, kxb1 - w + 1]. A clamped row still holds every pixel of its support that lies in the
+// box (the support's pixels of row ky are in [xs, xs + bw - 1]; clamping slides that window
+// into the box without dropping any of them, and when w is the box width the row is the whole
+// box row), so no pixel needs an in-box test. Rows are walked two pixels at a time; when w is
+// odd, the second pixel of each row's last pair lies just outside the box and is masked.
+struct BandWalk {
+    int w, npairs, tail, kxb0, kxlast;
+};
+
+__device__ __forceinline__ BandWalk band_walk(const Band& bd, int kxb0, int kxb1) {
+    BandWalk b;
+    b.w = min((bd.bw + 1) & ~1, kxb1 - kxb0 + 1);
+    b.npairs = (b.w + 1) >> 1;
+    b.tail = b.w & 1;  // value of the remaining-pair count at which the mask applies
+    b.kxb0 = kxb0;
+    b.kxlast = kxb1 - b.w + 1;
+    return b;
+}
+
+__device__ __forceinline__ int band_row_start(const Band& bd, const BandWalk& bw, int ky) {
+    return min(max(band_start(bd, ky), bw.kxb0), bw.kxlast);
+}
+
+// Backward moments over the band rows ky0..ky1 (ky0 <= ky1). Per row it keeps sum t g and
+// sum t g kx (kx the integer pixel offset) and folds them into the y moments at the row
+// change; sum t g kx^2 and sum t^2 g run over the whole band. The masked pixel of an odd row
+// (just outside the box) is read from the staged tile's spare column (the pitch is odd:
+// tile + 2 apron + 1, and a box never reaches past column tile + 2 apron - 1) and its product
+// discarded.
+struct BandMoments {
+    float sE, A0t, B1t, B2, Sy, Sxy, Syy;
+};
+
+__device__ __forceinline__ BandMoments gather_band_rows(const Band& bd, const BandWalk& bw,
+                                                        int ky, int ky1, const float* row,
+                                                        int sw, float a00, float a10, float c0,
+                                                        float c1, float m01sy, float m11sy,
+                                                        float sy, float dy0, float sx,
+                                                        float dx0) {
+    BandMoments m = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float A0 = 0.f, B1 = 0.f;
-    int ky = ky0, c = 0;
-    int xs = band_start(bd, ky);
-    float c0 = fmaf(float(ky), m01sy, c00), c1 = fmaf(float(ky), m11sy, c10);
-    const float* row = tg + (pyc + ky - ti.oy) * sw + (pxc - ti.ox);
-    for (int q = 0; q < total; ++q) {
-        const int kx = xs + c;
-        const bool in = uint32_t(kx - kxb0) <= kxspan;
-        const float kf = float(kx);
+    int xs = band_row_start(bd, bw, ky);
+    float kf = float(xs);
+    const float* q = row + xs;
+    int rem = bw.npairs;
+    for (;;) {
         const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
-        const float s = fmaf(u0, u0, u1 * u1);
-        // the load's column is clamped into the box, so it never leaves the staged tile
-        const float gv = row[min(max(kx, kxb0), kxb0 + int(kxspan))];
-        const float t = in ? fmaxf(1.f - s, 0.f) : 0.f;
-        const float g = in ? t * gv : 0.f;
-        sE = fmaf(t, g, sE);
-        A0 += g;
-        const float tk = g * kf;
-        B1 += tk;
-        B2 = fmaf(tk, kf, B2);
-        if (++c == bw) {
-            const float dy = fmaf(float(ky), ti.sy, r.dy0);
-            const float sdx = fmaf(ti.sx, B1, r.dx0 * A0);
-            Sy = fmaf(dy, A0, Sy);
-            Sxy = fmaf(dy, sdx, Sxy);
-            Syy = fmaf(dy * dy, A0, Syy);
-            A0t += A0;
-            B1t += B1;
+        const float v0 = u0 + a00, v1 = u1 + a10;
+        const float s = fmaf(u0, u0, u1 * u1), s2 = fmaf(v0, v0, v1 * v1);
+        const float t = fmaxf(1.f - s, 0.f), t2 = fmaxf(1.f - s2, 0.f);
+        const float g = t * q[0];
+        const float g2 = rem == bw.tail ? 0.f : t2 * q[1];
+        const float kf1 = kf + 1.f;
+        m.sE = fmaf(t, g, m.sE);
+        m.sE = fmaf(t2, g2, m.sE);
+        A0 += g + g2;
+        const float tk = g * kf, tk2 = g2 * kf1;
+        B1 += tk + tk2;
+        m.B2 = fmaf(tk, kf, m.B2);
+        m.B2 = fmaf(tk2, kf1, m.B2);
+        kf += 2.f;
+        q += 2;
+        if (--rem == 0) {
+            const float dy = fmaf(float(ky), sy, dy0);
+            const float sdx = fmaf(sx, B1, dx0 * A0);
+            m.Sy = fmaf(dy, A0, m.Sy);
+            m.Sxy = fmaf(dy, sdx, m.Sxy);
+            m.Syy = fmaf(dy * dy, A0, m.Syy);
+            m.A0t += A0;
+            m.B1t += B1;
+            if (++ky > ky1) break;
             A0 = 0.f;
             B1 = 0.f;
-            c = 0;
-            ++ky;
-            xs = band_start(bd, ky);
+            rem = bw.npairs;
+            xs = band_row_start(bd, bw, ky);
+            kf = float(xs);
             c0 += m01sy;
             c1 += m11sy;
             row += sw;
+            q = row + xs;
         }
     }
-    const float Sx = fmaf(ti.sx, B1t, r.dx0 * A0t);
-    const float Sxx = fmaf(ti.sx * ti.sx, B2, fmaf(2.f * ti.sx * r.dx0, B1t, r.dx0 * r.dx0 * A0t));
-    finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+    return m;
+}
+
+// Backward gather of one photon over its band rows ky0..ky1 (see BandWalk); with no row
+// inside the box (ky0 > ky1) its gradients are zero.
+__device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const TileInfo& ti,
+                                            int sw, const float* tg, uint32_t slot, int pxc,
+                                            int pyc, int ky0, int ky1, int kxb0, int kxb1,
+                                            const TileArgs& a) {
+    const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
+    const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
+    const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
+    const float c0 = fmaf(float(ky0), m01sy, c00), c1 = fmaf(float(ky0), m11sy, c10);
+    const float* row = tg + (pyc + ky0 - ti.oy) * sw + (pxc - ti.ox);
+    BandMoments m = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (ky0 <= ky1)
+        m = gather_band_rows(bd, band_walk(bd, kxb0, kxb1), ky0, ky1, row, sw, a00, a10, c0,
+                             c1, m01sy, m11sy, ti.sy, r.dy0, ti.sx, r.dx0);
+    const float Sx = fmaf(ti.sx, m.B1t, r.dx0 * m.A0t);
+    const float Sxx = fmaf(ti.sx * ti.sx, m.B2,
+                           fmaf(2.f * ti.sx * r.dx0, m.B1t, r.dx0 * r.dx0 * m.A0t));
+    finish_grad(a.stage, slot, r.e, r.m00, r.m01, r.m10, r.m11, m.sE, Sx, m.Sy, Sxx, m.Sxy,
+                m.Syy);
 }
 
 // Backward gather of one photon (photon_differentials.cu:169-218) from the staged gradient.
@@ -655,9 +647,11 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
     const int y0 = max(pyc - ry, 0), y1 = min(pyc + ry, ti.H - 1);
     const bool all = fl & kFlagEllipseAll;
     if (band && all) {
-        const Band bd = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy);
+        const Band bd = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy,
+                                  float(rx) + 1.f);
         if (bd.on) {
-            gather_band(r, bd, ti, sw, tg, rid, pxc, pyc, x0, x1, y0, y1, a);
+            const int ky0 = max(bd.ky0, y0 - pyc), ky1 = min(bd.ky1, y1 - pyc);
+            gather_band(r, bd, ti, sw, tg, rid, pxc, pyc, ky0, ky1, x0 - pxc, x1 - pxc, a);
             return;
         }
     }
@@ -757,58 +751,50 @@ template <int NT, int MINB>
 __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
     extern __shared__ float tg[];
     const Cfg cfg = a.cfg;
-    const int sw = cfg.sw, cb = cfg.class_bits;
+    const int sw = cfg.sw;
     const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
     __shared__ uint32_t chunk_slot;
     for (int64_t c = next_chunk(a.queue, &chunk_slot); c < nchunks;
          c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
-        uint32_t cur = a.skeys[p0] >> cb;
-        TileInfo ti = decode_tile(a.sims, cur, cfg);
-        uint32_t loaded = 0xFFFFFFFFu;
+        Segment sg = first_segment(a, c, p0);
+        TileInfo ti = decode_tile(a.sims, sg.tile, cfg);
+        // next_chunk's barrier ends the previous chunk's reads of the staged tile
+        load_region(tg, sw, ti, a.grad);
+        __syncthreads();
         for (int64_t base = p0; base < p1; base += NT) {
             const int64_t i = base + threadIdx.x;
             const bool have = i < p1;
-            uint32_t key = 0xFFFFFFFFu, rid = 0;
             Rec r = {};
-            if (have) {
-                key = a.skeys[i] >> cb;
-                rid = a.sidx[i];
-                r = a.srecs[i];
-            }
+            if (have) r = a.srecs[i];
             const int64_t bend = min(base + NT, p1);
-            // consecutive segments of the sorted batch, as in fwd_tiles_kernel
-            int done = 0;
+            // consecutive segments of the batch, as in fwd_tiles_kernel; a photon's gradient
+            // record goes to its sorted position
             for (int pass = 0; pass <= NT; ++pass) {
-                if (cur != loaded) {
-                    __syncthreads();
-                    load_region(tg, sw, ti, a.grad);
-                    __syncthreads();
-                    loaded = cur;
-                }
-                const bool mine = have && key == cur;
+                const bool mine = have && i >= sg.begin && i < sg.end;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
-                if (mine && !coop) gather(r, ti, sw, cfg.spans, cfg.band, tg, rid, a);
+                if (mine && !coop) gather(r, ti, sw, cfg.spans, cfg.band, tg, uint32_t(i), a);
                 for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
                     const int src = __ffs(cm) - 1;
                     const Rec rb = shfl_rec(r, src);
-                    gather_coop(rb, ti, sw, tg, __shfl_sync(0xFFFFFFFFu, rid, src), src, a);
+                    const uint32_t slot = uint32_t(base) + (threadIdx.x & ~31u) + uint32_t(src);
+                    gather_coop(rb, ti, sw, tg, slot, src, a);
                 }
-                done += __syncthreads_count(mine);
-                const int64_t nxt = base + done;
-                if (nxt >= bend) break;
-                cur = a.skeys[nxt] >> cb;
-                ti = decode_tile(a.sims, cur, cfg);
+                if (sg.end >= bend) break;
+                sg = next_segment(a, sg);
+                ti = decode_tile(a.sims, sg.tile, cfg);
+                __syncthreads();
+                load_region(tg, sw, ti, a.grad);
+                __syncthreads();
             }
         }
     }
 }
 
 // ------------------------------------------------------------------ tail ---------------
-// Sorted positions [n_tile, n_tile + n_big) hold footprints wider than the apron; they are
-// splatted straight into global memory, one warp per photon. Positions after that hold
-// photons that touch no pixel.
+// Footprints wider than the apron (the plan's wide list) are splatted straight into global
+// memory, one warp per photon; their gradient records follow the tile path's in the stage.
 
 struct Direct {
     int pxc, pyc, x0, x1, y0, y1;
@@ -848,12 +834,12 @@ __device__ __forceinline__ bool direct_setup(const TileArgs& a, uint32_t rid, Di
 }
 
 __global__ __launch_bounds__(256) void tail_fwd_kernel(TileArgs a) {
-    const int64_t n_tile = tile_count(a), n_big = wide_count(a);
+    const int64_t n_big = wide_count(a);
     const int lane = threadIdx.x & 31;
     const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
     for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_big;
          w += warps) {
-        const uint32_t rid = a.sidx[n_tile + w];
+        const uint32_t rid = __ldg(a.wide + w);
         Direct d;
         if (!direct_setup(a, rid, d) || !(d.e > 0.f)) continue;
         const float e3 = d.e * kThreeOverPi;
@@ -876,13 +862,12 @@ __global__ __launch_bounds__(256) void tail_fwd_kernel(TileArgs a) {
 }
 
 __global__ __launch_bounds__(256) void tail_bwd_kernel(TileArgs a) {
-    const int64_t n = a.ph.n;
     const int64_t n_tile = tile_count(a), n_big = wide_count(a);
     const int lane = threadIdx.x & 31;
     const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
     for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_big;
          w += warps) {
-        const uint32_t rid = a.sidx[n_tile + w];
+        const uint32_t rid = __ldg(a.wide + w);
         Direct d;
         float sE = 0.f, Sx = 0.f, Sy = 0.f, Sxx = 0.f, Sxy = 0.f, Syy = 0.f;
         const bool any = direct_setup(a, rid, d);
@@ -920,25 +905,29 @@ __global__ __launch_bounds__(256) void tail_bwd_kernel(TileArgs a) {
             if (!any) {
                 d.m00 = d.m01 = d.m10 = d.m11 = d.e = 0.f;
             }
-            finish_grad(a.stage, rid, d.e, d.m00, d.m01, d.m10, d.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+            finish_grad(a.stage, uint32_t(n_tile + w), d.e, d.m00, d.m01, d.m10, d.m11, sE, Sx,
+                        Sy, Sxx, Sxy, Syy);
         }
     }
-    // photons that touch no pixel: zero gradients
-    const int64_t inv0 = n_tile + n_big;
-    const int64_t threads = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t p = inv0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += threads)
-        store_grad(a.stage, a.sidx[p], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f);
 }
 
-// Spreads the per-photon gradient records (photon order) into the reference's outputs
-// grad_Ep[N], grad_xp[2][N], grad_Mp[2][3][N] (column 2 of grad_Mp is zero, :212, :218);
-// reads and writes are coalesced.
+// Spreads the gradient records into the reference's outputs grad_Ep[N], grad_xp[2][N],
+// grad_Mp[2][3][N] (column 2 of grad_Mp is zero, :212, :218) in photon order: each photon's
+// record is one 32-byte gather through the plan's inverse map, the writes are coalesced.
+// Photons that touch no pixel get zeros.
 __global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
     const int64_t n = a.ph.n;
+    const int64_t n_tile = tile_count(a);
     const float4* st = reinterpret_cast<const float4*>(a.stage);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x) {
-        const float4 lo = st[2 * i], hi = st[2 * i + 1];
+        const uint32_t v = __ldg(a.inv + i);
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+        const int64_t slot = (v & kWideBit) ? n_tile + int64_t(v & ~kWideBit) : int64_t(v);
+        if (v != kInvalidPos && slot < n) {
+            lo = st[2 * slot];
+            hi = st[2 * slot + 1];
+        }
         a.gE[i] = lo.x;
         a.gX[i] = lo.y;
         a.gX[n + i] = lo.z;
@@ -949,18 +938,6 @@ __global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
         a.gM[4 * n + i] = hi.z;
         a.gM[5 * n + i] = 0.f;
     }
-}
-
-// Records of the tile-path photons in sorted order, so that the tile kernels read them with
-// coalesced loads; this one random gather replaces one per tile kernel.
-__global__ __launch_bounds__(256) void sort_records_kernel(const Rec* __restrict__ recs,
-                                                           const uint32_t* __restrict__ sidx,
-                                                           const uint32_t* __restrict__ counters,
-                                                           int64_t n, Rec* __restrict__ srecs) {
-    const int64_t n_tile = min(int64_t(counters[0]), n);
-    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n_tile;
-         p += int64_t(gridDim.x) * blockDim.x)
-        srecs[p] = recs[__ldg(sidx + p)];
 }
 
 __global__ void iota_kernel(uint32_t* dst, int64_t n) {
@@ -1001,24 +978,6 @@ void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st) {
     if (n <= 0) return;
     const int64_t blocks = (n + 255) / 256;
     iota_kernel<<<unsigned(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(dst, n);
-}
-
-cudaError_t launch_sort_records(const Rec* recs, const uint32_t* sidx, const uint32_t* counters,
-                                int64_t n, Rec* srecs, cudaStream_t st) {
-    if (n <= 0) return cudaSuccess;
-    const int64_t blocks = (n + 255) / 256;
-    const int64_t cap = int64_t(num_sms()) * 16;
-    sort_records_kernel<<<unsigned(blocks < cap ? blocks : cap), 256, 0, st>>>(recs, sidx, counters,
-                                                                              n, srecs);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st) {
-    if (a.ph.n <= 0) return cudaSuccess;
-    const int64_t blocks = (a.ph.n + 255) / 256;
-    const int64_t cap = int64_t(num_sms()) * 8;
-    plan_kernel<<<unsigned(blocks < cap ? blocks : cap), 256, 0, st>>>(a);
-    return cudaGetLastError();
 }
 
 template <int MINB>

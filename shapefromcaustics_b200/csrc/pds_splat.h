@@ -1,4 +1,4 @@
-// Kernel argument blocks and launchers of the splatting kernels (pds_splat.cu).
+// Kernel argument blocks and launchers of the splatting kernels (pds_plan.cu, pds_splat.cu).
 #pragma once
 
 #include <cstdint>
@@ -23,10 +23,33 @@ struct PlanArgs {
     SimTable sims;
     int32_t mpr;
     Cfg cfg;
-    uint32_t key_big, key_invalid;
-    uint32_t* keys;      // [n] out
+    uint32_t key_big, key_invalid;  // bucket count (wide photons), and the untouched key
+    uint32_t* keys;      // [n] out: bucket of each photon, key_big or key_invalid
     Rec* recs;           // [n] out (tile-path photons only)
+    uint32_t* counts;    // [key_big] photons per bucket; zeroed by the caller
+    uint32_t* inv;       // [n] out for wide (kWideBit | k) and untouched (kInvalidPos) photons
+    uint32_t* wide;      // [n] out: photon index of the k-th wide photon
     uint32_t* counters;  // [0] tile-path, [1] wide, [2] untouched photons; zeroed by caller
+    int64_t range;       // photons per CTA (plan_range)
+};
+
+// Bucket scan and scatter of the plan.
+struct ScatterArgs {
+    SimTable sims;
+    const uint32_t* keys;
+    const Rec* recs;
+    const uint32_t* counts;
+    const uint32_t* counters;
+    uint32_t* part;        // [bucket_scan_parts(nb)] scan partials
+    uint32_t* start;       // [nb + 1] out: first sorted position of each bucket, then the total
+    uint32_t* cursor;      // [nb] scatter cursors
+    Rec* srecs;            // [n] out: records in sorted order
+    uint32_t* inv;         // [n] out for tile-path photons: sorted position
+    uint32_t* chunk_tile;  // [n / chunk + 1] out: tile of each work chunk's first photon
+    int64_t n, nb, n_tiles;
+    int64_t range;         // photons per CTA, as in the plan
+    uint32_t key_big;
+    int32_t chunk, cb;
 };
 
 struct TileArgs {
@@ -34,22 +57,27 @@ struct TileArgs {
     SimTable sims;
     int32_t mpr;
     Cfg cfg;
-    const uint32_t* skeys;     // sorted keys
-    const uint32_t* sidx;      // sorted photon indices
-    const Rec* srecs;          // records in sorted order
+    int64_t n_tiles;
+    const Rec* srecs;            // records in sorted order
+    const uint32_t* start;       // [(n_tiles << class_bits) + 1] bucket starts
+    const uint32_t* chunk_tile;  // tile of each chunk's first photon
+    const uint32_t* inv;         // per photon: sorted position, kWideBit | k, or kInvalidPos
+    const uint32_t* wide;        // photon index of each wide photon
     const uint32_t* counters;
-    uint32_t* queue;           // chunk work counter of the tile kernel (zeroed before launch)
-    float* out;                // forward: flat image buffer (zeroed by caller)
-    const float* grad;         // backward: flat upstream gradient buffer
-    float* gE;                 // backward outputs
+    uint32_t* queue;             // chunk work counter of the tile kernel (zeroed before launch)
+    float* out;                  // forward: flat image buffer (zeroed by caller)
+    const float* grad;           // backward: flat upstream gradient buffer
+    float* gE;                   // backward outputs
     float* gX;
     float* gM;
-    GradRec* stage;            // backward: per-photon gradient records (workspace)
+    GradRec* stage;              // backward: gradient records, sorted positions then the wide
+                                 // photons (workspace)
 };
 
+int64_t bucket_scan_parts(int64_t nb);
+int64_t plan_range(int64_t n);
 cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st);
-cudaError_t launch_sort_records(const Rec* recs, const uint32_t* sidx, const uint32_t* counters,
-                                int64_t n, Rec* srecs, cudaStream_t st);
+cudaError_t launch_bucket_sort(const ScatterArgs& a, cudaStream_t st);
 cudaError_t launch_forward(const TileArgs& a, cudaStream_t st);
 cudaError_t launch_backward(const TileArgs& a, cudaStream_t st);
 
