@@ -48,8 +48,9 @@ typedef struct pds_config {
     int32_t tile;       /* screen-tile edge in pixels: 16, 32 or 64 (default 64) */
     int32_t chunk;      /* sorted photons per CTA work item, multiple of 256 (default 2048) */
     int32_t class_bits; /* footprint-size bits appended to the sort key (photons of a tile
-                           are then grouped by footprint size): 1..4, or -1 for none
-                           (default 3) */
+                           are then grouped by footprint size; with the band walk, classes
+                           of 1/k octave of the band's area, k = 1 up to 3 bits, 2 for 4,
+                           3 for 5): 1..5, or -1 for none (default 5) */
     int32_t apron_max;  /* largest footprint radius (px) the tile path holds (default 32);
                            larger footprints take the direct path */
     int32_t walk;       /* pixels visited per photon: 1 = the reference's whole box,

@@ -40,7 +40,7 @@ struct Resolved {
 int resolve_cfg(const pds_config* in, pds_config& out) {
     out.tile = (in && in->tile) ? in->tile : 64;
     out.chunk = (in && in->chunk) ? in->chunk : 2048;
-    out.class_bits = (in && in->class_bits) ? in->class_bits : 3;
+    out.class_bits = (in && in->class_bits) ? in->class_bits : 5;
     if (out.class_bits == -1) out.class_bits = 0;
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
     out.walk = (in && in->walk) ? in->walk : 3;
@@ -58,8 +58,8 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
     if (out.chunk < 256 || out.chunk > (1 << 20) || out.chunk % 256 != 0)
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.chunk must be a multiple of 256 in [256, 1048576]");
-    if (out.class_bits < 0 || out.class_bits > 4)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be -1 or in [1, 4]");
+    if (out.class_bits < 0 || out.class_bits > 5)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be -1 or in [1, 5]");
     if (out.apron_max < 1 || out.apron_max > 63 || out.tile + 2 * out.apron_max > 255)
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.apron_max must be in [1, 63] with tile + 2*apron_max <= 255");
@@ -242,7 +242,7 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.inv = b.inv;
     a.wide = b.wide;
     a.counters = b.counters;
-    a.range = pds::plan_range(ph.n);
+    pds::plan_shape(ph.n, r.n_buckets, &a.window, &a.range);
     e = pds::launch_plan(a, s);
     if (e != cudaSuccess) return cuda_fail(e, "plan_kernel");
     pds::ScatterArgs sa;
@@ -261,6 +261,7 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     sa.nb = r.n_buckets;
     sa.n_tiles = n_tiles;
     sa.range = a.range;
+    sa.window = a.window;
     sa.key_big = r.key_big;
     sa.chunk = r.cfg.chunk;
     sa.cb = r.cfg.class_bits;

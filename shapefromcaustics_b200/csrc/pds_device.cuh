@@ -15,6 +15,7 @@
 // the closer one to the FP64 oracle.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -96,6 +97,12 @@ __device__ __forceinline__ int find_sim_of_photon(const SimTable& t, int64_t i) 
         if (__ldg(&t.dev[mid].photon_begin) <= i) lo = mid; else hi = mid - 1;
     }
     return lo;
+}
+
+// First photon after simulation s (the next simulation's photon_begin; no limit for the last).
+__device__ __forceinline__ int64_t sim_end(const SimTable& t, int s) {
+    if (t.dev == nullptr || s + 1 >= t.n) return INT64_MAX;
+    return __ldg(&t.dev[s + 1].photon_begin);
 }
 
 // Simulation owning global tile id g.

@@ -7,9 +7,10 @@
 //                    a bucket (simulation, channel, screen tile of the centre pixel, footprint
 //                    class) and a 32-byte record in photon order. Each CTA takes a contiguous
 //                    photon range (one or two simulations) and counts its buckets in a
-//                    shared-memory histogram over the window of buckets that starts at its
-//                    first photon's simulation; the histogram is added into the global counts
-//                    once per CTA. Photons wider than the apron go to the wide list.
+//                    shared-memory histogram over the window of buckets (up to 12160) that
+//                    starts at its first photon's simulation; the histogram is added into the
+//                    global counts once per CTA. Photons wider than the apron go to the wide
+//                    list.
 //   bucket scan      exclusive scan of the bucket counts (three parallel kernels), giving each
 //                    bucket its first sorted position; a copy serves as the scatter's cursors.
 //   bucket_scatter   the same CTA ranges: each CTA recounts its window, reserves its share of
@@ -40,24 +41,29 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-constexpr int kWindow = 12160;  // buckets of a CTA's shared histogram (47.5 KB)
+// One CTA of 1024 threads per SM: the histogram flush and the cursor reservations cost one
+// global atomic per CTA and touched bucket, so fewer, larger CTAs make fewer of them.
+constexpr int kPlanThreads = 1024;
+// buckets of a CTA's shared histogram (47.5 KB, which leaves the SM most of its L1 cache for
+// the simulation table and the streamed loads)
+constexpr int kMaxWindow = 12160;
 
 // First bucket of the simulation owning photon i.
 __device__ __forceinline__ uint32_t window_base(const SimTable& st, int64_t i, int cb) {
     return uint32_t(load_sim(st, find_sim_of_photon(st, i)).tile_base) << cb;
 }
 
-__device__ __forceinline__ void zero_window(uint32_t* hist) {
-    for (int j = threadIdx.x; j < kWindow; j += blockDim.x) hist[j] = 0u;
+__device__ __forceinline__ void zero_window(uint32_t* hist, int window) {
+    for (int j = threadIdx.x; j < window; j += blockDim.x) hist[j] = 0u;
 }
 
-__global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
-    __shared__ uint32_t hist[kWindow];
+__global__ __launch_bounds__(kPlanThreads) void plan_kernel(PlanArgs a) {
+    extern __shared__ uint32_t hist[];  // a.window buckets
     const int64_t n = a.ph.n;
     const int lane = threadIdx.x & 31;
     const int64_t r0 = int64_t(blockIdx.x) * a.range, r1 = min(r0 + a.range, n);
     const uint32_t kb0 = window_base(a.sims, r0, a.cfg.class_bits);
-    zero_window(hist);
+    zero_window(hist, a.window);
     __syncthreads();
     uint32_t c_tile = 0, c_inv = 0;
     const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
@@ -67,20 +73,28 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
     const float* __restrict__ R = a.ph.R;
     const float* __restrict__ E = a.ph.E;
     const float* __restrict__ M = a.ph.M;
+    // The thread's simulation is followed along its photons (contiguous per simulation) rather
+    // than searched per photon: one table load when a simulation boundary is crossed.
+    int sidx = find_sim_of_photon(a.sims, min(r0 + int64_t(threadIdx.x), n - 1));
+    pds_sim sim = load_sim(a.sims, sidx);
+    int64_t next_begin = sim_end(a.sims, sidx);
     // whole warps step together (the wide list's ballot needs every lane)
     for (int64_t base = r0; base < r1; base += blockDim.x) {
         const int64_t i = base + threadIdx.x;
         const bool valid = i < r1;
         uint32_t key = a.key_invalid;
         if (valid) {
+            while (i >= next_begin) {  // at most the table's length in all
+                ++sidx;
+                sim = load_sim(a.sims, sidx);
+                next_begin = sim_end(a.sims, sidx);
+            }
             // all of the photon's inputs are loaded up front (coalesced, one latency round)
             const int64_t ch = __ldg(cp + i);
             const float x = __ldg(X + i), y = __ldg(X + n + i), rad = __ldg(R + i);
             const float e = __ldg(E + i);
             const float m00 = __ldg(M + i), m01 = __ldg(M + n + i);
             const float m10 = __ldg(M + 3 * n + i), m11 = __ldg(M + 4 * n + i);
-            const int s = find_sim_of_photon(a.sims, i);
-            const pds_sim sim = load_sim(a.sims, s);
             if (ch >= 0 && ch < sim.channels) {
                 const Footprint f = make_footprint(x, y, rad, sim.height, sim.width, a.mpr);
                 int32_t x0, x1, y0, y1;
@@ -98,7 +112,9 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
                         const float dy0 = corner_offset(f.py_c, sim.height, y);
                         uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
                         if (a.cfg.band) {
-                            // photons of a warp then have similar band areas (trip counts)
+                            // photons of a warp then have similar band areas (trip counts):
+                            // classes of 1/k octave of the area, k = 1, 2, 3 for up to 3, 4
+                            // and 5 class bits
                             const float sy = float(2.0 / double(sim.height));
                             const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy,
                                                       0.5f * float(sim.width),
@@ -108,8 +124,12 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
                             if (bd.on && f.ellipse_all)
                                 area = min(area, (min(bd.ky1, f.ry) - max(bd.ky0, -f.ry) + 1) *
                                                      bd.bw);
-                            const int lg = 31 - __clz(max(area, 1));
-                            cls = min(uint32_t(max(lg - 1, 0)), cls_max);
+                            // floor(k log2 area) = floor(log2 area^k), exactly
+                            const int k = cb <= 3 ? 1 : cb - 2;
+                            const uint64_t a1 = uint64_t(max(area, 1));
+                            const uint64_t ak = k == 1 ? a1 : (k == 2 ? a1 * a1 : a1 * a1 * a1);
+                            const int lg = 63 - __clzll(ak);
+                            cls = min(uint32_t(max(lg - k, 0)), cls_max);
                         }
                         key = (tile << cb) | cls;
                         const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) |
@@ -137,7 +157,7 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
         c_inv += valid && key == a.key_invalid;
         if (tile_path) {
             const uint32_t j = key - kb0;
-            if (j < uint32_t(kWindow)) atomicAdd(hist + j, 1u);
+            if (j < uint32_t(a.window)) atomicAdd(hist + j, 1u);
             else atomicAdd(a.counts + key, 1u);
         }
         // wide photons: appended to the wide list (one atomic per warp)
@@ -157,7 +177,7 @@ __global__ __launch_bounds__(256) void plan_kernel(PlanArgs a) {
     __shared__ uint32_t red[2];
     if (threadIdx.x < 2) red[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t wend = min(int64_t(kWindow), int64_t(a.key_big) - int64_t(kb0));
+    const int64_t wend = min(int64_t(a.window), int64_t(a.key_big) - int64_t(kb0));
     for (int j = threadIdx.x; j < wend; j += blockDim.x)
         if (hist[j]) atomicAdd(a.counts + kb0 + j, hist[j]);
     c_tile = __reduce_add_sync(0xFFFFFFFFu, c_tile);
@@ -264,20 +284,20 @@ __global__ __launch_bounds__(kScanThreads) void bucket_down(const uint32_t* __re
 
 // ------------------------------------------------------------------ scatter ------------
 
-__global__ __launch_bounds__(256) void bucket_scatter(ScatterArgs a) {
-    __shared__ uint32_t hist[kWindow];
+__global__ __launch_bounds__(kPlanThreads) void bucket_scatter(ScatterArgs a) {
+    extern __shared__ uint32_t hist[];  // a.window buckets
     const int64_t r0 = int64_t(blockIdx.x) * a.range, r1 = min(r0 + a.range, a.n);
     const uint32_t kb0 = window_base(a.sims, r0, a.cb);
-    zero_window(hist);
+    zero_window(hist, a.window);
     __syncthreads();
     // the CTA's count per window bucket (as plan_kernel counted them)
     for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         const uint32_t j = __ldg(a.keys + i) - kb0;
-        if (j < uint32_t(kWindow) && j + kb0 < a.key_big) atomicAdd(hist + j, 1u);
+        if (j < uint32_t(a.window) && j + kb0 < a.key_big) atomicAdd(hist + j, 1u);
     }
     __syncthreads();
     // reserve the CTA's share of each bucket: hist[j] becomes its first position
-    const int64_t wend = min(int64_t(kWindow), int64_t(a.key_big) - int64_t(kb0));
+    const int64_t wend = min(int64_t(a.window), int64_t(a.key_big) - int64_t(kb0));
     for (int j = threadIdx.x; j < wend; j += blockDim.x) {
         const uint32_t c = hist[j];
         if (c) hist[j] = atomicAdd(a.cursor + kb0 + j, c);
@@ -287,7 +307,7 @@ __global__ __launch_bounds__(256) void bucket_scatter(ScatterArgs a) {
         const uint32_t key = __ldg(a.keys + i);
         if (key < a.key_big) {
             const uint32_t j = key - kb0;
-            const uint32_t pos = j < uint32_t(kWindow) ? atomicAdd(hist + j, 1u)
+            const uint32_t pos = j < uint32_t(a.window) ? atomicAdd(hist + j, 1u)
                                                        : atomicAdd(a.cursor + key, 1u);
             a.srecs[pos] = a.recs[i];
             a.inv[i] = pos;
@@ -329,18 +349,41 @@ unsigned capped_blocks(int64_t items, int per_sm) {
 
 int64_t bucket_scan_parts(int64_t nb) { return (nb + kScanItems - 1) / kScanItems; }
 
-// Photons per CTA of the plan and scatter kernels: enough CTAs for four per SM, each a
-// multiple of 256 photons and at least 4096 (the window's flush is amortised over them).
-int64_t plan_range(int64_t n) {
-    const int64_t ctas = int64_t(num_sms()) * 4;
+template <typename K>
+cudaError_t window_smem(K kernel, int32_t window) {
+    const size_t smem = size_t(window) * 4;
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+}
+
+// Window and photons per CTA of the plan and scatter kernels: the window holds a
+// simulation's buckets where it can (at most kMaxWindow); as many CTAs per SM as the window's
+// shared memory allows (the kernels' shared-memory limit is raised first, or the occupancy
+// query would see a kernel that cannot launch), and the photons are split evenly over one
+// wave of them (at least 8192 a CTA, so the window's clear and flush are amortised).
+void plan_shape(int64_t n, int64_t nb, int32_t* window, int64_t* range) {
+    const int64_t w = nb < kMaxWindow ? nb : kMaxWindow;
+    *window = int32_t(w > 0 ? w : 1);
+    const size_t smem = size_t(*window) * 4;
+    int per_sm = 1;
+    if (window_smem(plan_kernel, *window) != cudaSuccess ||
+        window_smem(bucket_scatter, *window) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plan_kernel, kPlanThreads,
+                                                      smem) != cudaSuccess)
+        per_sm = 1;
+    if (per_sm < 1) per_sm = 1;
+    const int64_t ctas = int64_t(num_sms()) * per_sm;
     int64_t r = (n + ctas - 1) / ctas;
-    r = (r + 255) / 256 * 256;
-    return r < 4096 ? 4096 : r;
+    r = (r + kPlanThreads - 1) / kPlanThreads * kPlanThreads;
+    *range = r < 8192 ? 8192 : r;
 }
 
 cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st) {
     if (a.ph.n <= 0) return cudaSuccess;
-    plan_kernel<<<unsigned((a.ph.n + a.range - 1) / a.range), 256, 0, st>>>(a);
+    cudaError_t e = window_smem(plan_kernel, a.window);
+    if (e != cudaSuccess) return e;
+    plan_kernel<<<unsigned((a.ph.n + a.range - 1) / a.range), kPlanThreads,
+                  size_t(a.window) * 4, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -352,7 +395,10 @@ cudaError_t launch_bucket_sort(const ScatterArgs& a, cudaStream_t st) {
                                                        a.cursor);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || a.n <= 0) return e;
-    bucket_scatter<<<unsigned((a.n + a.range - 1) / a.range), 256, 0, st>>>(a);
+    e = window_smem(bucket_scatter, a.window);
+    if (e != cudaSuccess) return e;
+    bucket_scatter<<<unsigned((a.n + a.range - 1) / a.range), kPlanThreads,
+                     size_t(a.window) * 4, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     chunk_tile_kernel<<<capped_blocks((a.n + a.chunk - 1) / a.chunk, 4), 256, 0, st>>>(a);

@@ -915,19 +915,25 @@ __global__ __launch_bounds__(256) void tail_bwd_kernel(TileArgs a) {
 // grad_Mp[2][3][N] (column 2 of grad_Mp is zero, :212, :218) in photon order: each photon's
 // record is one 32-byte gather through the plan's inverse map, the writes are coalesced.
 // Photons that touch no pixel get zeros.
+__device__ __forceinline__ void grad_record(const TileArgs& a, int64_t n, int64_t n_tile,
+                                            uint32_t v, float4& lo, float4& hi) {
+    const float4* st = reinterpret_cast<const float4*>(a.stage);
+    const int64_t slot = (v & kWideBit) ? n_tile + int64_t(v & ~kWideBit) : int64_t(v);
+    lo = make_float4(0.f, 0.f, 0.f, 0.f);
+    hi = lo;
+    if (v != kInvalidPos && slot < n) {
+        lo = st[2 * slot];
+        hi = st[2 * slot + 1];
+    }
+}
+
 __global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
     const int64_t n = a.ph.n;
     const int64_t n_tile = tile_count(a);
-    const float4* st = reinterpret_cast<const float4*>(a.stage);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x) {
-        const uint32_t v = __ldg(a.inv + i);
-        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
-        const int64_t slot = (v & kWideBit) ? n_tile + int64_t(v & ~kWideBit) : int64_t(v);
-        if (v != kInvalidPos && slot < n) {
-            lo = st[2 * slot];
-            hi = st[2 * slot + 1];
-        }
+        float4 lo, hi;
+        grad_record(a, n, n_tile, __ldg(a.inv + i), lo, hi);
         a.gE[i] = lo.x;
         a.gX[i] = lo.y;
         a.gX[n + i] = lo.z;
@@ -937,6 +943,36 @@ __global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
         a.gM[3 * n + i] = hi.y;
         a.gM[4 * n + i] = hi.z;
         a.gM[5 * n + i] = 0.f;
+    }
+}
+
+// The same for 4 photons per thread when N is a multiple of 4 and the outputs are 16-byte
+// aligned: one 16-byte store per output row instead of four.
+__global__ __launch_bounds__(256) void grad_scatter4_kernel(TileArgs a) {
+    const int64_t n = a.ph.n, nq = n >> 2;
+    const int64_t n_tile = tile_count(a);
+    const uint4* inv4 = reinterpret_cast<const uint4*>(a.inv);
+    float4* gE = reinterpret_cast<float4*>(a.gE);
+    float4* gX = reinterpret_cast<float4*>(a.gX);
+    float4* gM = reinterpret_cast<float4*>(a.gM);
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq;
+         q += int64_t(gridDim.x) * blockDim.x) {
+        const uint4 v = __ldg(inv4 + q);
+        float4 l0, h0, l1, h1, l2, h2, l3, h3;
+        grad_record(a, n, n_tile, v.x, l0, h0);
+        grad_record(a, n, n_tile, v.y, l1, h1);
+        grad_record(a, n, n_tile, v.z, l2, h2);
+        grad_record(a, n, n_tile, v.w, l3, h3);
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        gE[q] = make_float4(l0.x, l1.x, l2.x, l3.x);
+        gX[q] = make_float4(l0.y, l1.y, l2.y, l3.y);
+        gX[nq + q] = make_float4(l0.z, l1.z, l2.z, l3.z);
+        gM[q] = make_float4(l0.w, l1.w, l2.w, l3.w);
+        gM[nq + q] = make_float4(h0.x, h1.x, h2.x, h3.x);
+        gM[2 * nq + q] = z;
+        gM[3 * nq + q] = make_float4(h0.y, h1.y, h2.y, h3.y);
+        gM[4 * nq + q] = make_float4(h0.z, h1.z, h2.z, h3.z);
+        gM[5 * nq + q] = z;
     }
 }
 
@@ -1015,9 +1051,19 @@ cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
         tail_bwd_kernel<<<tgrid, 256, 0, st>>>(a);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        const int64_t sblocks = (a.ph.n + 255) / 256;
+        const auto al16 = [](const void* p) {
+            return (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+        };
+        const bool vec = (a.ph.n & 3) == 0 && al16(a.gE) && al16(a.gX) && al16(a.gM) &&
+                         al16(a.inv);
+        const int64_t items = vec ? a.ph.n / 4 : a.ph.n;
+        const int64_t sblocks = (items + 255) / 256;
         const int64_t scap = int64_t(num_sms()) * 16;
-        grad_scatter_kernel<<<unsigned(sblocks < scap ? sblocks : scap), 256, 0, st>>>(a);
+        const unsigned sgrid = unsigned(sblocks < scap ? sblocks : scap);
+        if (vec)
+            grad_scatter4_kernel<<<sgrid, 256, 0, st>>>(a);
+        else
+            grad_scatter_kernel<<<sgrid, 256, 0, st>>>(a);
         e = cudaGetLastError();
     }
     return e;

@@ -30,7 +30,8 @@ struct PlanArgs {
     uint32_t* inv;       // [n] out for wide (kWideBit | k) and untouched (kInvalidPos) photons
     uint32_t* wide;      // [n] out: photon index of the k-th wide photon
     uint32_t* counters;  // [0] tile-path, [1] wide, [2] untouched photons; zeroed by caller
-    int64_t range;       // photons per CTA (plan_range)
+    int64_t range;       // photons per CTA (plan_shape)
+    int32_t window;      // buckets of each CTA's shared histogram (plan_shape)
 };
 
 // Bucket scan and scatter of the plan.
@@ -47,7 +48,8 @@ struct ScatterArgs {
     uint32_t* inv;         // [n] out for tile-path photons: sorted position
     uint32_t* chunk_tile;  // [n / chunk + 1] out: tile of each work chunk's first photon
     int64_t n, nb, n_tiles;
-    int64_t range;         // photons per CTA, as in the plan
+    int64_t range;         // photons per CTA and histogram window, as in the plan
+    int32_t window;
     uint32_t key_big;
     int32_t chunk, cb;
 };
@@ -75,7 +77,7 @@ struct TileArgs {
 };
 
 int64_t bucket_scan_parts(int64_t nb);
-int64_t plan_range(int64_t n);
+void plan_shape(int64_t n, int64_t nb, int32_t* window, int64_t* range);
 cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st);
 cudaError_t launch_bucket_sort(const ScatterArgs& a, cudaStream_t st);
 cudaError_t launch_forward(const TileArgs& a, cudaStream_t st);

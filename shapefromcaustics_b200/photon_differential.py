@@ -6,8 +6,8 @@ output_size, max_pixel_radius)`` returns the ``[C,H,W]`` photon map and its back
 
 Difference from the reference: the forward's photon binning and sort (the plan) is kept for
 the backward instead of being recomputed. ``set_keep_plan(False)`` drops it after the forward
-and rebuilds it in the backward, trading one binning pass for ~40 bytes per photon of device
-memory held between the passes.
+and rebuilds it in the backward, trading one binning pass for the plan's workspace (about 76
+bytes per photon) held between the passes.
 """
 import torch
 
