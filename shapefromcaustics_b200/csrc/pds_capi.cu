@@ -66,7 +66,20 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
     return PDS_OK;
 }
 
-int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
+// Photons per tile-kernel work chunk: the configured chunk, lowered for small photon counts
+// so that every resident CTA of the tile kernels (3 per SM) gets about four chunks; at least
+// 256 photons (one CTA-wide batch).
+int32_t effective_chunk(int32_t chunk, int64_t n) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    const int64_t target = (n + int64_t(sms) * 12 - 1) / (int64_t(sms) * 12);
+    const int64_t c = (target + 255) / 256 * 256;
+    return int32_t(c < 256 ? 256 : (c < chunk ? c : chunk));
+}
+
+int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, int64_t n, Resolved& r) {
     pds_config c;
     int rc = resolve_cfg(in, c);
     if (rc) return rc;
@@ -76,7 +89,7 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, Resolved& r) {
     if (inv >= (uint64_t(1) << 32))
         return fail(PDS_ERR_UNSUPPORTED, "sort key space exceeds 32 bits; lower class_bits");
     r.cfg.tile = c.tile;
-    r.cfg.chunk = c.chunk;
+    r.cfg.chunk = effective_chunk(c.chunk, n);
     r.cfg.class_bits = c.class_bits;
     r.cfg.apron = mpr < 0 ? 0 : (mpr < c.apron_max ? mpr : c.apron_max);
     // odd pitch: the rows of one column of the accumulator fall in different banks
@@ -220,7 +233,7 @@ pds::SimTable table_dev(const pds_sim* dev, int32_t n) {
 int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, int32_t mpr,
               const pds_config* cfg, void* ws, size_t ws_bytes, cudaStream_t s) {
     Resolved r;
-    int rc = resolve(cfg, mpr, n_tiles, r);
+    int rc = resolve(cfg, mpr, n_tiles, ph.n, r);
     if (rc) return rc;
     const Layout L = make_layout(ph.n, r.n_buckets);
     rc = check_ws(ws, ws_bytes, L.total);
@@ -273,7 +286,7 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
 int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, int32_t mpr,
               const pds_config* cfg, void* ws, size_t ws_bytes, pds::TileArgs& a) {
     Resolved r;
-    int rc = resolve(cfg, mpr, n_tiles, r);
+    int rc = resolve(cfg, mpr, n_tiles, ph.n, r);
     if (rc) return rc;
     const Layout L = make_layout(ph.n, r.n_buckets);
     rc = check_ws(ws, ws_bytes, L.total);

@@ -946,15 +946,27 @@ __global__ __launch_bounds__(256) void grad_scatter_kernel(TileArgs a) {
     }
 }
 
-// The same for 4 photons per thread when N is a multiple of 4 and the outputs are 16-byte
-// aligned: one 16-byte store per output row instead of four.
+// The same for 4 photons per thread: quad q holds photons 4q..4q+3 and each output row takes
+// them in one 16-byte store, two 8-byte stores or four 4-byte stores, as the row's start
+// allows (row r starts N * r elements after its array's start, so for N not a multiple of 4
+// rows differ in alignment). The last N % 4 photons are written one by one.
+__device__ __forceinline__ void store_quad(float* p, float4 v) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    if ((a & 15) == 0) {
+        *reinterpret_cast<float4*>(p) = v;
+    } else if ((a & 7) == 0) {
+        reinterpret_cast<float2*>(p)[0] = make_float2(v.x, v.y);
+        reinterpret_cast<float2*>(p)[1] = make_float2(v.z, v.w);
+    } else {
+        p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
+    }
+}
+
 __global__ __launch_bounds__(256) void grad_scatter4_kernel(TileArgs a) {
     const int64_t n = a.ph.n, nq = n >> 2;
     const int64_t n_tile = tile_count(a);
     const uint4* inv4 = reinterpret_cast<const uint4*>(a.inv);
-    float4* gE = reinterpret_cast<float4*>(a.gE);
-    float4* gX = reinterpret_cast<float4*>(a.gX);
-    float4* gM = reinterpret_cast<float4*>(a.gM);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq;
          q += int64_t(gridDim.x) * blockDim.x) {
         const uint4 v = __ldg(inv4 + q);
@@ -963,16 +975,32 @@ __global__ __launch_bounds__(256) void grad_scatter4_kernel(TileArgs a) {
         grad_record(a, n, n_tile, v.y, l1, h1);
         grad_record(a, n, n_tile, v.z, l2, h2);
         grad_record(a, n, n_tile, v.w, l3, h3);
-        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-        gE[q] = make_float4(l0.x, l1.x, l2.x, l3.x);
-        gX[q] = make_float4(l0.y, l1.y, l2.y, l3.y);
-        gX[nq + q] = make_float4(l0.z, l1.z, l2.z, l3.z);
-        gM[q] = make_float4(l0.w, l1.w, l2.w, l3.w);
-        gM[nq + q] = make_float4(h0.x, h1.x, h2.x, h3.x);
-        gM[2 * nq + q] = z;
-        gM[3 * nq + q] = make_float4(h0.y, h1.y, h2.y, h3.y);
-        gM[4 * nq + q] = make_float4(h0.z, h1.z, h2.z, h3.z);
-        gM[5 * nq + q] = z;
+        const int64_t i = 4 * q;
+        store_quad(a.gE + i, make_float4(l0.x, l1.x, l2.x, l3.x));
+        store_quad(a.gX + i, make_float4(l0.y, l1.y, l2.y, l3.y));
+        store_quad(a.gX + n + i, make_float4(l0.z, l1.z, l2.z, l3.z));
+        store_quad(a.gM + i, make_float4(l0.w, l1.w, l2.w, l3.w));
+        store_quad(a.gM + n + i, make_float4(h0.x, h1.x, h2.x, h3.x));
+        store_quad(a.gM + 2 * n + i, z);
+        store_quad(a.gM + 3 * n + i, make_float4(h0.y, h1.y, h2.y, h3.y));
+        store_quad(a.gM + 4 * n + i, make_float4(h0.z, h1.z, h2.z, h3.z));
+        store_quad(a.gM + 5 * n + i, z);
+    }
+    // the last n % 4 photons
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < (n & 3)) {
+        const int64_t i = 4 * nq + t;
+        float4 lo, hi;
+        grad_record(a, n, n_tile, __ldg(a.inv + i), lo, hi);
+        a.gE[i] = lo.x;
+        a.gX[i] = lo.y;
+        a.gX[n + i] = lo.z;
+        a.gM[i] = lo.w;
+        a.gM[n + i] = hi.x;
+        a.gM[2 * n + i] = 0.f;
+        a.gM[3 * n + i] = hi.y;
+        a.gM[4 * n + i] = hi.z;
+        a.gM[5 * n + i] = 0.f;
     }
 }
 
@@ -1051,13 +1079,14 @@ cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
         tail_bwd_kernel<<<tgrid, 256, 0, st>>>(a);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        const auto al16 = [](const void* p) {
-            return (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+        // the quad form needs the inverse map 16-byte aligned (the workspace is) and every
+        // output 4-byte aligned; the rows' own alignment is handled per store
+        const auto al = [](const void* p, uintptr_t m) {
+            return (reinterpret_cast<uintptr_t>(p) & m) == 0;
         };
-        const bool vec = (a.ph.n & 3) == 0 && al16(a.gE) && al16(a.gX) && al16(a.gM) &&
-                         al16(a.inv);
+        const bool vec = al(a.inv, 15) && al(a.gE, 3) && al(a.gX, 3) && al(a.gM, 3);
         const int64_t items = vec ? a.ph.n / 4 : a.ph.n;
-        const int64_t sblocks = (items + 255) / 256;
+        const int64_t sblocks = items > 0 ? (items + 255) / 256 : 1;
         const int64_t scap = int64_t(num_sms()) * 16;
         const unsigned sgrid = unsigned(sblocks < scap ? sblocks : scap);
         if (vec)
