@@ -58,8 +58,8 @@ typedef struct pds_config {
                            3 = a sheared band of equal-width rows around the support
                            (2 and 3 give the same result: pixels outside the support add
                            exactly zero); default 3 */
-    int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2 (more
-                           registers per thread) or 3 (more warps); default 3 */
+    int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2, 3 or 4
+                           (fewer: more registers per thread; more: more warps); default 3 */
     int32_t coop_radius; /* footprints with a radius (px) of at least this are splatted by a
                            whole warp instead of one thread; -1 never; default -1 */
 } pds_config;
@@ -194,6 +194,16 @@ int pds_refract_backward_f32(const float* height, int32_t rows, int32_t cols,
                              const float* flux, int64_t n_photons, const float* grad_Ep,
                              const float* grad_xp, const float* grad_Mp, float* grad_height,
                              void* stream);
+
+/* Entry points of rows * cols * per_texel photons (per_texel per texel of a rows x cols
+ * height field of edge `texel`, centred on the origin), each jittered uniformly inside its
+ * texel (the reference's per-pixel random surface samples, model/caustics.py:78-83):
+ * px[i], py[i] for photon i = texel index * per_texel + k. The offsets come from Philox4x32-10
+ * (Salmon et al., SC 2011) keyed by `seed`; photons 2j and 2j + 1 use counter block
+ * offset + j, so a call is a pure function of (seed, offset) and calls with offsets advanced
+ * by ceil(n / 2) draw disjoint streams. */
+int pds_photon_source_f32(int32_t rows, int32_t cols, int32_t per_texel, float texel,
+                          uint64_t seed, uint64_t offset, float* px, float* py, void* stream);
 
 /* ---- projected Landweber update of the height field ------------------------------- */
 /* One update of the reference's pixel-basis Landweber loop (shape_from_caustics.py:386-398):

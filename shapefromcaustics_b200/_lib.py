@@ -84,6 +84,8 @@ SIGNATURES = {
                                                _P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "pds_refract_backward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate), _P, _P,
                                                 _P, _I64, _P, _P, _P, _P, _P]),
+    "pds_photon_source_f32": (ctypes.c_int, [_I32, _I32, _I32, ctypes.c_float, ctypes.c_uint64,
+                                             ctypes.c_uint64, _P, _P, _P]),
     "pds_landweber_workspace_bytes": (_SZ, [_I64, _I64]),
     "pds_landweber_update_f32": (ctypes.c_int, [_P, _P, _P, _I64, _I64,
                                                 ctypes.POINTER(PdsLandweber), _P, _SZ, _P]),

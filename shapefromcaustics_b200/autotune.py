@@ -17,7 +17,7 @@ from . import _lib
 __all__ = ["CANDIDATES", "signature", "tune_batch", "cached"]
 
 CANDIDATES = [dict(tile=t, chunk=c, class_bits=b, walk=w, min_blocks=m, coop_radius=-1)
-              for t, c, b, w, m in itertools.product((32, 64), (2048,), (3, 5), (1, 3), (2, 3))]
+              for t, c, b, w, m in itertools.product((32, 64), (2048,), (3, 5), (1, 3), (3, 4))]
 
 _cache = {}
 

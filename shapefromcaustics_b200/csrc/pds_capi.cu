@@ -48,8 +48,8 @@ int resolve_cfg(const pds_config* in, pds_config& out) {
     out.coop_radius = (in && in->coop_radius) ? in->coop_radius : -1;
     if (out.coop_radius < -1 || out.coop_radius > 63)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.coop_radius must be -1 or in [1, 63]");
-    if (out.min_blocks != 2 && out.min_blocks != 3)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.min_blocks must be 2 or 3");
+    if (out.min_blocks < 2 || out.min_blocks > 4)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.min_blocks must be 2, 3 or 4");
     if (out.walk < 1 || out.walk > 3)
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.walk must be 1 (box), 2 (support spans) or 3 (support band)");
@@ -548,6 +548,21 @@ int pds_refract_backward_f32(const float* h, int32_t rows, int32_t cols, const p
                                         nullptr, nullptr, nullptr, nullptr, nullptr, gE, gX, gM,
                                         gh, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel");
+    return PDS_OK;
+}
+
+int pds_photon_source_f32(int32_t rows, int32_t cols, int32_t per_texel, float texel,
+                          uint64_t seed, uint64_t offset, float* px, float* py, void* stream) {
+    if (rows < 1 || cols < 1 || per_texel < 1)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "rows, cols and per_texel must be positive");
+    const int64_t n = int64_t(rows) * cols * per_texel;
+    if (n >= int64_t(0x7FFFFFFFll))
+        return fail(PDS_ERR_UNSUPPORTED, "photon count must be below 2^31 - 1");
+    if (!(texel > 0.f)) return fail(PDS_ERR_INVALID_ARGUMENT, "texel must be positive");
+    if (!px || !py) return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
+    cudaError_t e = pds::launch_source(rows, cols, per_texel, texel, seed, offset, n, px, py,
+                                       static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "source_kernel");
     return PDS_OK;
 }
 

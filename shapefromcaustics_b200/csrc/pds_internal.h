@@ -26,6 +26,11 @@ cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pd
                            int64_t* cp, float* radius, const float* gE, const float* gX,
                            const float* gM, float* gh, cudaStream_t st);
 
+// photon source (pds_source.cu)
+cudaError_t launch_source(int32_t rows, int32_t cols, int32_t per_texel, float texel,
+                          uint64_t seed, uint64_t offset, int64_t n, float* px, float* py,
+                          cudaStream_t st);
+
 // Landweber update (pds_landweber.cu)
 size_t landweber_scratch_bytes(int64_t n);
 cudaError_t launch_landweber(float* d, const float* g, const float* mask, int64_t rows,

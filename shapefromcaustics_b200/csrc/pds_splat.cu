@@ -1099,11 +1099,13 @@ cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
-    return a.cfg.min_blocks >= 3 ? launch_forward_t<3>(a, st) : launch_forward_t<2>(a, st);
+    if (a.cfg.min_blocks >= 4) return launch_forward_t<4>(a, st);
+    return a.cfg.min_blocks == 3 ? launch_forward_t<3>(a, st) : launch_forward_t<2>(a, st);
 }
 
 cudaError_t launch_backward(const TileArgs& a, cudaStream_t st) {
-    return a.cfg.min_blocks >= 3 ? launch_backward_t<3>(a, st) : launch_backward_t<2>(a, st);
+    if (a.cfg.min_blocks >= 4) return launch_backward_t<4>(a, st);
+    return a.cfg.min_blocks == 3 ? launch_backward_t<3>(a, st) : launch_backward_t<2>(a, st);
 }
 
 }  // namespace pds

@@ -96,6 +96,20 @@ def render_plate(height, scene, px, py, flux, params, shape, max_pixel_radius=20
         return PlateSplat.apply(height, px, py, flux, params, shape, max_pixel_radius, False)
 
 
+def photon_source(H, W, per_texel, texel, seed, offset, device):
+    """Entry points of ``per_texel`` uniformly jittered photons per texel from the device
+    source (``pds_photon_source_f32``: Philox4x32-10 keyed by ``seed``, counter blocks from
+    ``offset``, two photons a block). Returns ``(px, py, next_offset)``; passing
+    ``next_offset`` to the next call draws a disjoint stream."""
+    n = H * W * per_texel
+    px = torch.empty(n, dtype=torch.float32, device=device)
+    py = torch.empty(n, dtype=torch.float32, device=device)
+    with torch.cuda.device(px.device):
+        check(lib().pds_photon_source_f32(H, W, per_texel, float(texel), int(seed) & (2 ** 64 - 1),
+                                          int(offset), _ptr(px), _ptr(py), _stream(px.device)))
+    return px, py, int(offset) + (n + 1) // 2
+
+
 def jitter(H, W, scene, per_texel, generator, device):
     """Entry points of ``per_texel`` uniformly jittered photons per texel, on the device."""
     n = H * W * per_texel
@@ -130,12 +144,11 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
     du0 = footprint_px * 2.0 * scene.receiver_half / image
     pp = plate_params(scene, du0)
     shape = (1, image, image)
-    g = torch.Generator(device=dev)
-    g.manual_seed(seed)
     flux = torch.full((n,), 1.0 / n, device=dev)
     d_true = h_true - base
+    offset = 0
     if target is None:
-        px, py = jitter(H, W, scene, per_texel * sims, g, dev)
+        px, py, offset = photon_source(H, W, per_texel * sims, scene.texel, seed, offset, dev)
         target = render_plate(h_true, scene, px, py, flux, pp, shape)
     tnorm2 = float((target * target).sum())
     if params is None:
@@ -147,7 +160,7 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
     ws = None
     hist = {"discrepancy": [], "rmse": []}
     for it in range(iterations):
-        px, py = jitter(H, W, scene, per_texel * sims, g, dev)
+        px, py, offset = photon_source(H, W, per_texel * sims, scene.texel, seed, offset, dev)
         hv = (base + d).requires_grad_(True)
         img = PlateSplat.apply(hv, px, py, flux, pp, shape, 20, keep_plan)
         diff = img - target

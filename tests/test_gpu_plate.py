@@ -113,3 +113,27 @@ def test_landweber_update_matches_reference_ops(cuda, vol):
     out = landweber_update(d.cuda(), grad.cuda(), mask.cuda(), p)
     torch.cuda.synchronize()
     assert rel_l2(out.cpu(), ref) < 1e-5
+
+
+def test_photon_source_matches_philox_restatement(cuda):
+    """The device photon source reproduces the numpy Philox4x32-10 restatement bit for bit
+    (odd photon count, nonzero counter offset, 64-bit seed), and successive calls advanced by
+    the returned offset draw disjoint streams."""
+    from oracle import philox as P
+    from shapefromcaustics_b200.landweber import photon_source
+    seed = 0x1234_5678_9ABC
+    px, py, nxt = photon_source(5, 7, 3, 0.25, seed, 11, "cuda")
+    torch.cuda.synchronize()
+    rx, ry = P.photon_source(5, 7, 3, 0.25, seed, 11)
+    assert nxt == 11 + 53
+    assert np.array_equal(px.cpu().numpy(), rx) and np.array_equal(py.cpu().numpy(), ry)
+    qx, qy, _ = photon_source(5, 7, 3, 0.25, seed, nxt, "cuda")
+    sx, sy = P.photon_source(5, 7, 3, 0.25, seed, nxt)
+    assert np.array_equal(qx.cpu().numpy(), sx)
+    assert not np.array_equal(qx.cpu().numpy(), rx)
+    # many photons: offsets uniform inside the texel
+    px, py, _ = photon_source(64, 64, 16, 1.0, 7, 0, "cuda")
+    t = torch.arange(px.numel(), device="cuda") // 16
+    jx = (px - ((t % 64).float() - 31.5)).cpu().numpy()
+    assert abs(jx.mean()) < 5e-3 and abs(jx.var() - 1 / 12) < 2e-3
+    assert jx.min() >= -0.5 and jx.max() <= 0.5  # (ix + j rounds to the texel edge at most)

@@ -74,7 +74,8 @@ def test_uniform_cluster_512(cuda):
                                  dict(walk=2, tile=16, class_bits=1), dict(min_blocks=2),
                                  dict(coop_radius=1), dict(coop_radius=-1),
                                  dict(coop_radius=2, min_blocks=2), dict(walk=1),
-                                 dict(walk=1, coop_radius=5), dict(walk=3, coop_radius=4, tile=32)])
+                                 dict(walk=1, coop_radius=5), dict(walk=3, coop_radius=4, tile=32),
+                                 dict(min_blocks=4), dict(min_blocks=4, class_bits=3)])
 def test_tuning_variants(cuda, cfg):
     ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
     assert_parity(ph, (1, 256, 256), 20, cfg=cfg)

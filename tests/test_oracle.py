@@ -163,3 +163,25 @@ def test_oracle_stable_sort_matches_numpy():
     rng = np.random.default_rng(1)
     keys = rng.integers(0, 300, 10000).astype(np.uint32)
     assert np.array_equal(O.stable_sort_u32(keys), np.argsort(keys, kind="stable"))
+
+
+def test_philox_known_answers():
+    """The numpy Philox4x32-10 (checker of the device photon source) against the published
+    known-answer vectors of the algorithm."""
+    from oracle import philox as P
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+             ((0xffffffff,) * 4, (0xffffffff,) * 2, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+             ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+              (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for ctr, key, want in cases:
+        got = P.philox4x32_10([np.array([w], dtype=np.uint64) for w in ctr], key)[:, 0]
+        assert [int(v) for v in got] == list(want)
+
+
+def test_photon_source_restatement_stays_in_texels():
+    from oracle import philox as P
+    px, py = P.photon_source(5, 7, 3, 0.25, seed=99, offset=4)
+    assert px.shape == (105,) and px.dtype == np.float32
+    t = np.arange(105) // 3
+    assert np.all(np.abs(px / 0.25 - (t % 7 - 3.0)) <= 0.5)
+    assert np.all(np.abs(py / 0.25 - (t // 7 - 2.0)) <= 0.5)
