@@ -1,7 +1,7 @@
-// Stable LSD radix sort of 32-bit keys with a 32-bit index payload, for sm_100a.
-//
-// The splatting plan sorts photons by (simulation, channel, screen tile, footprint class);
-// the permutation must equal a CPU stable sort bit for bit, so every pass is stable:
+// Stable LSD radix sort of 32-bit keys with a 32-bit index payload, for sm_100a, exposed as
+// pds_sort_u32. (The splatting plan bins photons with a counting sort by bucket, pds_plan.cu;
+// this sort serves callers that need the stable order of arbitrary keys.) The permutation
+// equals a CPU stable sort bit for bit, so every pass is stable:
 //   upsweep    per 2048-key block digit counts (warp-aggregated shared atomics), block-major
 //   col scan   column-wise exclusive scan of the [blocks][radix] count matrix in three
 //              coalesced kernels (group partials, one-CTA top scan with digit bases, group
