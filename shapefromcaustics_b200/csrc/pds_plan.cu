@@ -7,7 +7,7 @@
 //                    a bucket (simulation, channel, screen tile of the centre pixel, footprint
 //                    class) and a 32-byte record in photon order. Each CTA takes a contiguous
 //                    photon range (one or two simulations) and counts its buckets in a
-//                    shared-memory histogram over the window of buckets (up to 12160) that
+//                    shared-memory histogram over the window of buckets (up to 32768) that
 //                    starts at its first photon's simulation; the histogram is added into the
 //                    global counts once per CTA. Photons wider than the apron go to the wide
 //                    list.
@@ -48,9 +48,9 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // with one photon in flight; the scatter measured slower with two photons a thread).
 constexpr int kPlanThreads = 1024;      // bucket_scatter
 constexpr int kPlanKernelThreads = 768;  // plan_kernel
-// buckets of a CTA's shared histogram (47.5 KB, which leaves the SM most of its L1 cache for
-// the simulation table and the streamed loads)
-constexpr int kMaxWindow = 12160;
+// buckets of a CTA's shared histogram (128 KB: a 2048^2 image's buckets at 5 class bits; the
+// SM keeps about 100 KB of L1 cache for the streamed loads)
+constexpr int kMaxWindow = 32768;
 
 // First bucket of the simulation owning photon i.
 __device__ __forceinline__ uint32_t window_base(const SimTable& st, int64_t i, int cb) {
