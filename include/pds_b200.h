@@ -46,7 +46,9 @@ extern "C" {
 /* Kernel tuning. A NULL pointer or a zero field selects the default. */
 typedef struct pds_config {
     int32_t tile;       /* screen-tile edge in pixels: 16, 32 or 64 (default 64) */
-    int32_t chunk;      /* sorted photons per CTA work item, multiple of 256 (default 2048) */
+    int32_t chunk;      /* sorted photons per CTA work item, multiple of 256 (default 2048;
+                           lowered, to no less than 256, when the call has too few photons to
+                           give every resident tile CTA about four work items) */
     int32_t class_bits; /* footprint-size bits appended to the sort key (photons of a tile
                            are then grouped by footprint size; with the band walk, classes
                            of 1/k octave of the band's area, k = 1 up to 3 bits, 2 for 4,
