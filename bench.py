@@ -268,12 +268,19 @@ def time_graph(graph, steps, stream):
 
 
 def run_ours(args, rank, world, device):
+    from shapefromcaustics_b200 import _lib
     from shapefromcaustics_b200.splatting import BatchedSplat, SplatPlan
     torch.cuda.set_device(device)
     specs, photons, gflat, desc = workload(args.workload, rank, device)
     n_total = sum(n for n, _ in specs)
     pixels = sum(C * H * W for _, (C, H, W) in specs)
-    batch = BatchedSplat(specs, MPR, device)
+    # the project's autotuner picks the launch configuration on this workload (untimed)
+    tuned = None
+    if not (args.no_autotune or args.lean):
+        from shapefromcaustics_b200 import autotune
+        tuned, _ = autotune.tune_batch(specs, photons, gflat, MPR, device, reps=2)
+    cfg = _lib.config(**tuned) if tuned else None
+    batch = BatchedSplat(specs, MPR, device, config=cfg)
     out = torch.empty(batch.image_elems, device=device)
     grads = tuple(torch.empty_like(t) for t in photons[:3])
     stream = torch.cuda.Stream(device)
@@ -348,7 +355,7 @@ def run_ours(args, rank, world, device):
 
     def plain_step():
         for (n, shape), ph, g in zip(specs, per_sim, gviews):
-            p = SplatPlan(*ph, shape, MPR)
+            p = SplatPlan(*ph, shape, MPR, config=cfg)
             p.forward()
             p.backward(g)
 
@@ -466,7 +473,8 @@ def run_ours(args, rank, world, device):
                    "simulations_per_gpu": len(specs), "image_pixels_per_gpu": pixels,
                    "max_pixel_radius": MPR, "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"simulation-sharded x{world}, no collective",
-                   "mode": "batched: one CUDA graph per step (plan + fwd + bwd)"},
+                   "mode": "batched: one CUDA graph per step (plan + fwd + bwd)",
+                   "launch_config": tuned or "library default"},
         "landweber_it_per_s": {"batched": 1e3 / ms_per_step, "plain": 1e3 / plain_ms,
                                "batched_over_plain": plain_ms / ms_per_step},
         "phase_ms": ph_ms,
@@ -681,6 +689,16 @@ def run_landweber_step(args, rank, world, device):
     params = LandweberParams(d1=0.75 * vol, d2=1.25 * vol)
     tn = float((target * target).sum())
     ws = torch.empty(1 << 22, dtype=torch.uint8, device=device)
+    # the autotuner picks the splat configuration on the first iterate's refracted photons
+    tuned = None
+    if not args.no_autotune:
+        from shapefromcaustics_b200 import autotune
+        from shapefromcaustics_b200.plate import refract_forward
+        from shapefromcaustics_b200.splatting import set_default_config
+        ph = refract_forward((base + d).contiguous(), px, py, flux, pp)
+        tuned, _ = autotune.tune_batch([(n, shape)], ph, torch.zeros(img * img, device=device),
+                                       MPR, device, reps=2)
+        set_default_config(**tuned)
 
     def step():
         hv = (base + d).requires_grad_(True)
@@ -709,7 +727,8 @@ def run_landweber_step(args, rank, world, device):
             "config": {"workload": "landweber256: 256^2 height field (1 mm + 32 bumps), 4 "
                                    "jittered photons/texel (262144), n=1.5, receiver 50 mm, "
                                    "512^2 image, L2 vs second field; refraction + splat "
-                                   "fwd/bwd + fused update", "photons": n}}
+                                   "fwd/bwd + fused update", "photons": n,
+                       "launch_config": tuned or "library default"}}
 
 
 def run_reconstruction(args, rank, world, device):
@@ -757,8 +776,11 @@ def main():
                     choices=["batch64", "uniform1m", "medium", "contention", "contention24",
                              "landweber256", "recon1024"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="time the library's default configuration instead of the tuned one")
     ap.add_argument("--lean", action="store_true",
-                    help="timed steps and phase timings only (for profiler runs)")
+                    help="timed steps and phase timings only, default configuration "
+                         "(for profiler runs)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-sample", type=float, default=2 ** 21)
     args = ap.parse_args()

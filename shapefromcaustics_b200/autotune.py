@@ -1,8 +1,9 @@
 """Autotuner for the splat kernels' launch configuration.
 
-Times candidate ``pds_config`` values (screen-tile edge, photons per CTA work item,
-footprint-class sort bits, pixel walk) on the caller's actual workload with CUDA events, and
-keeps the fastest per workload signature (photon count and image sizes, bucketed). The
+Times candidate ``pds_config`` values (screen-tile edge, footprint-class sort bits, pixel
+walk, resident CTAs per SM, warp-cooperative splat of large footprints) on the caller's
+actual workload with CUDA events, and keeps the fastest per workload signature (photon count
+and image sizes, bucketed); the first candidate is the library default, which wins ties. The
 reference has a single fixed launch shape (512 threads per photon block,
 ``photon_differentials.cu:120``); here the best tile and chunk depend on footprint sizes and
 photon density, so they are measured rather than fixed.
@@ -16,8 +17,8 @@ from . import _lib
 
 __all__ = ["CANDIDATES", "signature", "tune_batch", "cached"]
 
-CANDIDATES = [dict(tile=t, chunk=c, class_bits=b, walk=w, min_blocks=m, coop_radius=-1)
-              for t, c, b, w, m in itertools.product((32, 64), (2048,), (3, 5), (1, 3), (3, 4))]
+CANDIDATES = [dict(tile=t, chunk=2048, class_bits=b, walk=w, min_blocks=m, coop_radius=k)
+              for t, b, w, m, k in itertools.product((64, 32), (5, 3), (3, 1), (3, 4), (-1, 8))]
 
 _cache = {}
 

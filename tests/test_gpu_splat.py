@@ -314,3 +314,16 @@ def test_radix_sort_is_bit_exact_stable(cuda, n, bits):
     expect = np.argsort(keys_u, kind="stable")
     assert np.array_equal(perm, expect)
     assert np.array_equal(ko.cpu().numpy().view(np.uint32), keys_u[expect])
+
+
+def test_autotuner_picks_and_caches_a_candidate(cuda):
+    from shapefromcaustics_b200 import autotune
+    specs = S.batch_specs(4, seed=5, n_range=(2 ** 10, 2 ** 13), sizes=(64, 128))
+    photons = [t.cuda() for t in S.batch_photons(specs, seed=5)]
+    gflat = torch.cat([S.upstream_grad(shape, seed=s).reshape(-1)
+                       for s, (_, shape) in enumerate(specs)]).cuda()
+    cands = [dict(tile=64, class_bits=5), dict(tile=32, class_bits=3, walk=1)]
+    best, times = autotune.tune_batch(specs, photons, gflat, 20, torch.device("cuda"),
+                                      candidates=cands, reps=1)
+    assert best in cands and len(times) == 2 and all(t > 0 for t in times.values())
+    assert autotune.cached(specs, 20) == best
