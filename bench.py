@@ -689,17 +689,6 @@ def run_landweber_step(args, rank, world, device):
     params = LandweberParams(d1=0.75 * vol, d2=1.25 * vol)
     tn = float((target * target).sum())
     ws = torch.empty(1 << 22, dtype=torch.uint8, device=device)
-    # the autotuner picks the splat configuration on the first iterate's refracted photons
-    tuned = None
-    if not args.no_autotune:
-        from shapefromcaustics_b200 import autotune
-        from shapefromcaustics_b200.plate import refract_forward
-        from shapefromcaustics_b200.splatting import set_default_config
-        ph = refract_forward((base + d).contiguous(), px, py, flux, pp)
-        tuned, _ = autotune.tune_batch([(n, shape)], ph, torch.zeros(img * img, device=device),
-                                       MPR, device, reps=2)
-        set_default_config(**tuned)
-
     def step():
         hv = (base + d).requires_grad_(True)
         im = PlateSplat.apply(hv, px, py, flux, pp, shape, MPR, True)
@@ -728,7 +717,7 @@ def run_landweber_step(args, rank, world, device):
                                    "jittered photons/texel (262144), n=1.5, receiver 50 mm, "
                                    "512^2 image, L2 vs second field; refraction + splat "
                                    "fwd/bwd + fused update", "photons": n,
-                       "launch_config": tuned or "library default"}}
+                       "launch_config": "library default"}}
 
 
 def run_reconstruction(args, rank, world, device):
