@@ -234,6 +234,36 @@ def test_batched_uneven_simulations_match_per_simulation_oracle(cuda):
         off += n
 
 
+@pytest.mark.parametrize("cfg", [None, dict(tile=32)])
+def test_bucket_window_overflow_on_2048_images(cuda, cfg):
+    # 2048^2 images: 32768 buckets a simulation at tile 64 (the plan's whole shared window) and
+    # 131072 at tile 32, so CTAs that straddle the two simulations, or whose photons reach past
+    # the window inside one, count and place those photons with global atomics
+    from shapefromcaustics_b200 import _lib
+    from shapefromcaustics_b200.splatting import BatchedSplat
+    specs = [(2 ** 18 + 3001, (1, 2048, 2048)), (2 ** 17, (1, 2048, 2048))]
+    parts = [S.uniform_cluster_photons(n, 2048, 2048, seed=300 + s) for s, (n, _) in
+             enumerate(specs)]
+    cat = [torch.cat([p[k] for p in parts], dim=-1).contiguous().cuda() for k in range(5)]
+    b = BatchedSplat(specs, 20, "cuda:0", config=_lib.config(**(cfg or {})))
+    b.plan(*cat)
+    flat = b.forward()
+    grads = [S.upstream_grad(shape, seed=60 + s) for s, (_, shape) in enumerate(specs)]
+    gflat = torch.cat([g.reshape(-1) for g in grads]).cuda()
+    gE, gX, gM = b.backward(gflat)
+    torch.cuda.synchronize()
+    imgs = b.images(flat)
+    off = 0
+    for s, ((n, shape), ph) in enumerate(zip(specs, parts)):
+        rimg, (rE, rX, rM) = run_oracle(ph, shape, 20, grads[s])
+        assert rel_l2(imgs[s].cpu().numpy(), rimg) <= FWD_TOL
+        sl = slice(off, off + n)
+        assert rel_l2(gE[sl].cpu().numpy(), rE) <= GRAD_TOL
+        assert rel_l2(gX[:, sl].cpu().numpy(), rX) <= GRAD_TOL
+        assert rel_l2(gM[:, :, sl].cpu().numpy(), rM) <= GRAD_TOL
+        off += n
+
+
 def test_simulations_sharing_an_image_are_summed(cuda):
     # the reference's caller sums its simulations' images (shape_from_caustics.py:351-353)
     from shapefromcaustics_b200 import _lib
