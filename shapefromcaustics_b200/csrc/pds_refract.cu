@@ -72,9 +72,6 @@ __device__ __forceinline__ Dual operator*(float s, const Dual& a) {
     for (int k = 0; k < K; ++k) r.d[k] = s * a.d[k];
     return r;
 }
-__device__ __forceinline__ Dual operator+(const Dual& a, float s) {
-    Dual r = a; r.v += s; return r;
-}
 __device__ __forceinline__ Dual operator/(const Dual& a, const Dual& b) {
     const float inv = 1.f / b.v;
     Dual r; r.v = a.v * inv;
@@ -90,12 +87,8 @@ __device__ __forceinline__ Dual dsqrt(const Dual& a) {
     return r;
 }
 __device__ __forceinline__ Dual dabs(const Dual& a) { return a.v < 0.f ? -a : a; }
-__device__ __forceinline__ Dual dmax(const Dual& a, const Dual& b) { return a.v >= b.v ? a : b; }
 
 __device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
-__device__ __forceinline__ float dabs(float a) { return fabsf(a); }
-__device__ __forceinline__ float dmax(float a, float b) { return fmaxf(a, b); }
-__device__ __forceinline__ float dconstf(float v) { return v; }
 
 template <class T>
 struct V3 {
