@@ -15,7 +15,7 @@ import torch
 
 from . import _lib
 
-__all__ = ["CANDIDATES", "signature", "tune_batch", "cached"]
+__all__ = ["CANDIDATES", "signature", "pick", "tune_batch", "cached"]
 
 CANDIDATES = [dict(tile=t, chunk=2048, class_bits=b, walk=w, min_blocks=m, coop_radius=k)
               for t, b, w, m, k in itertools.product((64, 32), (5, 3), (3, 1), (3, 4), (-1, 8))]
@@ -57,6 +57,20 @@ def _measure(batch, photons, out, gflat, grads, reps, stream, min_ms=20.0, round
                for _ in range(rounds))
 
 
+def pick(timed, margin=0.02):
+    """The winner of ``timed``, a list of ``(config, ms)`` in candidate order: the first entry
+    (the library default) unless another is faster than it by more than ``margin`` (a
+    fraction), in which case the fastest of those. ``None`` for an empty list."""
+    if not timed:
+        return None
+    first_cfg, first_ms = timed[0]
+    best, best_ms = first_cfg, first_ms
+    for c, ms in timed[1:]:
+        if ms < best_ms and ms < first_ms * (1.0 - margin):
+            best, best_ms = c, ms
+    return best
+
+
 def tune_batch(specs, photons, gflat, max_pixel_radius, device, candidates=None, reps=3,
                verbose=False, margin=0.02):
     """Times every candidate on ``BatchedSplat(specs)`` with the given photons and upstream
@@ -67,7 +81,7 @@ def tune_batch(specs, photons, gflat, max_pixel_radius, device, candidates=None,
     candidates = candidates or CANDIDATES
     stream = torch.cuda.Stream(device)
     results = {}
-    best, best_ms, first_ms = None, float("inf"), None
+    timed = []
     grads = tuple(torch.empty_like(t) for t in photons[:3])
     out = None
     for c in candidates:
@@ -81,13 +95,10 @@ def tune_batch(specs, photons, gflat, max_pixel_radius, device, candidates=None,
         ms = _measure(batch, photons, out, gflat, grads, reps, stream)
         key = tuple(sorted(c.items()))
         results[key] = ms
+        timed.append((c, ms))
         if verbose:
             print(f"autotune {c}: {ms:.3f} ms")
-        if first_ms is None:
-            first_ms = ms
-            best, best_ms = c, ms
-        elif ms < best_ms and ms < first_ms * (1.0 - margin):
-            best, best_ms = c, ms
         del batch
+    best = pick(timed, margin)
     _cache[signature(specs, max_pixel_radius)] = best
     return best, results
