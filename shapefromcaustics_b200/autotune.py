@@ -1,8 +1,8 @@
 """Autotuner for the splat kernels' launch configuration.
 
-Times candidate ``pds_config`` values (screen-tile edge, footprint-class sort bits, pixel
-walk, resident CTAs per SM, warp-cooperative splat of large footprints) on the caller's
-actual workload with CUDA events, and keeps the fastest per workload signature (photon count
+Times candidate ``pds_config`` values (screen-tile edge, sorted photons per work chunk,
+footprint-class sort bits, pixel walk, resident CTAs per SM, warp-cooperative splat of large
+footprints) on the caller's actual workload with CUDA events, and keeps the fastest per workload signature (photon count
 and image sizes, bucketed); the first candidate is the library default, which wins ties. The
 reference has a single fixed launch shape (512 threads per photon block,
 ``photon_differentials.cu:120``); here the best tile and chunk depend on footprint sizes and
@@ -15,10 +15,15 @@ import torch
 
 from . import _lib
 
-__all__ = ["CANDIDATES", "signature", "pick", "tune_batch", "cached"]
+__all__ = ["DEFAULT", "CANDIDATES", "signature", "pick", "tune_batch", "cached"]
 
+# the library default first; then tile, class bits, walk, CTAs per SM and the cooperative
+# splat in all combinations, and the default with smaller and larger work chunks (sorted
+# photons a CTA takes at a time)
+DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=3, coop_radius=-1)
 CANDIDATES = [dict(tile=t, chunk=2048, class_bits=b, walk=w, min_blocks=m, coop_radius=k)
               for t, b, w, m, k in itertools.product((64, 32), (5, 3), (3, 1), (3, 4), (-1, 8))]
+CANDIDATES += [dict(DEFAULT, chunk=c) for c in (1024, 4096)]
 
 _cache = {}
 

@@ -7,9 +7,10 @@ DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=3, coop_rad
 
 
 def test_first_candidate_is_the_library_default_and_all_are_valid():
-    assert AT.CANDIDATES[0] == DEFAULT
+    assert AT.CANDIDATES[0] == DEFAULT == AT.DEFAULT
     keys = {tuple(sorted(c.items())) for c in AT.CANDIDATES}
-    assert len(keys) == len(AT.CANDIDATES) == 32
+    assert len(keys) == len(AT.CANDIDATES) == 34
+    assert {c["chunk"] for c in AT.CANDIDATES} == {1024, 2048, 4096}
     for c in AT.CANDIDATES:
         assert c["tile"] in (16, 32, 64)
         assert c["chunk"] % 256 == 0
