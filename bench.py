@@ -6,7 +6,8 @@
 Workloads (synthetic, seeded; the reference publishes no benchmark and its photons come from
 OptiX tracing, which these generators replace):
   batch64     (default) 64 independent simulations, photon counts ~ logU[2^16, 2^22]
-              (62.6 M photons in all), square images drawn from {256, 512, 1024}^2,
+              (45.4 M photons in all at the rank-0 seed), square images drawn from
+              {256, 512, 1024}^2,
               half-uniform/half-clustered photons with differentials s ~ logU[0.5, 4] px,
               max_pixel_radius 20, fp32. One step = binning + forward + backward of every
               simulation (one Landweber iteration's splatting work) with fixed upstream
@@ -320,6 +321,10 @@ def run_ours(args, rank, world, device):
     ms_per_step = total_ms / args.steps
     photons_all = sum_over_ranks(float(n_total), world, device)
     value = photons_all / (ms_per_step / 1e3)
+    # error of the timed step's own outputs against the FP64 oracle (outside the timed region)
+    parity = None
+    if not args.lean and rank == 0:
+        parity = parity_vs_oracle(specs, photons, gflat, batch, out, grads)
 
     # ---- roofline window: the same steps eager, CUDA events around each phase ----
     phases = {"plan": [], "forward": [], "backward": []}
@@ -381,7 +386,7 @@ def run_ours(args, rank, world, device):
     p0 = SplatPlan(*split_photons(specs[:1], photons)[0], specs[0][1], MPR)
     ref0 = p0.forward()
     torch.cuda.synchronize()
-    parity = float((imgs[0] - ref0).norm() / ref0.norm())
+    parity_plain = float((imgs[0] - ref0).norm() / ref0.norm())
 
     # ---- e2e: host (pinned) photons and gradients in, loss out, through the public API ----
     # Every step copies its photons and upstream gradient from pinned host memory and reads
@@ -458,6 +463,13 @@ def run_ours(args, rank, world, device):
            "backward": n_total * 76 + pixels * 4}
     flops = {"plan": 0, "forward": pix_sup * FLOP_FWD_PX, "backward": pix_sup * FLOP_BWD_PX}
     dom = max(("forward", "backward"), key=lambda k: ph_ms[k])
+    # the whole step against the roofline: sum_sims [N_i 116 B + C H_i W_i 4 B 2]
+    step_bytes = n_total * 116 + pixels * 8
+    step_roofline = {"bound": "hbm", "kernel": "whole step (plan + forward + backward)",
+                     "algorithmic_bytes": step_bytes,
+                     "achieved": step_bytes / (ms_per_step / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": step_bytes / (ms_per_step / 1e3) / 1e9 / peak,
+                     "peak_source": peak_kind}
     achieved = alg[dom] / (ph_ms[dom] / 1e3) / 1e9
     simt = flops[dom] / (ph_ms[dom] / 1e3) / 1e12
     # plan: plan_kernel, bucket_reduce/top/down, bucket_scatter, chunk_tile_kernel;
@@ -475,8 +487,9 @@ def run_ours(args, rank, world, device):
                    "parallelism": f"simulation-sharded x{world}, no collective",
                    "mode": "batched: one CUDA graph per step (plan + fwd + bwd)",
                    "launch_config": tuned or "library default"},
-        "landweber_it_per_s": {"batched": 1e3 / ms_per_step, "plain": 1e3 / plain_ms,
-                               "batched_over_plain": plain_ms / ms_per_step},
+        "splat_steps_per_s": {"batched": 1e3 / ms_per_step, "plain": 1e3 / plain_ms,
+                              "batched_over_plain": plain_ms / ms_per_step,
+                              "step": "plan + forward + backward of every simulation"},
         "phase_ms": ph_ms,
         "roofline": {"bound": "hbm", "kernel": f"{dom} phase ({PHASE_KERNELS[dom]})",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -493,13 +506,78 @@ def run_ours(args, rank, world, device):
                           "support_pixels_per_step": pix_sup, "box_pixels_per_step": pix_box},
         "e2e": {"value": photons_all / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+        "roofline_step": step_roofline,
         "gpu_launches": launches_per_step * args.steps,
-        "parity_batched_vs_plain_relL2": parity,
+        "parity_vs_oracle": parity,
+        "parity_batched_vs_plain_relL2": parity_plain,
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        result["reference_gpu"] = reference_gpu_subprocess(args, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(specs, photons, gflat, budget_s=args.cpu_seconds)
     return result
+
+
+def parity_vs_oracle(specs, photons, gflat, batch, out, grads, max_photons=2 ** 23):
+    """Relative L2 error of the benchmark step's own outputs (image, grad_Ep, grad_xp,
+    grad_Mp) against the FP64 oracle, over the workload's first simulations up to
+    ``max_photons`` photons (errors accumulated over those simulations)."""
+    import numpy as np
+    from oracle import oracle as O
+    torch.cuda.synchronize()
+    imgs = batch.images(out)
+    num = {"image": 0.0, "grad_Ep": 0.0, "grad_xp": 0.0, "grad_Mp": 0.0}
+    den = dict(num)
+    b = gb = 0
+    sims = n_ph = 0
+    t0 = time.perf_counter()
+    for s, (n, shape) in enumerate(specs):
+        if n_ph + n > max_photons and sims > 0:
+            break
+        C, H, W = shape
+        sl = slice(b, b + n)
+        ph = [photons[0][sl], photons[1][:, sl], photons[2][:, :, sl], photons[3][:, sl],
+              photons[4][sl]]
+        npy = [t.cpu().numpy() for t in ph]
+        G = gflat[gb:gb + C * H * W].view(C, H, W).cpu().double().numpy()
+        rimg = O.forward(*npy, shape, MPR)
+        rg = O.backward(G, *npy, MPR)
+        got = [imgs[s].cpu().double().numpy(), grads[0][sl].cpu().double().numpy(),
+               grads[1][:, sl].cpu().double().numpy(), grads[2][:, :, sl].cpu().double().numpy()]
+        for k, a, r in zip(num, got, [rimg, *rg]):
+            num[k] += float(np.sum((a - r) ** 2))
+            den[k] += float(np.sum(r ** 2))
+        b += n
+        gb += C * H * W
+        sims += 1
+        n_ph += n
+    res = {k: (num[k] / den[k]) ** 0.5 if den[k] > 0 else 0.0 for k in num}
+    res.update({"metric": "relative L2 vs FP64 oracle", "simulations": sims, "photons": n_ph,
+                "tolerance": {"image": 1e-5, "gradients": 1e-4},
+                "oracle_seconds": round(time.perf_counter() - t0, 2)})
+    return res
+
+
+def reference_gpu_subprocess(args, our_value):
+    """The reference's own CUDA extension on the same workload (``--impl reference-gpu`` in a
+    child process, after this arm's timing); -> its value, step time and clocks."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference-gpu", "--workload",
+           args.workload, "--steps", str(max(3, min(args.steps, 10))), "--warmup", "2"]
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE"):
+        env.pop(k, None)
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+        line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
+        r = json.loads(line)
+    except Exception as e:  # the reference extension may be absent (not built here)
+        return {"unavailable": f"reference-gpu arm failed: {type(e).__name__}: {e}"}
+    if "unavailable" in r:
+        return r
+    return {"value": r["value"], "unit": r["unit"], "ms_per_step": r["ms_per_step"],
+            "steps": r["steps"], "clocks": r.get("clocks"), "mode": r["config"]["mode"],
+            "ours_over_reference_gpu": our_value / r["value"]}
 
 
 # ------------------------------------------------------------------ CPU (reference) ------
@@ -629,20 +707,27 @@ def run_reference_gpu(args, rank, world, device):
     for _ in range(max(args.warmup, 1)):
         step()
     torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    clocks = ClockSampler(vis.split(",")[device.index].strip() if vis else str(device.index))
+    clocks.start()
+    time.sleep(0.3)
     barrier(world)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clocks.mark_start()
     e0.record()
     for _ in range(args.steps):
         step()
     e1.record()
     torch.cuda.synchronize()
+    clocks.mark_stop()
+    clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, device)
     photons_all = sum_over_ranks(float(n_total), world, device)
     return {"metric": METRIC, "value": photons_all / (ms / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "impl": "reference-gpu",
+            "data": "synthetic", "impl": "reference-gpu", "clocks": clocks.summary(),
             "config": {"workload": f"{args.workload}: {desc}", "max_pixel_radius": MPR,
                        "mode": "plain: pds_forward + pds_backward per simulation"}}
 
@@ -765,6 +850,8 @@ def main():
                     choices=["batch64", "uniform1m", "medium", "contention", "contention24",
                              "landweber256", "recon1024"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference CUDA extension's run on the same workload")
     ap.add_argument("--no-autotune", action="store_true",
                     help="time the library's default configuration instead of the tuned one")
     ap.add_argument("--lean", action="store_true",

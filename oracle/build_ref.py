@@ -15,7 +15,10 @@ SDK; that part is not built. This recipe calls ``torch.utils.cpp_extension.load`
 splatting sources only, for sm_100 (``TORCH_CUDA_ARCH_LIST=10.0``), since the reference
 carries no architecture flags of its own.
 
-Usage: ``python oracle/build_ref.py [--ref-root PATH]`` (default ``/root/reference``).
+Usage: ``python oracle/build_ref.py [--ref-root PATH]``. The reference checkout is taken from
+``--ref-root``, else from the ``PDS_REFERENCE_ROOT`` environment variable, else from
+``/root/reference``; where none of these exists the recipe has nothing to build
+(``reference_root()`` returns None).
 """
 import argparse
 import os
@@ -24,6 +27,18 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 MODULE = "pds_reference_ext"
+
+
+DEFAULT_ROOT = "/root/reference"
+
+
+def reference_root():
+    """The reference checkout to build from, or None when it is not on this machine."""
+    for cand in (os.environ.get("PDS_REFERENCE_ROOT"), DEFAULT_ROOT):
+        if cand and os.path.isfile(os.path.join(cand, "PyOptix", "kernel",
+                                                "photon_differentials.cu")):
+            return cand
+    return None
 
 
 def built_path():
@@ -37,7 +52,10 @@ def built_path():
     return None
 
 
-def build(ref_root="/root/reference", verbose=False):
+def build(ref_root=None, verbose=False):
+    ref_root = ref_root or reference_root()
+    if ref_root is None:
+        raise FileNotFoundError("no reference checkout (set PDS_REFERENCE_ROOT)")
     srcs = [os.path.join(ref_root, "PyOptix", "PhotonDifferentialSplattig.cpp"),
             os.path.join(ref_root, "PyOptix", "kernel", "photon_differentials.cu")]
     for s in srcs:
@@ -67,7 +85,7 @@ def load_module():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=None)
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
     print(build(a.ref_root, a.verbose))

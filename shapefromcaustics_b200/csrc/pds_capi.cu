@@ -608,12 +608,10 @@ int pds_landweber_update_noalloc_f32(float* d, const float* grad, const float* m
                     "pds_landweber_update_noalloc_f32: field of " + std::to_string(rows) + " x " +
                         std::to_string(cols) + " exceeds its static scratch of " +
                         std::to_string(maxpx) + " pixels; use pds_landweber_update_f32");
-    void* scratch = nullptr;
-    cudaError_t e = pds::landweber_noalloc_scratch(&scratch);
+    float* t = nullptr;
+    float* partial = nullptr;
+    cudaError_t e = pds::landweber_noalloc_scratch(&t, &partial);
     if (e != cudaSuccess) return cuda_fail(e, "noalloc scratch address (cudaGetSymbolAddress)");
-    float* t = static_cast<float*>(scratch);
-    float* partial = reinterpret_cast<float*>(static_cast<char*>(scratch) +
-                                              size_t(maxpx) * sizeof(float));
     e = pds::launch_landweber(d, grad, mask, rows, cols, *p, t, partial,
                               static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "landweber kernels (noalloc)");

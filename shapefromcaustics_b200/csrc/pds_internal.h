@@ -37,6 +37,6 @@ cudaError_t launch_landweber(float* d, const float* g, const float* mask, int64_
                              int64_t cols, const pds_landweber& p, float* t, float* partial,
                              cudaStream_t st);
 int64_t landweber_noalloc_max_pixels();
-cudaError_t landweber_noalloc_scratch(void** out);
+cudaError_t landweber_noalloc_scratch(float** t, float** partial);
 
 }  // namespace pds

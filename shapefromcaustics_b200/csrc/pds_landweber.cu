@@ -142,10 +142,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 int64_t landweber_noalloc_max_pixels() { return kNoAllocMaxPixels; }
 
-// Device address of the scratch on the current device. In host code the symbol is only a
-// host-side stand-in, so the address is looked up once per device (with that device
-// current) and cached.
-cudaError_t landweber_noalloc_scratch(void** out) {
+// Device addresses of the scratch's two parts on the current device: the shrunk image `t`
+// (kNoAllocMaxPixels floats) and the per-block partial sums `partial` right after it. In host
+// code the symbol is only a host-side stand-in, so the array's address is looked up once per
+// device (with that device current) and cached.
+cudaError_t landweber_noalloc_scratch(float** t, float** partial) {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
     static void* addr[kMaxDevices] = {};
@@ -160,7 +161,9 @@ cudaError_t landweber_noalloc_scratch(void** out) {
         if (e != cudaSuccess) return e;
         addr[dev] = p;
     }
-    *out = addr[dev];
+    unsigned char* base = static_cast<unsigned char*>(addr[dev]);
+    *t = reinterpret_cast<float*>(base);
+    *partial = reinterpret_cast<float*>(base + kNoAllocImageBytes);
     return cudaSuccess;
 }
 

@@ -31,9 +31,15 @@ def shard_range(n, rank, world):
 
 
 def shard_photons(Ep, xp, Mp, cp, radius, rank, world):
-    """This rank's contiguous slice of the reference's photon arrays (views)."""
+    """This rank's slice of the reference's photon arrays, as contiguous tensors.
+
+    The slice of a ``[2, N]`` or ``[2, 3, N]`` array along its photon axis is a strided view;
+    the splat ops take contiguous arrays only (``PyOptix/utils.hpp:37-41``), so the rows are
+    copied into this rank's own ``[2, n]`` / ``[2, 3, n]`` arrays (``Ep`` and ``radius``
+    slices are contiguous already and stay views)."""
     b, e = shard_range(Ep.shape[0], rank, world)
-    return Ep[b:e], xp[:, b:e], Mp[:, :, b:e], cp[:, b:e], radius[b:e]
+    return (Ep[b:e].contiguous(), xp[:, b:e].contiguous(), Mp[:, :, b:e].contiguous(),
+            cp[:, b:e].contiguous(), radius[b:e].contiguous())
 
 
 def sharded_forward(Ep, xp, Mp, cp, radius, output_size, max_pixel_radius, group=None,
@@ -43,6 +49,7 @@ def sharded_forward(Ep, xp, Mp, cp, radius, output_size, max_pixel_radius, group
 
     ``splat`` replaces ``pds_forward`` (same signature); the default is the CUDA op."""
     splat = splat or splatting.pds_forward
+    Ep, xp, Mp, cp, radius = (t.contiguous() for t in (Ep, xp, Mp, cp, radius))
     img = splat(Ep, xp, Mp, cp, radius, output_size, max_pixel_radius)[0]
     if dist.is_available() and dist.is_initialized():
         dist.all_reduce(img, op=dist.ReduceOp.SUM, group=group)
@@ -53,4 +60,5 @@ def sharded_backward(grad_pds, Ep, xp, Mp, cp, radius, max_pixel_radius, splat_b
     """Gradients of this rank's photon shard from the (replicated) upstream gradient; no
     exchange. ``splat_backward`` replaces ``pds_backward`` (same signature)."""
     fn = splat_backward or splatting.pds_backward
+    Ep, xp, Mp, cp, radius = (t.contiguous() for t in (Ep, xp, Mp, cp, radius))
     return fn(grad_pds.contiguous(), Ep, xp, Mp, cp, radius, max_pixel_radius)

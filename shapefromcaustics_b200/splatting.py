@@ -230,9 +230,24 @@ class BatchedSplat:
                                            self.mpr, _ptr(self.ws), self.ws.numel(),
                                            ctypes.byref(self.cfg), _stream(self.device)))
 
+    def _planned(self, op):
+        if self.inputs is None:
+            raise RuntimeError(f"BatchedSplat.{op}() called before plan()")
+
+    def _check_flat(self, t, name):
+        if not (t.is_cuda and t.device == self.device):
+            raise RuntimeError(f"{name} must be a CUDA tensor on {self.device}")
+        if t.dtype != torch.float32:
+            raise RuntimeError(f"{name} must be float32, got {t.dtype}")
+        if t.numel() != self.image_elems or not t.is_contiguous():
+            raise RuntimeError(f"{name} must be a contiguous flat buffer of the batch's "
+                               f"{self.image_elems} image elements")
+
     def forward(self, out=None):
+        self._planned("forward")
         if out is None:
             out = torch.empty(self.image_elems, dtype=torch.float32, device=self.device)
+        self._check_flat(out, "out")
         with torch.cuda.device(self.device):
             check(lib().pds_batch_forward_planned_f32(*(_ptr(t) for t in self.inputs),
                                                       *self._common(), self.image_elems,
@@ -242,8 +257,8 @@ class BatchedSplat:
         return out
 
     def backward(self, grad_flat, out=None):
-        if grad_flat.numel() != self.image_elems or not grad_flat.is_contiguous():
-            raise RuntimeError("grad must be a contiguous flat buffer of the batch's images")
+        self._planned("backward")
+        self._check_flat(grad_flat, "grad")
         Ep, xp, Mp = self.inputs[:3]
         if out is None:
             out = (torch.empty_like(Ep), torch.empty_like(xp), torch.empty_like(Mp))

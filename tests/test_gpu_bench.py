@@ -2,8 +2,9 @@
 
 Runs the 2^20-photon 512^2 workload for three timed steps (library default configuration, a
 short CPU-baseline sample) and checks that the line carries the metric, the device roofline,
-the end-to-end number with its copied bytes, the launch count, the sampled clocks and the CPU
-baseline.
+the end-to-end number with its copied bytes, the launch count, the sampled clocks, the CPU
+baseline, the step's error against the FP64 oracle, the whole-step roofline and the reference
+CUDA extension's run on the same workload.
 """
 import json
 import os
@@ -41,3 +42,14 @@ def test_bench_line_carries_every_key(cuda):
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(r["clocks"])
     cb = r["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] > 0
+    # per-result error of the timed step against the FP64 oracle, within the stated tolerances
+    pv = r["parity_vs_oracle"]
+    assert pv["image"] <= 1e-5 and pv["photons"] == 2 ** 20
+    assert max(pv["grad_Ep"], pv["grad_xp"], pv["grad_Mp"]) <= 1e-4
+    # the whole step against the roofline
+    rs = r["roofline_step"]
+    assert rs["algorithmic_bytes"] == 2 ** 20 * 116 + 512 * 512 * 8
+    assert abs(rs["frac"] - rs["achieved"] / rs["peak"]) < 1e-9
+    # the reference's own CUDA extension on the same workload (when it is built)
+    rg = r["reference_gpu"]
+    assert "unavailable" in rg or (rg["value"] > 0 and rg["ours_over_reference_gpu"] > 0)

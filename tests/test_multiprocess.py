@@ -77,6 +77,8 @@ def _sharded_worker(rank, world, port, q):
         shape = (1, 96, 80)
         ph = S.uniform_cluster_photons(3001, 96, 80, seed=21, sigma=6.0)
         local = SH.shard_photons(*ph, rank, world)
+        # the CUDA ops take contiguous arrays only
+        assert all(t.is_contiguous() for t in local)
 
         def oracle_fwd(E, X, M, C, R, size, mpr):
             img = O.forward(*[t.numpy() for t in (E, X, M, C, R)], tuple(size), mpr)
