@@ -40,26 +40,27 @@ struct Resolved {
 int resolve_cfg(const pds_config* in, pds_config& out) {
     out.tile = (in && in->tile) ? in->tile : 64;
     out.chunk = (in && in->chunk) ? in->chunk : 2048;
-    out.class_bits = (in && in->class_bits) ? in->class_bits : 5;
+    out.class_bits = (in && in->class_bits) ? in->class_bits : 6;
     if (out.class_bits == -1) out.class_bits = 0;
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
-    out.walk = (in && in->walk) ? in->walk : 3;
+    out.walk = (in && in->walk) ? in->walk : 4;
     out.min_blocks = (in && in->min_blocks) ? in->min_blocks : 3;
     out.coop_radius = (in && in->coop_radius) ? in->coop_radius : -1;
     if (out.coop_radius < -1 || out.coop_radius > 63)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.coop_radius must be -1 or in [1, 63]");
     if (out.min_blocks < 2 || out.min_blocks > 4)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.min_blocks must be 2, 3 or 4");
-    if (out.walk < 1 || out.walk > 3)
+    if (out.walk < 1 || out.walk > 4)
         return fail(PDS_ERR_INVALID_ARGUMENT,
-                    "pds_config.walk must be 1 (box), 2 (support spans) or 3 (support band)");
+                    "pds_config.walk must be 1 (box), 2 (support spans), 3 (support band) or "
+                    "4 (band rows padded per warp)");
     if (out.tile != 16 && out.tile != 32 && out.tile != 64)
         return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.tile must be 16, 32 or 64");
     if (out.chunk < 256 || out.chunk > (1 << 20) || out.chunk % 256 != 0)
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.chunk must be a multiple of 256 in [256, 1048576]");
-    if (out.class_bits < 0 || out.class_bits > 5)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be -1 or in [1, 5]");
+    if (out.class_bits < 0 || out.class_bits > 6)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_config.class_bits must be -1 or in [1, 6]");
     if (out.apron_max < 1 || out.apron_max > 63 || out.tile + 2 * out.apron_max > 255)
         return fail(PDS_ERR_INVALID_ARGUMENT,
                     "pds_config.apron_max must be in [1, 63] with tile + 2*apron_max <= 255");
@@ -94,8 +95,10 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, int64_t n, Resol
     r.cfg.apron = mpr < 0 ? 0 : (mpr < c.apron_max ? mpr : c.apron_max);
     // odd pitch: the rows of one column of the accumulator fall in different banks
     r.cfg.sw = (c.tile + 2 * r.cfg.apron) | 1;
-    r.cfg.spans = c.walk == 2 ? 1 : 0;
+    // the row walk sends photons without a band to the support-span walk
+    r.cfg.spans = (c.walk == 2 || c.walk == 4) ? 1 : 0;
     r.cfg.band = c.walk == 3 ? 1 : 0;
+    r.cfg.rows = c.walk == 4 ? 1 : 0;
     r.cfg.min_blocks = c.min_blocks;
     r.cfg.coop_r = c.coop_radius > 0 ? c.coop_radius : 0;
     r.n_buckets = n_tiles << c.class_bits;

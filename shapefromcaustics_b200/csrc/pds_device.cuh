@@ -72,6 +72,7 @@ struct Cfg {
     int32_t sw;          // tile + 2 * apron: edge of the shared accumulator
     int32_t spans;       // 1: walk only the support's rows / row spans; 0: the whole box
     int32_t band;        // 1: walk each footprint's sheared band (see Band)
+    int32_t rows;        // 1: walk the bands' rows padded to a common count and width per warp
     int32_t min_blocks;  // resident CTAs per SM the tile kernels' register budget targets
     int32_t coop_r;      // footprint radius from which a photon is splatted by a whole warp
 };
@@ -267,6 +268,44 @@ __device__ __forceinline__ Band make_band(float m00, float m01, float m10, float
 
 __device__ __forceinline__ int band_start(const Band& b, int ky) {
     return __float2int_rd(fmaf(float(ky), b.beta, b.alpha - b.hw));
+}
+
+// The rows a photon's band walk visits inside its clipped box [kxb0, kxb1] x [kyb0, kyb1]
+// (pixel offsets from the centre pixel): rows ky0 .. ky0 + rows - 1, each w pixels wide and
+// starting at the band's start clamped into [kxb0, kxlast]. A clamped row still holds every
+// pixel of its support that lies in the box: the support's pixels of row ky are in
+// [xs, xs + bw - 1]; clamping slides that window into the box without dropping any of them,
+// and when w is the box width the row is the whole box row. Every visited pixel is in the box,
+// so the walks need no per-pixel box test.
+struct RowWalk {
+    int ky0, rows, w, kxb0, kxlast;
+};
+
+__device__ __forceinline__ RowWalk row_walk(const Band& b, int kxb0, int kxb1, int kyb0, int kyb1) {
+    RowWalk r;
+    r.ky0 = max(b.ky0, kyb0);
+    r.rows = max(min(b.ky1, kyb1) - r.ky0 + 1, 0);
+    r.w = min(b.bw, kxb1 - kxb0 + 1);
+    r.kxb0 = kxb0;
+    r.kxlast = kxb1 - r.w + 1;
+    return r;
+}
+
+__device__ __forceinline__ int row_start(const Band& b, const RowWalk& r, int ky) {
+    return min(max(band_start(b, ky), r.kxb0), r.kxlast);
+}
+
+// Footprint class of the row walk: 3 bits for the row count and 3 for the row width, levels
+// 1, 2, 3, 4, 5-6, 7-8, 9-12, 13+ each. Photons of one class have nearly the same rows and
+// widths, so a warp of them pads its rows to a common count and width with little waste.
+constexpr int kRowClassBits = 6;
+
+__host__ __device__ __forceinline__ uint32_t row_level(int v) {
+    return v <= 4 ? uint32_t((v < 1 ? 1 : v) - 1) : (v <= 6 ? 4u : (v <= 8 ? 5u : (v <= 12 ? 6u : 7u)));
+}
+
+__host__ __device__ __forceinline__ uint32_t row_class(int rows, int w) {
+    return (row_level(rows) << 3) | row_level(w);
 }
 
 // delta = (2 p_c / w - 1) - x in double, rounded once to float.

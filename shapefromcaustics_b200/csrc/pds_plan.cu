@@ -131,7 +131,21 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_kernel(PlanArgs a) {
                         const float dx0 = corner_offset(f.px_c, sim.width, x);
                         const float dy0 = corner_offset(f.py_c, sim.height, y);
                         uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
-                        if (a.cfg.band) {
+                        if (cb == kRowClassBits) {
+                            // the row walk's classes: rows and row width inside the box
+                            const float sy = float(2.0 / double(sim.height));
+                            const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy,
+                                                      0.5f * float(sim.width),
+                                                      0.5f * float(sim.height),
+                                                      float(f.rx) + 1.f);
+                            if (bd.on && f.ellipse_all) {
+                                const RowWalk rw = row_walk(bd, x0 - f.px_c, x1 - f.px_c,
+                                                            y0 - f.py_c, y1 - f.py_c);
+                                cls = row_class(rw.rows, rw.w);
+                            } else {
+                                cls = cls_max;
+                            }
+                        } else if (a.cfg.band) {
                             // photons of a warp then have similar band areas (trip counts):
                             // classes of 1/k octave of the area, k = 1, 2, 3 for up to 3, 4
                             // and 5 class bits

@@ -47,8 +47,11 @@ struct TileInfo {
     int32_t ox, oy;   // pixel coordinates of the accumulator's (0, 0)
     float sx, sy;     // 2 / W, 2 / H
     float isx, isy;   // W / 2, H / 2
-    double wd, hd;    // float(W), float(H) in double (the reference's w, h)
 };
+
+// float(W), float(H) in double: the reference's w, h of the :93 ellipse test
+__device__ __forceinline__ double img_wd(const TileInfo& t) { return double(float(t.W)); }
+__device__ __forceinline__ double img_hd(const TileInfo& t) { return double(float(t.H)); }
 
 __device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t tile, const Cfg& cfg) {
     const int s = find_sim_of_tile(st, tile);
@@ -68,8 +71,6 @@ __device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t til
     t.sy = float(2.0 / double(sim.height));
     t.isx = 0.5f * float(sim.width);
     t.isy = 0.5f * float(sim.height);
-    t.wd = double(float(sim.width));
-    t.hd = double(float(sim.height));
     return t;
 }
 
@@ -145,7 +146,7 @@ __device__ __forceinline__ void deposit_band(const Rec& r, const Band& bd, const
 // add exactly zero in the reference (value > 0 fails, :106). Photons that fail the
 // reference's image-half-size ellipse test somewhere in their box (tiny images only) take
 // the per-pixel test path.
-__device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
+__device__ __noinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                         bool band, float* acc, int& bx0, int& bx1, int& by0,
                                         int& by1) {
     const uint32_t p = r.packed;
@@ -199,7 +200,7 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
             const float c1 = fmaf(r.m10, r.dx0, r.m11 * dy);
             const uint32_t arow = acc_base + 4u * uint32_t((pyc + ky - ti.oy) * sw + (pxc - ti.ox));
             for (int kx = x0 - pxc; kx <= x1 - pxc; ++kx) {
-                if (!ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
+                if (!ellipse_ok(kx, ky, img_wd(ti), img_hd(ti))) continue;
                 const float u0 = fmaf(float(kx), a00, c0), u1 = fmaf(float(kx), a10, c1);
                 const float s = fmaf(u0, u0, u1 * u1);
                 const float t = 1.f - s;
@@ -208,6 +209,210 @@ __device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw
         }
     }
 }
+
+// ---- the padded-row walk (walk 4) -------------------------------------------------------
+// Each lane holds one photon and walks its band's rows inside the clipped box (RowWalk). The
+// warp pads every lane to the warp's largest row count and row width, so all lanes change
+// rows on the same iteration and the loops stay converged; the plan's row classes group
+// photons of nearly equal rows and widths into a warp, so little of the padding is wasted.
+// Along a row, s = |M d|^2 is a quadratic in the column c, stepped by its first and second
+// differences (two adds per pixel). Padding pixels (c >= the lane's width, rows past the
+// lane's count) are predicated off.
+
+// Per-lane constants of the row walk of one photon.
+struct RowGeo {
+    float xs0, beta;        // band start of row ky: floor(xs0 + beta ky) (xs0 = alpha - hw)
+    int ky0, rows, w;       // rows ky0 .. ky0 + rows - 1 of w pixels (RowWalk)
+    int kxb0, kxlast;       // clamp range of the row starts
+    int off;                // accumulator index of the centre pixel: (pyc - oy) sw + pxc - ox
+    float a00, a10;         // u step per pixel column: M (sx, 0)
+    float b0, b1;           // u step per pixel row: M (0, sy)
+    float c00, c10;         // u at the centre pixel's corner: M (dx0, dy0)
+    float A;                // |M (sx, 0)|^2: half the second difference of s along a row
+};
+
+// The clipped box of a record (pixel coordinates) and its centre pixel.
+__device__ __forceinline__ void rec_clip(const Rec& r, const TileInfo& ti, int& pxc, int& pyc,
+                                         int& x0, int& x1, int& y0, int& y1) {
+    const uint32_t p = r.packed;
+    pxc = ti.ox + rec_lx(p);
+    pyc = ti.oy + rec_ly(p);
+    const int rx = rec_rx(p), ry = rec_ry(p);
+    x0 = max(pxc - rx, 0);
+    x1 = min(pxc + rx, ti.W - 1);
+    y0 = max(pyc - ry, 0);
+    y1 = min(pyc + ry, ti.H - 1);
+}
+
+// Row walk of a record inside its clipped box (x0..y1, from rec_clip); false when the photon
+// needs the generic walk (the image-half-size ellipse quirk of tiny images, or an M without a
+// band).
+__device__ __forceinline__ bool prep_rows(const Rec& r, const TileInfo& ti, int sw, int pxc,
+                                          int pyc, int x0, int x1, int y0, int y1, RowGeo& g) {
+    if (!(rec_flags(r.packed) & kFlagEllipseAll)) return false;
+    const Band band = make_band(r.m00, r.m01, r.m10, r.m11, r.dx0, r.dy0, ti.sy, ti.isx, ti.isy,
+                                float(rec_rx(r.packed)) + 1.f);
+    if (!band.on) return false;
+    const RowWalk rw = row_walk(band, x0 - pxc, x1 - pxc, y0 - pyc, y1 - pyc);
+    g.xs0 = band.alpha - band.hw;
+    g.beta = band.beta;
+    g.ky0 = rw.ky0;
+    g.rows = rw.rows;
+    g.w = rw.w;
+    g.kxb0 = rw.kxb0;
+    g.kxlast = rw.kxlast;
+    g.off = (pyc - ti.oy) * sw + (pxc - ti.ox);
+    g.a00 = r.m00 * ti.sx;
+    g.a10 = r.m10 * ti.sx;
+    g.b0 = r.m01 * ti.sy;
+    g.b1 = r.m11 * ti.sy;
+    g.c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0);
+    g.c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
+    g.A = fmaf(g.a00, g.a00, g.a10 * g.a10);
+    return true;
+}
+
+// First column of row ky (band start clamped into the box), s and its first difference there.
+__device__ __forceinline__ int row_begin(const RowGeo& g, int ky, float& s, float& d) {
+    const float kyf = float(ky);
+    const int xs = min(max(__float2int_rd(fmaf(kyf, g.beta, g.xs0)), g.kxb0), g.kxlast);
+    const float kxf = float(xs);
+    const float u0 = fmaf(kxf, g.a00, fmaf(kyf, g.b0, g.c00));
+    const float u1 = fmaf(kxf, g.a10, fmaf(kyf, g.b1, g.c10));
+    s = fmaf(u0, u0, u1 * u1);
+    d = fmaf(2.f, fmaf(u0, g.a00, u1 * g.a10), g.A);  // s(c + 1) - s(c) at c = 0
+    return xs;
+}
+
+// Shared add of v at shared byte address a + OFF when c < w and s < 1, as one predicated
+// reduction.
+template <int OFF>
+__device__ __forceinline__ void red_row(uint32_t a, float s, float v, int c, int w) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.lt.s32 q, %3, %4;\n\t"
+        "setp.lt.and.f32 q, %1, 0f3F800000, q;\n\t@q red.shared.add.f32 [%0+%5], %2;\n\t}"
+        :: "r"(a), "f"(s), "f"(v), "r"(c), "r"(w), "n"(OFF) : "memory");
+}
+
+// Shared load of the float at shared byte address a when c < w, else 0.
+__device__ __forceinline__ float lds_row(uint32_t a, int c, int w) {
+    float v;
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.lt.s32 q, %2, %3;\n\tmov.b32 %0, 0;\n\t"
+        "@q ld.shared.f32 %0, [%1];\n\t}"
+        : "=f"(v) : "r"(a), "r"(c), "r"(w) : "memory");
+    return v;
+}
+
+// Forward deposit of the warp's photons by padded rows. rows = 0 for lanes with nothing to
+// walk (their g is not read). Lanes start at rotated rows (lane mod rows), so co-located
+// photons of a caustic add into different rows, and so different banks, at the same time.
+// Every lane of the warp calls it.
+__device__ __forceinline__ void deposit_rows(const RowGeo& g, int rows, float e3, uint32_t acc_base,
+                                             int sw) {
+    const int rm = __reduce_max_sync(0xFFFFFFFFu, rows);
+    if (rm == 0) return;
+    const int wm = __reduce_max_sync(0xFFFFFFFFu, rows > 0 ? g.w : 0);
+    const int rot = rows > 1 ? int(threadIdx.x & 31) % rows : 0;
+    const float dd = 2.f * g.A;
+    for (int j = 0; j < rm; ++j) {
+        const int wl = j < rows ? g.w : 0;
+        int jj = j + rot;
+        jj = jj >= rows ? jj - rows : jj;
+        const int ky = g.ky0 + jj;
+        float s, d;
+        const int xs = row_begin(g, ky, s, d);
+        uint32_t a = acc_base + 4u * uint32_t(g.off + ky * sw + xs);
+        int c = 0;
+        for (; c + 2 <= wm; c += 2) {
+            const float t = 1.f - s;
+            red_row<0>(a, s, (t * e3) * t, c, wl);
+            s += d;
+            d += dd;
+            const float t2 = 1.f - s;
+            red_row<4>(a, s, (t2 * e3) * t2, c + 1, wl);
+            s += d;
+            d += dd;
+            a += 8u;
+        }
+        if (c < wm) {
+            const float t = 1.f - s;
+            red_row<0>(a, s, (t * e3) * t, c, wl);
+        }
+    }
+}
+
+// Backward moments of the warp's photons by padded rows (no rotation: the gathers read).
+// Per row it keeps sum t g, sum t g c and sum t g c^2 over the row's columns c and folds them
+// into the photon's moments in the integer x offset kx = xs + c and the normalised y offset,
+// as gather_band_rows does. Every lane of the warp calls it.
+struct RowMoments {
+    float sE, A0t, B1t, B2t, Sy, Sxy, Syy;
+};
+
+__device__ __forceinline__ RowMoments gather_rows(const RowGeo& g, int rows, uint32_t tg_base,
+                                                 int sw, float sy, float dy0) {
+    RowMoments m = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const int rm = __reduce_max_sync(0xFFFFFFFFu, rows);
+    if (rm == 0) return m;
+    const int wm = __reduce_max_sync(0xFFFFFFFFu, rows > 0 ? g.w : 0);
+    const float dd = 2.f * g.A;
+    for (int j = 0; j < rm; ++j) {
+        const bool act = j < rows;
+        const int wl = act ? g.w : 0;
+        const int ky = g.ky0 + j;
+        float s, d;
+        const int xs = row_begin(g, ky, s, d);
+        // lanes without this row read nothing (their address is not formed from their rows)
+        uint32_t a = act ? tg_base + 4u * uint32_t(g.off + ky * sw + xs) : tg_base;
+        float A0 = 0.f, Bc = 0.f, Bcc = 0.f, sEr = 0.f, cf = 0.f;
+        int c = 0;
+        for (; c + 2 <= wm; c += 2) {
+            const float q0 = lds_row(a, c, wl);
+            const float q1 = lds_row(a + 4u, c + 1, wl);
+            const float t0 = fmaxf(1.f - s, 0.f);
+            s += d;
+            d += dd;
+            const float t1 = fmaxf(1.f - s, 0.f);
+            s += d;
+            d += dd;
+            const float g0 = t0 * q0, g1 = t1 * q1;
+            sEr = fmaf(t0, g0, sEr);
+            sEr = fmaf(t1, g1, sEr);
+            A0 += g0 + g1;
+            const float h0 = g0 * cf, h1 = g1 * (cf + 1.f);
+            Bc += h0 + h1;
+            Bcc = fmaf(h0, cf, Bcc);
+            Bcc = fmaf(h1, cf + 1.f, Bcc);
+            cf += 2.f;
+            a += 8u;
+        }
+        if (c < wm) {
+            const float q0 = lds_row(a, c, wl);
+            const float t0 = fmaxf(1.f - s, 0.f);
+            const float g0 = t0 * q0;
+            sEr = fmaf(t0, g0, sEr);
+            A0 += g0;
+            const float h0 = g0 * cf;
+            Bc += h0;
+            Bcc = fmaf(h0, cf, Bcc);
+        }
+        // sum g kx and sum g kx^2 with kx = xs + c
+        const float xf = float(xs);
+        const float B1 = fmaf(xf, A0, Bc);
+        const float B2 = fmaf(xf, fmaf(xf, A0, 2.f * Bc), Bcc);
+        const float dy = fmaf(float(ky), sy, dy0);
+        m.sE += sEr;
+        m.A0t += A0;
+        m.B1t += B1;
+        m.B2t += B2;
+        m.Sy = fmaf(dy, A0, m.Sy);
+        m.Syy = fmaf(dy * dy, A0, m.Syy);
+        m.Sxy = fmaf(dy, B1, m.Sxy);  // sum g kx dy; finish_rows adds the dx0 part
+    }
+    return m;
+}
+
 
 // Photons with a footprint radius of at least cfg.coop_r are splatted by their whole warp:
 // lane j takes rows j, j + 32, ... of the photon and walks each row's span of the support
@@ -249,7 +454,7 @@ __device__ __forceinline__ void rec_box(const Rec& r, const TileInfo& ti, int& p
 }
 
 // Forward deposit of one photon by the whole warp (see use_coop).
-__device__ __forceinline__ void deposit_coop(const Rec& r, const TileInfo& ti, int sw,
+__device__ __noinline__ void deposit_coop(const Rec& r, const TileInfo& ti, int sw,
                                              uint32_t acc_base, int lane) {
     int pxc, pyc, x0, x1, y0, y1;
     rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
@@ -390,7 +595,7 @@ __device__ __forceinline__ int64_t next_chunk(uint32_t* queue, uint32_t* slot) {
     return int64_t(*slot);
 }
 
-template <int NT, int MINB>
+template <int NT, int MINB, bool ROWS>
 __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     extern __shared__ float acc[];
     __shared__ int sb[4];
@@ -423,7 +628,22 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
                 const bool mine = have && i >= sg.begin && i < sg.end;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-                if (mine && !coop) deposit(r, ti, sw, cfg.spans, cfg.band, acc, x0, x1, y0, y1);
+                if constexpr (ROWS) {
+                    // padded-row walk; photons without a band take the generic walk below
+                    RowGeo g;
+                    int rows = 0;
+                    bool generic = false;
+                    if (mine && !coop && !(rec_flags(r.packed) & kFlagFwdSkip)) {
+                        int pxc, pyc;
+                        rec_clip(r, ti, pxc, pyc, x0, x1, y0, y1);
+                        generic = !prep_rows(r, ti, sw, pxc, pyc, x0, x1, y0, y1, g);
+                        rows = generic ? 0 : g.rows;
+                    }
+                    deposit_rows(g, rows, r.e * kThreeOverPi, acc_base, sw);
+                    if (generic) deposit(r, ti, sw, cfg.spans, false, acc, x0, x1, y0, y1);
+                } else if (mine && !coop) {
+                    deposit(r, ti, sw, cfg.spans, cfg.band, acc, x0, x1, y0, y1);
+                }
                 if (coop) {
                     int pxc, pyc;
                     rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
@@ -482,6 +702,17 @@ __device__ __forceinline__ void finish_grad(GradRec* stage, uint32_t rid, float 
                -fmaf(m01, v0, m11 * v1), c * fmaf(m00, Sxx, m01 * Sxy),
                c * fmaf(m00, Sxy, m01 * Syy), c * fmaf(m10, Sxx, m11 * Sxy),
                c * fmaf(m10, Sxy, m11 * Syy));
+}
+
+// The gradients of one photon from its row moments: sum g dx = sx B1t + dx0 A0t and
+// sum g dx dy = sx (sum g kx dy) + dx0 Sy, with dx = kx sx + dx0.
+__device__ __forceinline__ void finish_rows(GradRec* stage, uint32_t slot, const Rec& r,
+                                            const TileInfo& ti, const RowMoments& m) {
+    const float Sx = fmaf(ti.sx, m.B1t, r.dx0 * m.A0t);
+    const float Sxx = fmaf(ti.sx * ti.sx, m.B2t,
+                           fmaf(2.f * ti.sx * r.dx0, m.B1t, r.dx0 * r.dx0 * m.A0t));
+    const float Sxy = fmaf(ti.sx, m.Sxy, r.dx0 * m.Sy);
+    finish_grad(stage, slot, r.e, r.m00, r.m01, r.m10, r.m11, m.sE, Sx, m.Sy, Sxx, Sxy, m.Syy);
 }
 
 // One row of a backward gather: n pixels from q, the first at pixel offset k0 (relative to
@@ -636,7 +867,7 @@ __device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const 
 // Pixels outside the support contribute 0 * g in the reference; with spans on they are not
 // visited. The offset d of pixel (kx, ky) is (kx sx + dx0, ky sy + dy0); moments in x are
 // kept in the integer offset kx and converted once per photon.
-__device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
+__device__ __noinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                        bool band, const float* tg, uint32_t rid,
                                        const TileArgs& a) {
     const uint32_t p = r.packed;
@@ -674,7 +905,7 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
                     sE, A0, B1, B2);
         } else {
             for (int kx = kx0; kx <= kx1; ++kx) {
-                if (!ellipse_ok(kx, ky, ti.wd, ti.hd)) continue;
+                if (!ellipse_ok(kx, ky, img_wd(ti), img_hd(ti))) continue;
                 const float kf = float(kx);
                 const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
                 const float s = fmaf(u0, u0, u1 * u1);
@@ -701,7 +932,7 @@ __device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw,
 
 // Backward gather of one photon by the whole warp (see use_coop): lanes take rows and walk
 // their support spans, and a warp reduction hands the moments to the owning lane.
-__device__ __forceinline__ void gather_coop(const Rec& r, const TileInfo& ti, int sw,
+__device__ __noinline__ void gather_coop(const Rec& r, const TileInfo& ti, int sw,
                                             const float* tg, uint32_t rid, int owner,
                                             const TileArgs& a) {
     const int lane = threadIdx.x & 31;
@@ -747,11 +978,12 @@ __device__ __forceinline__ void gather_coop(const Rec& r, const TileInfo& ti, in
     }
 }
 
-template <int NT, int MINB>
+template <int NT, int MINB, bool ROWS>
 __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
     extern __shared__ float tg[];
     const Cfg cfg = a.cfg;
     const int sw = cfg.sw;
+    const uint32_t tg_base = static_cast<uint32_t>(__cvta_generic_to_shared(tg));
     const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
     __shared__ uint32_t chunk_slot;
@@ -774,7 +1006,24 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
             for (int pass = 0; pass <= NT; ++pass) {
                 const bool mine = have && i >= sg.begin && i < sg.end;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
-                if (mine && !coop) gather(r, ti, sw, cfg.spans, cfg.band, tg, uint32_t(i), a);
+                if constexpr (ROWS) {
+                    // padded-row walk; photons without a band take the generic gather below
+                    RowGeo g;
+                    int rows = 0;
+                    bool walk = false, generic = false;
+                    if (mine && !coop) {
+                        int pxc, pyc, x0, x1, y0, y1;
+                        rec_clip(r, ti, pxc, pyc, x0, x1, y0, y1);
+                        walk = prep_rows(r, ti, sw, pxc, pyc, x0, x1, y0, y1, g);
+                        generic = !walk;
+                        rows = walk ? g.rows : 0;
+                    }
+                    const RowMoments m = gather_rows(g, rows, tg_base, sw, ti.sy, r.dy0);
+                    if (walk) finish_rows(a.stage, uint32_t(i), r, ti, m);
+                    if (generic) gather(r, ti, sw, cfg.spans, false, tg, uint32_t(i), a);
+                } else if (mine && !coop) {
+                    gather(r, ti, sw, cfg.spans, cfg.band, tg, uint32_t(i), a);
+                }
                 for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
                     const int src = __ffs(cm) - 1;
                     const Rec rb = shfl_rec(r, src);
@@ -1044,10 +1293,10 @@ void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st) {
     iota_kernel<<<unsigned(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(dst, n);
 }
 
-template <int MINB>
+template <int MINB, bool ROWS>
 cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
     const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
-    auto kern = fwd_tiles_kernel<kTileThreads, MINB>;
+    auto kern = fwd_tiles_kernel<kTileThreads, MINB, ROWS>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
@@ -1063,10 +1312,10 @@ cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
     return e;
 }
 
-template <int MINB>
+template <int MINB, bool ROWS>
 cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
     const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
-    auto kern = bwd_tiles_kernel<kTileThreads, MINB>;
+    auto kern = bwd_tiles_kernel<kTileThreads, MINB, ROWS>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
@@ -1099,13 +1348,25 @@ cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
 }
 
 cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
-    if (a.cfg.min_blocks >= 4) return launch_forward_t<4>(a, st);
-    return a.cfg.min_blocks == 3 ? launch_forward_t<3>(a, st) : launch_forward_t<2>(a, st);
+    if (a.cfg.rows) {
+        if (a.cfg.min_blocks >= 4) return launch_forward_t<4, true>(a, st);
+        return a.cfg.min_blocks == 3 ? launch_forward_t<3, true>(a, st)
+                                     : launch_forward_t<2, true>(a, st);
+    }
+    if (a.cfg.min_blocks >= 4) return launch_forward_t<4, false>(a, st);
+    return a.cfg.min_blocks == 3 ? launch_forward_t<3, false>(a, st)
+                                 : launch_forward_t<2, false>(a, st);
 }
 
 cudaError_t launch_backward(const TileArgs& a, cudaStream_t st) {
-    if (a.cfg.min_blocks >= 4) return launch_backward_t<4>(a, st);
-    return a.cfg.min_blocks == 3 ? launch_backward_t<3>(a, st) : launch_backward_t<2>(a, st);
+    if (a.cfg.rows) {
+        if (a.cfg.min_blocks >= 4) return launch_backward_t<4, true>(a, st);
+        return a.cfg.min_blocks == 3 ? launch_backward_t<3, true>(a, st)
+                                     : launch_backward_t<2, true>(a, st);
+    }
+    if (a.cfg.min_blocks >= 4) return launch_backward_t<4, false>(a, st);
+    return a.cfg.min_blocks == 3 ? launch_backward_t<3, false>(a, st)
+                                 : launch_backward_t<2, false>(a, st);
 }
 
 }  // namespace pds

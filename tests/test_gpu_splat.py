@@ -75,7 +75,11 @@ def test_uniform_cluster_512(cuda):
                                  dict(coop_radius=1), dict(coop_radius=-1),
                                  dict(coop_radius=2, min_blocks=2), dict(walk=1),
                                  dict(walk=1, coop_radius=5), dict(walk=3, coop_radius=4, tile=32),
-                                 dict(min_blocks=4), dict(min_blocks=4, class_bits=3)])
+                                 dict(min_blocks=4), dict(min_blocks=4, class_bits=3),
+                                 dict(walk=3, class_bits=5), dict(walk=4, min_blocks=2),
+                                 dict(walk=4, class_bits=5), dict(walk=4, tile=32),
+                                 dict(walk=4, coop_radius=4), dict(walk=4, class_bits=-1),
+                                 dict(walk=4, tile=16, apron_max=5)])
 def test_tuning_variants(cuda, cfg):
     ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
     assert_parity(ph, (1, 256, 256), 20, cfg=cfg)
@@ -96,7 +100,8 @@ def test_wide_footprints_take_the_direct_path(cuda):
 
 
 @pytest.mark.parametrize("cfg", [dict(walk=1, coop_radius=3), dict(walk=1, coop_radius=-1),
-                                 dict(), dict(class_bits=4), dict(walk=2)])
+                                 dict(), dict(class_bits=4), dict(walk=2), dict(walk=3),
+                                 dict(walk=4, min_blocks=2)])
 def test_caustic_curves_large_footprints(cuda, cfg):
     # the contention workload's shape at a small size: most photons on thin curves
     ph = S.caustic_curve_photons(2 ** 16, 256, 256, seed=13, s_range=(0.25, 16.0))
