@@ -738,12 +738,12 @@ def plate_setup(n_field, image, per_texel, device, seed=0, texel=0.1, dist=50.0)
     """Height-field plate of the Landweber workloads: a 1 mm base plus 32 Gaussian bumps
     (amplitude U[0, 50] um, width U[4, 24] texels), collimated light at normal incidence,
     n = 1.5, receiver 50 mm below; photons jittered per texel."""
-    from shapefromcaustics_b200 import refraction as RF
+    from shapefromcaustics_b200 import scene as SC
     half = 0.5 * n_field * texel * 1.1
-    scene = RF.PlateScene(texel=texel, ior=1.5, receiver_distance=dist, receiver_half=half)
-    h = RF.height_field_bumps(n_field, n_field, seed=seed, bumps=32, base=1.0,
+    scene = SC.PlateScene(texel=texel, ior=1.5, receiver_distance=dist, receiver_half=half)
+    h = SC.height_field_bumps(n_field, n_field, seed=seed, bumps=32, base=1.0,
                               amp=(0.0, 0.05), width=(4.0, 24.0)).float().to(device)
-    t = RF.height_field_bumps(n_field, n_field, seed=seed + 1, bumps=32, base=1.0,
+    t = SC.height_field_bumps(n_field, n_field, seed=seed + 1, bumps=32, base=1.0,
                               amp=(0.0, 0.05), width=(4.0, 24.0)).float().to(device)
     return scene, h, t
 

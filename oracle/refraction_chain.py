@@ -1,4 +1,8 @@
-"""Refraction-to-receiver for a glass plate with a height-field top surface, in PyTorch ops.
+"""FP64 restatement of the refraction-to-receiver chain for a height-field glass plate.
+TEST INFRASTRUCTURE ONLY: the tests use it as the float64 reference of the fused refraction
+kernels (``pds_refract_forward_f32`` / ``pds_refract_backward_f32``); the product never imports
+it. Its building blocks are pinned to the reference's own functions by the fixture
+``tests/golden/refraction_ref.npz`` (``tests/golden/make_refraction_golden.py``).
 
 The differentiable step between a height field and the splat inputs, for collimated light
 falling on the plate (the analytic height-field case the reference's OptiX tracer handles for
@@ -10,17 +14,19 @@ this scene). Per photon:
   2. positional-differential transfer onto the surface (Frisvad 2014,
      ``model/photon_differential.py:69-78``): ``D' = D - (n.D)/(n.d) d + t (Dd - (n.Dd)/(n.d) d)``.
   3. Snell refraction of the direction and of its differentials (Igehy 1999,
-     ``model/caustics.py:152-212``, refraction branch): with ``cosi = d.N``, ``eta``,
+     ``model/caustics.py:152-212``): with ``cosi = d.N``, ``eta``,
      ``k = 1 - eta^2 (1 - cosi^2)``, ``coso = eta cosi + sqrt(k)``,
      ``d' = eta d - coso N`` and
      ``Dd' = eta Dd - (coso dN + (eta - eta^2 cosi / -sqrt(k)) (Dd.N + d.dN) N)``;
-     the normal derivative ``dN`` along the positional differential uses
+     a ray leaving the denser side (``d.N > 0``) swaps the indices and flips the normal, and
+     ``k <= 0`` reflects (``d - 2 (d.N) N``, Igehy's reflection differentials), as the
+     reference does; the normal derivative ``dN`` along the positional differential uses
      ``(|N|^2 dN~ - (N.dN~) N) / |N|^3`` of the un-normalised normal ``N~``
      (``model/renderable_object.py:391-401``).
   4. propagation inside the glass to the flat bottom face (z = 0), refraction out
      (flat face: ``dN = 0``), propagation to the receiver plane ``z = -receiver_distance``.
   5. receiver coordinates normalised by the receiver half-extent, and the splat inputs of
-     ``model/caustics.py:224-239`` (``caustics.splat_inputs``).
+     ``model/caustics.py:224-239`` (``change_of_basis_matrix``, ``splat_photons``).
 
 The normal derivative is taken along the photon's whole positional differential at the hit
 (position and direction parts). The reference passes only the direction-induced part
@@ -35,30 +41,11 @@ import math
 import torch
 import torch.nn.functional as F
 
-from .caustics import splat_inputs
+from shapefromcaustics_b200.scene import PlateScene, height_field_bumps  # noqa: F401
 
 __all__ = ["PlateScene", "sobel_normals", "sample_surface", "trace_to_receiver",
-           "height_field_bumps", "jittered_photons"]
-
-
-class PlateScene:
-    """Glass plate over a receiver.
-
-    ``texel``: height-field texel size (mm), the field spans ``[-W texel/2, W texel/2]`` in x
-    (columns) and the same in y (rows); ``ior``: refractive index; ``receiver_distance``:
-    from the flat bottom face (z = 0) to the receiver (mm); ``receiver_half``: half-extent of
-    the square receiver (mm); ``light_dir``: unit propagation direction (default straight
-    down).
-    """
-
-    def __init__(self, texel=0.1, ior=1.5, receiver_distance=50.0, receiver_half=14.08,
-                 light_dir=(0.0, 0.0, -1.0)):
-        self.texel = float(texel)
-        self.ior = float(ior)
-        self.receiver_distance = float(receiver_distance)
-        self.receiver_half = float(receiver_half)
-        d = torch.tensor(light_dir, dtype=torch.float64)
-        self.light_dir = tuple((d / d.norm()).tolist())
+           "height_field_bumps", "jittered_photons", "splat_inputs", "refract_differentials",
+           "transfer"]
 
 
 def sobel_normals(h, texel):
@@ -110,24 +97,73 @@ def _dot(a, b):
     return (a * b).sum(0)
 
 
-def _transfer(D, Dd, t, n, d):
-    """Positional differential carried along direction d for length t onto a plane of normal n
-    (``model/photon_differential.py:69-78``)."""
+def transfer(D, Dd, t, n, d):
+    """Positional differential D with direction differential Dd carried along direction d for
+    length t onto a plane of normal n (``model/photon_differential.py:69-78``: the hit's
+    positional part ``D - (n.D)/(n.d) d`` plus ``t (Dd - (n.Dd)/(n.d) d)``)."""
     nd = _dot(n, d)
     return D - _dot(n, D) / nd * d + t * (Dd - _dot(n, Dd) / nd * d)
 
 
-def _refract(d, N, Dd, dN, eta):
-    """Refraction of direction d and its differential Dd at unit normal N (facing the incident
-    side, d.N < 0), ``model/caustics.py:176-189``. Total internal reflection is not handled
-    (it does not occur for the plate geometries here)."""
+_transfer = transfer
+
+
+def refract_differentials(d, N, Dd, dN, n_outer, n_inner):
+    """Direction and direction differential after refraction (or total internal reflection)
+    at unit normal N with normal derivative dN, ``model/caustics.py:152-212``:
+    ``cosi = clamp(d.N, -1, 1)``; where ``cosi > 0`` the indices swap and N, dN flip sign
+    (``cosi`` itself keeps its sign, as in the reference); ``eta = n_i / n_t``,
+    ``k = 1 - eta^2 (1 - cosi^2)``; ``k > 0`` refracts (Igehy 1999, p. 4), otherwise the ray
+    reflects, ``d - 2 cosi N`` with ``Dd - 2 (cosi dN + (Dd.N + d.dN) N)`` (p. 3).
+    Vectors are ``[3, N]``; ``n_outer``, ``n_inner`` scalars or ``[N]``."""
     cosi = _dot(d, N).clamp(-1, 1)
+    flip = cosi > 0
+    no = torch.as_tensor(n_outer, dtype=d.dtype, device=d.device).expand_as(cosi)
+    ni = torch.as_tensor(n_inner, dtype=d.dtype, device=d.device).expand_as(cosi)
+    etai = torch.where(flip, ni, no)
+    etat = torch.where(flip, no, ni)
+    sgn = torch.where(flip, -torch.ones_like(cosi), torch.ones_like(cosi))
+    Nf = sgn * N
+    dNf = sgn * dN
+    eta = etai / etat
     k = 1 - eta * eta * (1 - cosi * cosi)
-    neg_sq = -torch.sqrt(k.clamp(min=0))
+    rm = k > 0
+    neg_sq = -torch.sqrt(torch.where(rm, k, torch.ones_like(k)))
     coso = eta * cosi - neg_sq
-    out = eta * d - coso * N
-    Dout = eta * Dd - (coso * dN + ((eta - eta * eta * cosi / neg_sq) * (_dot(Dd, N) + _dot(d, dN))) * N)
-    return out, Dout
+    dn_term = _dot(Dd, Nf) + _dot(d, dNf)
+    out_r = eta * d - coso * Nf
+    Dout_r = eta * Dd - (coso * dNf + ((eta - eta * eta * cosi / neg_sq) * dn_term) * Nf)
+    out_l = d - 2 * cosi * Nf
+    Dout_l = Dd - 2 * (cosi * dNf + dn_term * Nf)
+    return torch.where(rm, out_r, out_l), torch.where(rm, Dout_r, Dout_l)
+
+
+def _refract(d, N, Dd, dN, eta):
+    """Refraction at unit normal N facing the incident side (d.N < 0) with index ratio eta."""
+    return refract_differentials(d, N, Dd, dN, eta, 1.0)
+
+
+def change_of_basis_matrix(Du, Dv, normal):
+    """``model/caustics.py:224-230``: ``Mp = 2 / (Du.(Dv x n)) [Dv x n ; n x Du]`` (2 x 3 x N)
+    and the non-degenerate mask (denominator != 0); degenerate photons get a finite
+    placeholder here instead of being dropped."""
+    tmp = torch.cross(Dv, normal, dim=0)
+    den = (Du * tmp).sum(0)
+    good = den != 0
+    factor = 2.0 / torch.where(good, den, torch.ones_like(den))
+    return factor * torch.stack((tmp, torch.cross(normal, Du, dim=0)), dim=0), good
+
+
+def splat_inputs(Du, Dv, normal, flux, channel):
+    """Splat inputs ``(Ep, Mp, cp, radius)`` of ``model/caustics.py:233-239``:
+    ``radius = 0.5 max(|Du|, |Dv|)``, ``Ep = 4 flux / |Du x Dv|``; degenerate photons keep
+    their slot with channel -1 (the splat skips them)."""
+    Mp, good = change_of_basis_matrix(Du, Dv, normal)
+    radius = 0.5 * torch.maximum(Du.norm(dim=0), Dv.norm(dim=0))
+    area = torch.cross(Du, Dv, dim=0).norm(dim=0)
+    Ep = flux / torch.where(good, area, torch.ones_like(area)) * 4
+    cp = torch.where(good, channel, torch.full_like(channel, -1)).reshape(1, -1)
+    return Ep.contiguous(), Mp.contiguous(), cp.contiguous(), radius.contiguous()
 
 
 def _unit_normal_and_derivative(Nt, dNt):
@@ -180,23 +216,6 @@ def trace_to_receiver(h, scene, px, py, Du0, Dv0):
     Dv3 = _transfer(Dv2, Ddv2, s2, nz, t2)
     inv = 1.0 / scene.receiver_half
     return p3[:2] * inv, Du3 * inv, Dv3 * inv
-
-
-def height_field_bumps(H, W, seed=0, bumps=32, base=1.0, amp=(0.0, 0.05), width=(4.0, 24.0),
-                       dtype=torch.float64, device="cpu"):
-    """Base thickness plus Gaussian bumps (amplitude and width uniform in the given ranges,
-    width in texels, centres uniform); millimetres."""
-    g = torch.Generator(device="cpu").manual_seed(int(seed))
-    cy = torch.rand(bumps, generator=g, dtype=torch.float64) * H
-    cx = torch.rand(bumps, generator=g, dtype=torch.float64) * W
-    a = amp[0] + torch.rand(bumps, generator=g, dtype=torch.float64) * (amp[1] - amp[0])
-    w = width[0] + torch.rand(bumps, generator=g, dtype=torch.float64) * (width[1] - width[0])
-    yy, xx = torch.meshgrid(torch.arange(H, dtype=torch.float64), torch.arange(W, dtype=torch.float64),
-                            indexing="ij")
-    h = torch.full((H, W), base, dtype=torch.float64)
-    for k in range(bumps):
-        h += a[k] * torch.exp(-((yy - cy[k]) ** 2 + (xx - cx[k]) ** 2) / (2 * w[k] ** 2))
-    return h.to(dtype=dtype, device=device)
 
 
 def jittered_photons(H, W, scene, per_texel=4, seed=0, smoothing=4.0, dtype=torch.float64,

@@ -1,25 +1,22 @@
 """Projected Landweber update of the height field and the reconstruction loop around it.
 
-``landweber_update`` is the fused device update (``pds_landweber_update_f32``);
-``landweber_update_reference`` restates the reference's PyTorch ops
-(``shape_from_caustics.py:184-189`` extShrink, ``:228-241`` VconsHeur, ``:386-398`` the
-update) for tests. ``reconstruct`` runs the reference's pixel-basis Landweber loop
+``landweber_update`` is the fused device update (``pds_landweber_update_f32``) of the
+reference's PyTorch ops (``shape_from_caustics.py:184-189`` extShrink, ``:228-241``
+VconsHeur, ``:386-398`` the update). ``reconstruct`` runs the reference's pixel-basis Landweber loop
 (``optimization_loop_landweber_pixel``, ``:343-420``) for a height-field plate on the
 sm_100a kernels: simulate (refraction + splat), L2 discrepancy against the target image,
 backward to the height field, update.
 """
 import ctypes
-import math
 from dataclasses import dataclass
 
 import torch
-import torch.nn.functional as F
 
 from . import _lib
 from ._lib import check, lib
 from .splatting import _ptr, _stream
 
-__all__ = ["LandweberParams", "landweber_update", "landweber_update_reference"]
+__all__ = ["LandweberParams", "landweber_update", "reconstruct"]
 
 
 @dataclass
@@ -61,32 +58,6 @@ def landweber_update(d, grad, mask, params, workspace=None):
                                              ctypes.byref(p), _ptr(workspace), workspace.numel(),
                                              _stream(d.device)))
     return d
-
-
-def ext_shrink(x, alpha, a, b):
-    """``shape_from_caustics.py:184-189``."""
-    zeros = torch.zeros_like(x)
-    ones = torch.ones_like(x)
-    return torch.max(torch.min(torch.max(torch.abs(x) - alpha, zeros) * torch.sign(x), b * ones),
-                     a * ones)
-
-
-def vcons_heur(x, d1, d2, mask, gamma, radius):
-    """``shape_from_caustics.py:228-241``."""
-    vx = torch.sum(x)
-    xmean = F.avg_pool2d(x[None, None], 2 * radius + 1, stride=1, padding=radius)[0, 0]
-    if vx <= d1:
-        x = x + mask * xmean * torch.sin(vx / d1 * math.pi) * gamma
-    elif vx >= d2:
-        x = x - mask * xmean * torch.sin((vx / d2 - 1) * math.pi) * gamma
-    return x
-
-
-def landweber_update_reference(d, grad, mask, params):
-    """The reference's update ops (``shape_from_caustics.py:386-398``), out of place."""
-    x = d - params.tau * grad
-    x = mask * ext_shrink(x, params.tau * params.alpha, params.lower, params.upper)
-    return vcons_heur(x, params.d1, params.d2, mask, params.gamma, params.radius)
 
 
 def render_plate(height, scene, px, py, flux, params, shape, max_pixel_radius=20):

@@ -10,7 +10,7 @@ field: refracted positions and differentials are never stored, and with
 the height field and the photons' entry points (12 bytes per photon).
 
 ``photons`` is ``(px, py, flux)`` (``[N]`` each, float32, device) plus an optional channel
-``[N]`` int64; ``plate`` a ``PlateScene`` (``refraction.py``) with ``du0``, the initial
+``[N]`` int64; ``plate`` a ``PlateScene`` (``scene.py``) with ``du0``, the initial
 positional differential length.
 """
 import ctypes

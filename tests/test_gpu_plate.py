@@ -7,7 +7,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from shapefromcaustics_b200 import refraction as RF
+from oracle import refraction_chain as RF
 
 pytestmark = pytest.mark.gpu
 
@@ -98,8 +98,8 @@ def test_plate_splat_end_to_end_gradient(cuda):
 
 @pytest.mark.parametrize("vol", ["low", "mid", "high"])
 def test_landweber_update_matches_reference_ops(cuda, vol):
-    from shapefromcaustics_b200.landweber import (LandweberParams, landweber_update,
-                                                  landweber_update_reference)
+    from oracle.landweber_ref import landweber_update_reference
+    from shapefromcaustics_b200.landweber import LandweberParams, landweber_update
     g = torch.Generator().manual_seed(3)
     H, W = 130, 97
     d = torch.rand((H, W), generator=g) * 0.2
@@ -137,3 +137,51 @@ def test_photon_source_matches_philox_restatement(cuda):
     jx = (px - ((t % 64).float() - 31.5)).cpu().numpy()
     assert abs(jx.mean()) < 5e-3 and abs(jx.var() - 1 / 12) < 2e-3
     assert jx.min() >= -0.5 and jx.max() <= 0.5  # (ix + j rounds to the texel edge at most)
+
+
+def test_refract_forward_matches_the_reference_functions_fixture(cuda):
+    """pds_refract_forward_f32 against the plate's chain composed from the reference's own
+    functions in float64 (tests/golden/refraction_ref.npz; float32 kernel, float64 fixture)."""
+    import os
+    from shapefromcaustics_b200 import plate as PL
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                "refraction_ref.npz"))
+    texel, ior, dist, half, du0 = (float(v) for v in gold["chain_params"])
+    scene = RF.PlateScene(texel=texel, ior=ior, receiver_distance=dist, receiver_half=half,
+                          light_dir=tuple(gold["chain_light"]))
+    params = PL.plate_params(scene, du0)
+    h = torch.from_numpy(gold["chain_h"]).float().cuda()
+    px, py, flux = (torch.from_numpy(gold[k]).float().cuda()
+                    for k in ("chain_px", "chain_py", "chain_flux"))
+    Ep, xp, Mp, cp, radius = PL.refract_forward(h, px, py, flux, params)
+    torch.cuda.synchronize()
+    assert bool((cp >= 0).all())
+    assert rel_l2(xp.cpu(), gold["chain_xp"]) < 1e-6
+    assert rel_l2(Ep.cpu(), gold["chain_Ep"]) < 1e-4
+    assert rel_l2(Mp.cpu(), gold["chain_Mp"]) < 1e-4
+    assert rel_l2(radius.cpu(), gold["chain_radius"]) < 1e-4
+
+
+def test_config2_gpu_gradient_matches_fp64_central_differences(cuda):
+    """The 256^2 Landweber configuration in full on the GPU (float32 refraction + splat
+    kernels, PlateSplat): the height-field gradient of 0.5 |I - T|^2 against FP64 central
+    differences on 64 random texels (texels whose photons keep their truncation boxes under
+    the steps)."""
+    import plate_fd as PF
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, t, photons, du0 = PF.config2()
+    target = PF.splat64(t, scene, photons)
+    params = PL.plate_params(scene, du0)
+    px, py, _, _, flux = (x.float().cuda() for x in photons)
+    shape = (1, PF.IMAGE, PF.IMAGE)
+    hv = h.float().cuda().requires_grad_(True)
+    img = PL.PlateSplat.apply(hv, px, py, flux, params, shape, PF.MPR, True)
+    loss = 0.5 * ((img - torch.from_numpy(target).float().cuda()) ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    texels, skipped = PF.smooth_texels(h, scene, photons, 64)
+    an = np.array([float(hv.grad[i, j]) for (i, j) in texels])
+    fd, smooth = PF.fd_gradient(h, target, scene, photons, texels)
+    assert smooth.all() and skipped < 64
+    err = np.linalg.norm(fd - an) / np.linalg.norm(fd)
+    assert err < 1e-3, (err, fd, an)
