@@ -808,35 +808,46 @@ def run_landweber_step(args, rank, world, device):
 def run_reconstruction(args, rank, world, device):
     """Full reconstruction: 1024^2 field, 16 simulations x 4 photons per texel (2^22 each,
     67M per iteration) into a 1024^2 image, Landweber iterations with the refracted photon
-    positions recomputed in the backward; final height RMSE and peak HBM."""
-    from shapefromcaustics_b200.landweber import reconstruct
+    positions recomputed in the backward; final height RMSE, peak HBM and the CUDA-event time
+    of each phase of one iteration."""
+    from shapefromcaustics_b200.landweber import LandweberParams, iteration_phases, reconstruct
     torch.cuda.set_device(device)
     nf = 1024
     scene, h_true, _ = plate_setup(nf, nf, 4, device, seed=7)
+    d_true = h_true - 1.0
+    vol = float(d_true.sum())
+    params = LandweberParams(tau=args.recon_tau, d1=0.75 * vol, d2=1.25 * vol)
     torch.cuda.reset_peak_memory_stats(device)
     iters = args.steps
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
     res = reconstruct(h_true, 1.0, scene, iterations=iters, sims=16, per_texel=4, image=nf,
-                      footprint_px=3.0, seed=rank, keep_plan=False,
-                      log_every=max(iters // 10, 1))
+                      footprint_px=args.recon_footprint, params=params, seed=rank,
+                      keep_plan=False, log_every=max(iters // 10, 1),
+                      objective=args.recon_objective)
     t1.record()
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
     peak = torch.cuda.max_memory_allocated(device)
-    d_true = h_true - 1.0
+    phases = iteration_phases(1.0, res["target"], scene, res["d"].clone(),
+                              torch.ones_like(h_true), params, sims=16, per_texel=4, image=nf,
+                              footprint_px=args.recon_footprint, seed=rank + 99,
+                              objective=args.recon_objective)
     return {"metric": "Landweber it/s", "value": iters / (ms / 1e3), "unit": "it/s",
             "n_gpus": world, "steps": iters, "warmup": 0, "ms_per_step": ms / iters,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "recon1024: 1024^2 field, 16 sims x 2^22 photons per "
                                    "iteration into 1024^2, positions recomputed in backward",
-                       "photons_per_iteration": res["photons_per_iteration"]},
+                       "photons_per_iteration": res["photons_per_iteration"],
+                       "objective": args.recon_objective, "tau": args.recon_tau,
+                       "footprint_px": args.recon_footprint},
             "final_height_rmse_mm": res["rmse"],
             "initial_height_rmse_mm": float((d_true ** 2).mean().sqrt()),
             "rmse_history": res["history"]["rmse"],
             "discrepancy_history": res["history"]["discrepancy"],
+            "phase_ms": phases,
             "peak_hbm_bytes": peak}
 
 
@@ -859,6 +870,12 @@ def main():
                          "(for profiler runs)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-sample", type=float, default=2 ** 21)
+    ap.add_argument("--recon-objective", default="l2_sq", choices=["l2_sq", "normalized"],
+                    help="recon1024: the reference's 0.5 |I - T|^2 or it divided by |T|^2")
+    ap.add_argument("--recon-tau", type=float, default=0.1,
+                    help="recon1024: gradient step (the reference's tau_pixel)")
+    ap.add_argument("--recon-footprint", type=float, default=3.0,
+                    help="recon1024: initial photon footprint in receiver pixels")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -127,6 +127,20 @@ int pds_backward_planned_f32(const float* grad_pds, const float* Ep, const float
                              float* grad_xp, float* grad_Mp, void* workspace,
                              size_t workspace_bytes, const pds_config* cfg, void* stream);
 
+/* The binning of a plan built by pds_plan_f32 or pds_batch_plan_f32 (the same n, tile count,
+ * max_pixel_radius and config), per photon, for checks of its exactness; it has no
+ * counterpart in the reference, whose kernels do not bin. bucket[i] is the photon's sort key:
+ * (tile << class_bits) | footprint class for photons of the tile path, with tile = the
+ * simulation's tile_base + (channel * tiles_y + ty) * tiles_x + tx of the photon's centre pixel
+ * clamped into the image; n_tiles << class_bits for photons whose footprint is wider than the
+ * tile path holds; (n_tiles + 1) << class_bits for photons that touch no pixel (channel out of
+ * range or an empty clipped box). slot[i] is the photon's position in the sorted order (tile
+ * path), its index in the wide list, or 0xFFFFFFFF. n_tiles: C * tiles_y * tiles_x for a single
+ * simulation, the total from pds_batch_layout for a batch. */
+int pds_plan_export(const void* workspace, size_t workspace_bytes, int64_t n_photons,
+                    int64_t n_tiles, int32_t max_pixel_radius, const pds_config* cfg,
+                    uint32_t* bucket, uint32_t* slot, void* stream);
+
 /* ---- batches of uneven simulations in one launch sequence -------------------------- */
 /* The reference runs its simulations one after another and sums them
  * (shape_from_caustics.py:351-353); these entry points run many simulations, each with

@@ -3,7 +3,7 @@
 // This layer validates arguments the way the reference's binding does
 // (PyOptix/PhotonDifferentialSplattig.cpp:14-22: matching photon counts, 2-row positions,
 // 2x3 matrices, one channel row), lays the workspace out, and enqueues
-//   plan:     counter and bucket-count reset, plan_kernel, bucket scan, bucket_scatter,
+//   plan:     counter and bucket-count reset, plan count pass, bucket scan, plan place pass,
 //             chunk_tile_kernel
 //   forward:  output reset, fwd_tiles_kernel, tail_fwd_kernel
 //   backward: bwd_tiles_kernel, tail_bwd_kernel, grad_scatter_kernel
@@ -107,11 +107,12 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, int64_t n, Resol
     return PDS_OK;
 }
 
-// The plan's workspace. recs holds the records in photon order until bucket_scatter has copied
-// them into srecs in sorted order; it is then free, and the backward reuses it for its
-// gradient records.
+// The plan's workspace: the inverse map, the wide list, the records in sorted order, the
+// bucket counts, starts and cursors, each plan CTA's window histogram (kept from the count pass
+// for the place pass), the chunks' tiles, and the backward's gradient records (stage, 32 bytes
+// a photon).
 struct Layout {
-    size_t counters, keys, inv, wide, recs, srecs, counts, start, cursor, part, chunk_tile,
+    size_t counters, inv, wide, stage, srecs, counts, start, cursor, part, cta_hist, chunk_tile,
         total;
 };
 
@@ -122,15 +123,16 @@ Layout make_layout(int64_t n, int64_t nb) {
     const size_t nbb = size_t(nb > 0 ? nb : 1);
     size_t off = 0;
     L.counters = off; off += 256;
-    L.keys = off; off += pds::align_up(nn * 4, 256);
     L.inv = off; off += pds::align_up(nn * 4, 256);
     L.wide = off; off += pds::align_up(nn * 4, 256);
-    L.recs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
+    L.stage = off; off += pds::align_up(nn * sizeof(pds::GradRec), 256);
     L.srecs = off; off += pds::align_up(nn * sizeof(pds::Rec), 256);
     L.counts = off; off += pds::align_up(nbb * 4, 256);
     L.start = off; off += pds::align_up((nbb + 1) * 4, 256);
     L.cursor = off; off += pds::align_up(nbb * 4, 256);
     L.part = off; off += pds::align_up(size_t(pds::bucket_scan_parts(int64_t(nbb))) * 4, 256);
+    L.cta_hist = off;
+    off += pds::align_up(size_t(pds::plan_hist_entries(int64_t(nn), int64_t(nbb))) * 4, 256);
     L.chunk_tile = off; off += pds::align_up((nn / 256 + 2) * 4, 256);  // chunks >= 256
     L.total = off;
     return L;
@@ -138,8 +140,7 @@ Layout make_layout(int64_t n, int64_t nb) {
 
 struct Bufs {
     uint32_t* counters;
-    uint32_t *keys, *inv, *wide, *counts, *start, *cursor, *part, *chunk_tile;
-    pds::Rec* recs;
+    uint32_t *inv, *wide, *counts, *start, *cursor, *part, *cta_hist, *chunk_tile;
     pds::Rec* srecs;
     pds::GradRec* stage;
 };
@@ -148,18 +149,16 @@ Bufs bufs(void* ws, const Layout& L) {
     char* b = static_cast<char*>(ws);
     Bufs r;
     r.counters = reinterpret_cast<uint32_t*>(b + L.counters);
-    r.keys = reinterpret_cast<uint32_t*>(b + L.keys);
     r.inv = reinterpret_cast<uint32_t*>(b + L.inv);
     r.wide = reinterpret_cast<uint32_t*>(b + L.wide);
     r.counts = reinterpret_cast<uint32_t*>(b + L.counts);
     r.start = reinterpret_cast<uint32_t*>(b + L.start);
     r.cursor = reinterpret_cast<uint32_t*>(b + L.cursor);
     r.part = reinterpret_cast<uint32_t*>(b + L.part);
+    r.cta_hist = reinterpret_cast<uint32_t*>(b + L.cta_hist);
     r.chunk_tile = reinterpret_cast<uint32_t*>(b + L.chunk_tile);
-    r.recs = reinterpret_cast<pds::Rec*>(b + L.recs);
     r.srecs = reinterpret_cast<pds::Rec*>(b + L.srecs);
-    r.stage = reinterpret_cast<pds::GradRec*>(b + L.recs);
-    static_assert(sizeof(pds::GradRec) == sizeof(pds::Rec), "gradient records reuse recs");
+    r.stage = reinterpret_cast<pds::GradRec*>(b + L.stage);
     return r;
 }
 
@@ -252,37 +251,34 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.cfg = r.cfg;
     a.key_big = r.key_big;
     a.key_invalid = r.key_invalid;
-    a.keys = b.keys;
-    a.recs = b.recs;
     a.counts = b.counts;
     a.inv = b.inv;
     a.wide = b.wide;
     a.counters = b.counters;
+    a.cta_hist = b.cta_hist;
+    a.cursor = b.cursor;
+    a.srecs = b.srecs;
     pds::plan_shape(ph.n, r.n_buckets, &a.window, &a.range);
-    e = pds::launch_plan(a, s);
-    if (e != cudaSuccess) return cuda_fail(e, "plan_kernel");
-    pds::ScatterArgs sa;
-    sa.sims = st;
-    sa.keys = b.keys;
-    sa.recs = b.recs;
+    e = pds::launch_plan_count(a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "plan count pass");
+    pds::ScanArgs sa;
     sa.counts = b.counts;
     sa.counters = b.counters;
     sa.part = b.part;
     sa.start = b.start;
     sa.cursor = b.cursor;
-    sa.srecs = b.srecs;
-    sa.inv = b.inv;
     sa.chunk_tile = b.chunk_tile;
     sa.n = ph.n;
     sa.nb = r.n_buckets;
     sa.n_tiles = n_tiles;
-    sa.range = a.range;
-    sa.window = a.window;
-    sa.key_big = r.key_big;
     sa.chunk = r.cfg.chunk;
     sa.cb = r.cfg.class_bits;
-    e = pds::launch_bucket_sort(sa, s);
-    if (e != cudaSuccess) return cuda_fail(e, "bucket sort");
+    e = pds::launch_bucket_scan(sa, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bucket scan");
+    e = pds::launch_plan_place(a, s);
+    if (e != cudaSuccess) return cuda_fail(e, "plan place pass");
+    e = pds::launch_chunk_tiles(sa, s);
+    if (e != cudaSuccess) return cuda_fail(e, "chunk_tile_kernel");
     return PDS_OK;
 }
 
@@ -618,6 +614,24 @@ int pds_landweber_update_noalloc_f32(float* d, const float* grad, const float* m
     e = pds::launch_landweber(d, grad, mask, rows, cols, *p, t, partial,
                               static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "landweber kernels (noalloc)");
+    return PDS_OK;
+}
+
+int pds_plan_export(const void* ws, size_t ws_bytes, int64_t n, int64_t n_tiles, int32_t mpr,
+                    const pds_config* cfg, uint32_t* bucket, uint32_t* slot, void* stream) {
+    if (n < 0 || n >= int64_t(0x7FFFFFFFll))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "photon count outside [0, 2^31 - 1)");
+    if (n > 0 && (!bucket || !slot)) return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
+    Resolved r;
+    int rc = resolve(cfg, mpr, n_tiles, n, r);
+    if (rc) return rc;
+    const Layout L = make_layout(n, r.n_buckets);
+    rc = check_ws(const_cast<void*>(ws), ws_bytes, L.total);
+    if (rc) return rc;
+    const Bufs b = bufs(const_cast<void*>(ws), L);
+    cudaError_t e = pds::launch_plan_export(b.inv, b.start, r.n_buckets, r.key_big, r.key_invalid,
+                                            n, bucket, slot, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "plan_export_kernel");
     return PDS_OK;
 }
 

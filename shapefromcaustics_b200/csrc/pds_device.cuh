@@ -308,9 +308,39 @@ __host__ __device__ __forceinline__ uint32_t row_class(int rows, int w) {
     return (row_level(rows) << 3) | row_level(w);
 }
 
-// delta = (2 p_c / w - 1) - x in double, rounded once to float.
+// The row class of the plan's sort key, from the band's row range and width in IEEE
+// round-to-nearest single-precision operations in a fixed order (no contraction, no
+// approximate intrinsics), so that a CPU restatement of the binning reproduces every key bit
+// for bit. It follows make_band's geometry (the walks themselves use make_band; a photon whose
+// rows or width round differently here lands in a neighbouring class, which only changes how
+// photons are grouped). kxb0..kyb1: the clipped box in offsets from the centre pixel; the last
+// class when the photon takes the generic walk (no band).
+__device__ __forceinline__ uint32_t plan_row_class(float m00, float m01, float m10, float m11,
+                                                   float dy0, int32_t W, int32_t H, int rx,
+                                                   int kxb0, int kxb1, int kyb0, int kyb1) {
+    const float a = __fadd_rn(__fmul_rn(m00, m00), __fmul_rn(m10, m10));
+    const float p = __fmul_rn(m00, m11), q = __fmul_rn(m01, m10);
+    const float det = __fsub_rn(p, q);
+    if (!(a > 0.f) || !(a < 1e30f)) return 63u;
+    if (!(fabsf(det) > __fmul_rn(1e-3f, __fadd_rn(fabsf(p), fabsf(q))))) return 63u;
+    const float isx = __fmul_rn(0.5f, float(W)), isy = __fmul_rn(0.5f, float(H));
+    const float sa = __fsqrt_rn(a);
+    const float hw = __fdiv_rn(isx, sa);
+    const float ey = __fdiv_rn(sa, fabsf(det));
+    if (!(hw <= float(rx) + 1.f) || !(__fmul_rn(ey, isy) < 1e6f)) return 63u;
+    const int ky0 = int(ceilf(__fmul_rn(__fsub_rn(-ey, dy0), isy)));
+    const int ky1 = int(floorf(__fmul_rn(__fsub_rn(ey, dy0), isy)));
+    const int bw = int(floorf(__fmul_rn(2.f, hw))) + 2;
+    const int rows = max(min(ky1, kyb1) - max(ky0, kyb0) + 1, 0);
+    const int w = min(bw, kxb1 - kxb0 + 1);
+    return row_class(rows, w);
+}
+
+// delta = (2 p_c / w - 1) - x in double (separately rounded operations, in this order),
+// rounded once to float.
 __device__ __forceinline__ float corner_offset(int32_t p_c, int32_t W, float x) {
-    return float(double(p_c) * (2.0 / double(W)) - 1.0 - double(x));
+    return float(__dsub_rn(__dsub_rn(__dmul_rn(double(p_c), __ddiv_rn(2.0, double(W))), 1.0),
+                           double(x)));
 }
 
 // Predicated shared-memory add without a branch (the compiler otherwise branches around

@@ -24,33 +24,27 @@ struct PlanArgs {
     int32_t mpr;
     Cfg cfg;
     uint32_t key_big, key_invalid;  // bucket count (wide photons), and the untouched key
-    uint32_t* keys;      // [n] out: bucket of each photon, key_big or key_invalid
-    Rec* recs;           // [n] out (tile-path photons only)
-    uint32_t* counts;    // [key_big] photons per bucket; zeroed by the caller
-    uint32_t* inv;       // [n] out for wide (kWideBit | k) and untouched (kInvalidPos) photons
-    uint32_t* wide;      // [n] out: photon index of the k-th wide photon
+    uint32_t* counts;    // [key_big] photons per bucket; zeroed by the caller (count pass)
+    uint32_t* inv;       // [n] out: sorted position (place pass), kWideBit | k for wide and
+                         // kInvalidPos for untouched photons (count pass)
+    uint32_t* wide;      // [n] out: photon index of the k-th wide photon (count pass)
     uint32_t* counters;  // [0] tile-path, [1] wide, [2] untouched photons; zeroed by caller
+    uint32_t* cta_hist;  // [plan_hist_entries] each CTA's window histogram, count -> place
+    uint32_t* cursor;    // [key_big] place cursors (the bucket starts, from the scan)
+    Rec* srecs;          // [n] out: records in sorted order (place pass)
     int64_t range;       // photons per CTA (plan_shape)
     int32_t window;      // buckets of each CTA's shared histogram (plan_shape)
 };
 
-// Bucket scan and scatter of the plan.
-struct ScatterArgs {
-    SimTable sims;
-    const uint32_t* keys;
-    const Rec* recs;
+// Bucket scan and the chunks' tiles.
+struct ScanArgs {
     const uint32_t* counts;
     const uint32_t* counters;
     uint32_t* part;        // [bucket_scan_parts(nb)] scan partials
     uint32_t* start;       // [nb + 1] out: first sorted position of each bucket, then the total
-    uint32_t* cursor;      // [nb] scatter cursors
-    Rec* srecs;            // [n] out: records in sorted order
-    uint32_t* inv;         // [n] out for tile-path photons: sorted position
+    uint32_t* cursor;      // [nb] out: a copy of the starts for the place pass
     uint32_t* chunk_tile;  // [n / chunk + 1] out: tile of each work chunk's first photon
     int64_t n, nb, n_tiles;
-    int64_t range;         // photons per CTA and histogram window, as in the plan
-    int32_t window;
-    uint32_t key_big;
     int32_t chunk, cb;
 };
 
@@ -78,8 +72,14 @@ struct TileArgs {
 
 int64_t bucket_scan_parts(int64_t nb);
 void plan_shape(int64_t n, int64_t nb, int32_t* window, int64_t* range);
-cudaError_t launch_plan(const PlanArgs& a, cudaStream_t st);
-cudaError_t launch_bucket_sort(const ScatterArgs& a, cudaStream_t st);
+int64_t plan_hist_entries(int64_t n, int64_t nb);
+cudaError_t launch_plan_count(const PlanArgs& a, cudaStream_t st);
+cudaError_t launch_bucket_scan(const ScanArgs& a, cudaStream_t st);
+cudaError_t launch_plan_place(const PlanArgs& a, cudaStream_t st);
+cudaError_t launch_chunk_tiles(const ScanArgs& a, cudaStream_t st);
+cudaError_t launch_plan_export(const uint32_t* inv, const uint32_t* start, int64_t nb,
+                               uint32_t key_big, uint32_t key_invalid, int64_t n,
+                               uint32_t* bucket, uint32_t* slot, cudaStream_t st);
 cudaError_t launch_forward(const TileArgs& a, cudaStream_t st);
 cudaError_t launch_backward(const TileArgs& a, cudaStream_t st);
 

@@ -96,19 +96,25 @@ def jitter(H, W, scene, per_texel, generator, device):
 
 def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image=1024,
                 footprint_px=3.0, params=None, mask=None, seed=0, keep_plan=False, target=None,
-                log_every=0):
+                log_every=0, objective="l2_sq"):
     """The reference's pixel-basis Landweber loop (``shape_from_caustics.py:343-420``,
     default options) for a height-field plate, all on the device.
 
     Each iteration splats ``sims`` simulations of ``per_texel`` freshly jittered photons
     per texel into one image (the reference's sum over simulations, ``:351-353``), takes the
-    L2 discrepancy ``0.5 |I - T|^2 / |T|^2`` against the target, back-propagates to the
-    height-field offset through the splat and refraction kernels (refracted positions
-    recomputed, not stored) and applies the fused projected update. ``footprint_px`` sets the
-    photons' initial positional differentials to that many receiver pixels (the reference's
-    splat smoothing, ``model/caustics.py:60-61``). Returns a dict with the reconstructed
-    offset, the per-iteration discrepancy and height RMSE."""
+    data term against the target, back-propagates to the height-field offset through the splat
+    and refraction kernels (refracted positions recomputed, not stored) and applies the fused
+    projected update. ``objective``: ``"l2_sq"`` is the reference's data term
+    ``0.5 |I - T|^2`` (``hyperparameter_helper.py:29-30``, its default ``--data_norm``), for
+    which ``params.tau`` is the reference's ``tau_pixel``; ``"normalized"`` divides it by
+    ``|T|^2``. The logged discrepancy is the reference's ``sqrt(2 fdis) / |T|``
+    (``shape_from_caustics.py:363``) either way. ``footprint_px`` sets the photons' initial
+    positional differentials to that many receiver pixels (the reference's splat smoothing,
+    ``model/caustics.py:60-61``). Returns a dict with the reconstructed offset, the
+    per-iteration discrepancy and height RMSE."""
     from .plate import PlateSplat, plate_params
+    if objective not in ("l2_sq", "normalized"):
+        raise ValueError("objective must be 'l2_sq' or 'normalized'")
     dev = h_true.device
     H, W = h_true.shape
     n = H * W * per_texel * sims
@@ -122,27 +128,77 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
         px, py, offset = photon_source(H, W, per_texel * sims, scene.texel, seed, offset, dev)
         target = render_plate(h_true, scene, px, py, flux, pp, shape)
     tnorm2 = float((target * target).sum())
+    scale = 1.0 if objective == "l2_sq" else 1.0 / tnorm2
     if params is None:
         vol = float(d_true.sum())
         params = LandweberParams(d1=0.75 * vol, d2=1.25 * vol)
     if mask is None:
         mask = torch.ones_like(h_true)
     d = torch.zeros_like(h_true)
-    ws = None
+    ws = torch.empty(int(lib().pds_landweber_workspace_bytes(H, W)), dtype=torch.uint8, device=dev)
     hist = {"discrepancy": [], "rmse": []}
     for it in range(iterations):
         px, py, offset = photon_source(H, W, per_texel * sims, scene.texel, seed, offset, dev)
         hv = (base + d).requires_grad_(True)
         img = PlateSplat.apply(hv, px, py, flux, pp, shape, 20, keep_plan)
         diff = img - target
-        loss = 0.5 * (diff * diff).sum() / tnorm2
-        loss.backward()
-        if ws is None:
-            ws = torch.empty(int(lib().pds_landweber_workspace_bytes(H, W)), dtype=torch.uint8,
-                             device=dev)
+        fdis = 0.5 * (diff * diff).sum()
+        (fdis * scale).backward()
         landweber_update(d, hv.grad, mask, params, ws)
         if log_every and (it % log_every == 0 or it == iterations - 1):
-            hist["discrepancy"].append((it, float(loss.detach())))
+            hist["discrepancy"].append((it, float((2.0 * fdis.detach()).sqrt()) / tnorm2 ** 0.5))
             hist["rmse"].append((it, float(((d - d_true) ** 2).mean().sqrt())))
     rmse = float(((d - d_true) ** 2).mean().sqrt())
     return {"d": d, "rmse": rmse, "history": hist, "target": target, "photons_per_iteration": n}
+
+
+def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4, image=1024,
+                     footprint_px=3.0, seed=0, offset=0, objective="l2_sq", reps=3):
+    """CUDA-event times (ms, median of ``reps``) of the phases of one Landweber iteration of
+    ``reconstruct``, run phase by phase on the current stream: photon source, refraction
+    forward, plan, splat forward, data-term gradient, refraction recomputed for the backward,
+    splat backward, refraction backward, update. The height field is ``base + d``; ``d`` is
+    updated in place."""
+    import statistics
+    from .plate import plate_params, refract_backward, refract_forward
+    from .splatting import SplatPlan
+    dev = d.device
+    H, W = d.shape
+    n = H * W * per_texel * sims
+    pp = plate_params(scene, footprint_px * 2.0 * scene.receiver_half / image)
+    shape = (1, image, image)
+    flux = torch.full((n,), 1.0 / n, device=dev)
+    ws = torch.empty(int(lib().pds_landweber_workspace_bytes(H, W)), dtype=torch.uint8, device=dev)
+    scale = 1.0 if objective == "l2_sq" else 1.0 / float((target * target).sum())
+    names = ["source", "refract_fwd", "plan", "splat_fwd", "data_grad", "refract_fwd_again",
+             "splat_bwd", "refract_bwd", "update"]
+    times = {k: [] for k in names}
+    for r in range(reps + 1):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
+        ev[0].record()
+        px, py, offset = photon_source(H, W, per_texel * sims, scene.texel, seed, offset, dev)
+        ev[1].record()
+        hv = (base + d).contiguous()
+        Ep, xp, Mp, cp, radius = refract_forward(hv, px, py, flux, pp)
+        ev[2].record()
+        plan = SplatPlan(Ep, xp, Mp, cp, radius, shape, 20)
+        ev[3].record()
+        img = plan.forward()
+        ev[4].record()
+        g_img = ((img - target) * scale).contiguous()
+        ev[5].record()
+        Ep, xp, Mp, cp, radius = refract_forward(hv, px, py, flux, pp)
+        ev[6].record()
+        gE, gX, gM = plan.backward(g_img)
+        ev[7].record()
+        gh = refract_backward(hv, px, py, flux, pp, gE, gX, gM)
+        ev[8].record()
+        landweber_update(d, gh, mask, params, ws)
+        ev[9].record()
+        torch.cuda.synchronize()
+        if r > 0:
+            for k, name in enumerate(names):
+                times[name].append(ev[k].elapsed_time(ev[k + 1]))
+    out = {k: statistics.median(v) for k, v in times.items()}
+    out["total"] = sum(out.values())
+    return out
