@@ -3,12 +3,13 @@ workloads.
 
 ``PlateScene`` holds the plate's geometry and the light (the quantities ``pds_plate`` carries
 to the refraction kernels, ``plate.plate_params``); ``height_field_bumps`` draws the seeded
-height fields of the Landweber workloads (a base thickness plus Gaussian bumps). Units:
-millimetres.
+height fields of the Landweber workloads (a base thickness plus Gaussian bumps);
+``fused_silica`` is the glass's dispersion (refractive index per wavelength). Units:
+millimetres, wavelengths in micrometres.
 """
 import torch
 
-__all__ = ["PlateScene", "height_field_bumps"]
+__all__ = ["PlateScene", "height_field_bumps", "fused_silica"]
 
 
 class PlateScene:
@@ -46,3 +47,16 @@ def height_field_bumps(H, W, seed=0, bumps=32, base=1.0, amp=(0.0, 0.05), width=
     for k in range(bumps):
         h += a[k] * torch.exp(-((yy - cy[k]) ** 2 + (xx - cx[k]) ** 2) / (2 * w[k] ** 2))
     return h.to(dtype=dtype, device=device)
+
+
+def fused_silica(wavelength_um):
+    """Refractive index of fused silica at a wavelength in micrometres: the three-term Sellmeier
+    fit the reference uses (``model/caustics.py:13-23``, fitted on 0.21-6.7 um),
+    ``n^2 = 1 + sum_k B_k / (1 - (C_k / lambda)^2)`` with B = (0.6961663, 0.4079426,
+    0.8974794) and C = (0.0684043, 0.1162414, 9.896161) um. Scalars or tensors."""
+    lam = wavelength_um
+    terms = ((0.6961663, 0.0684043), (0.4079426, 0.1162414), (0.8974794, 9.896161))
+    n2 = 1.0
+    for b, c in terms:
+        n2 = n2 + b / (1.0 - (c / lam) ** 2)
+    return n2 ** 0.5

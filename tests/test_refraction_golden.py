@@ -95,3 +95,15 @@ def test_plate_chain_equals_the_reference_functions_composed():
     assert rel(Ep, GOLD["chain_Ep"]) < 1e-10
     assert rel(Mp, GOLD["chain_Mp"]) < 1e-10
     assert rel(radius, GOLD["chain_radius"]) < 1e-10
+
+
+def test_fused_silica_dispersion_equals_the_reference():
+    from shapefromcaustics_b200.scene import fused_silica
+    lam = GOLD["silica_lambda_um"]
+    n = np.array([fused_silica(float(v)) for v in lam])
+    assert rel(n, GOLD["silica_n"]) < 1e-15
+    # over the visible range the index falls from about 1.470 to 1.456
+    assert 1.45 < n.min() < n.max() < 1.48 and np.all(np.diff(n) < 0)
+    # tensors too
+    nt = fused_silica(torch.from_numpy(lam))
+    assert rel(nt.numpy(), GOLD["silica_n"]) < 1e-15
