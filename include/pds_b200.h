@@ -221,6 +221,35 @@ int pds_refract_backward_f32(const float* height, int32_t rows, int32_t cols,
 int pds_photon_source_f32(int32_t rows, int32_t cols, int32_t per_texel, float texel,
                           uint64_t seed, uint64_t offset, float* px, float* py, void* stream);
 
+/* A point light whose photons spread over a rectangle of the plane z = plane_z
+ * (model/caustics.py:26-70, compute_point_light_dirs; the rectangle is the height field's
+ * extent, the plane its base height). */
+typedef struct pds_point_light {
+    float position[3];                /* light position */
+    float plane_z;                    /* plane the directions are spread over */
+    float xmin, ymin, xmax, ymax;     /* the rectangle on that plane */
+    float smoothing;                  /* splat smoothing (scales the direction differentials) */
+    float energy;                     /* light energy; each photon carries
+                                         energy / (simulations * inner) */
+    int32_t simulations;              /* simulations whose photons share the light's energy */
+    int32_t inner;                    /* inner simulations per simulation */
+    int32_t wavelengths;              /* photons per direction, one per wavelength */
+} pds_point_light;
+
+/* Photon directions and direction differentials of a point light (model/caustics.py:26-70):
+ * direction k is the bilinear slerp of the rectangle's corner directions by two uniform
+ * numbers (u0, u1); its differentials are the Frisvad orthonormal basis of the direction
+ * (model/utils.py compute_orthonormal_basis) scaled by 2 smoothing sqrt(omega / (pi N)), with
+ * omega the rectangle's solid angle seen from the light (model/utils.py subtended_angle,
+ * computed on the device: no host read-back) and N = n_directions * simulations * wavelengths.
+ * Each direction is repeated for each wavelength (photon k * wavelengths + w). The uniform
+ * numbers are coeffs[0][k], coeffs[1][k] when coeffs is not NULL, else Philox4x32-10 keyed by
+ * seed (directions 2j and 2j + 1 use counter block offset + j). Outputs: direction[3][n],
+ * dtheta[3][n], dphi[3][n], flux[n] with n = n_directions * wavelengths. */
+int pds_point_light_source_f32(const pds_point_light* light, int64_t n_directions, uint64_t seed,
+                               uint64_t offset, const float* coeffs, float* direction,
+                               float* dtheta, float* dphi, float* flux, void* stream);
+
 /* ---- projected Landweber update of the height field ------------------------------- */
 /* One update of the reference's pixel-basis Landweber loop (shape_from_caustics.py:386-398):
  * d <- VconsHeur(mask * extShrink(d - tau * grad, shrink, lower, upper)), with extShrink

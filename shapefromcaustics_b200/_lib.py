@@ -43,6 +43,15 @@ class PdsPlate(ctypes.Structure):
                 ("receiver_distance", ctypes.c_float), ("receiver_half", ctypes.c_float),
                 ("light_dir", ctypes.c_float * 3), ("du0", ctypes.c_float)]
 
+class PdsPointLight(ctypes.Structure):
+    """Mirror of ``pds_point_light``."""
+    _fields_ = [("position", ctypes.c_float * 3), ("plane_z", ctypes.c_float),
+                ("xmin", ctypes.c_float), ("ymin", ctypes.c_float), ("xmax", ctypes.c_float),
+                ("ymax", ctypes.c_float), ("smoothing", ctypes.c_float),
+                ("energy", ctypes.c_float), ("simulations", ctypes.c_int32),
+                ("inner", ctypes.c_int32), ("wavelengths", ctypes.c_int32)]
+
+
 class PdsLandweber(ctypes.Structure):
     """Mirror of ``pds_landweber``."""
     _fields_ = [("tau", ctypes.c_float), ("shrink", ctypes.c_float), ("lower", ctypes.c_float),
@@ -86,6 +95,9 @@ SIGNATURES = {
                                                 _P, _I64, _P, _P, _P, _P, _P]),
     "pds_photon_source_f32": (ctypes.c_int, [_I32, _I32, _I32, ctypes.c_float, ctypes.c_uint64,
                                              ctypes.c_uint64, _P, _P, _P]),
+    "pds_point_light_source_f32": (ctypes.c_int, [ctypes.POINTER(PdsPointLight), _I64,
+                                                   ctypes.c_uint64, ctypes.c_uint64, _P, _P, _P,
+                                                   _P, _P, _P]),
     "pds_landweber_workspace_bytes": (_SZ, [_I64, _I64]),
     "pds_landweber_update_f32": (ctypes.c_int, [_P, _P, _P, _I64, _I64,
                                                 ctypes.POINTER(PdsLandweber), _P, _SZ, _P]),

@@ -565,6 +565,26 @@ int pds_photon_source_f32(int32_t rows, int32_t cols, int32_t per_texel, float t
     return PDS_OK;
 }
 
+int pds_point_light_source_f32(const pds_point_light* light, int64_t n_dir, uint64_t seed,
+                               uint64_t offset, const float* coeffs, float* direction,
+                               float* dtheta, float* dphi, float* flux, void* stream) {
+    if (!light) return fail(PDS_ERR_INVALID_ARGUMENT, "null light");
+    if (n_dir < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative direction count");
+    if (light->simulations < 1 || light->inner < 1 || light->wavelengths < 1)
+        return fail(PDS_ERR_INVALID_ARGUMENT,
+                    "simulations, inner and wavelengths must be positive");
+    if (!(light->xmax > light->xmin) || !(light->ymax > light->ymin))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "empty light rectangle");
+    if (n_dir * int64_t(light->wavelengths) >= int64_t(0x7FFFFFFFll))
+        return fail(PDS_ERR_UNSUPPORTED, "photon count must be below 2^31 - 1");
+    if (n_dir > 0 && (!direction || !dtheta || !dphi || !flux))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
+    cudaError_t e = pds::launch_point_light(*light, n_dir, seed, offset, coeffs, direction, dtheta,
+                                            dphi, flux, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "point_light_kernel");
+    return PDS_OK;
+}
+
 size_t pds_landweber_workspace_bytes(int64_t rows, int64_t cols) {
     return pds::landweber_scratch_bytes(rows * cols);
 }

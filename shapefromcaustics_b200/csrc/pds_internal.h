@@ -31,6 +31,10 @@ cudaError_t launch_source(int32_t rows, int32_t cols, int32_t per_texel, float t
                           uint64_t seed, uint64_t offset, int64_t n, float* px, float* py,
                           cudaStream_t st);
 
+cudaError_t launch_point_light(const pds_point_light& L, int64_t n_dir, uint64_t seed,
+                               uint64_t offset, const float* coeffs, float* dir, float* dth,
+                               float* dph, float* flux, cudaStream_t st);
+
 // Landweber update (pds_landweber.cu)
 size_t landweber_scratch_bytes(int64_t n);
 cudaError_t launch_landweber(float* d, const float* g, const float* mask, int64_t rows,

@@ -63,7 +63,128 @@ __global__ __launch_bounds__(256) void source_kernel(int32_t rows, int32_t cols,
     }
 }
 
+// ---- point light -----------------------------------------------------------------------
+// Directions of a point light spread over a rectangle of the plane z = plane_z by a bilinear
+// slerp (model/caustics.py:26-70, compute_point_light_dirs): with the corner directions
+// c_ab = normalize(corner_ab - light) (a: x min/max, b: y min/max), a photon's direction is
+// slerp(slerp(c_00, c_10, u0), slerp(c_01, c_11, u0), u1) for its two uniform numbers
+// (u0, u1); its direction differentials are the Frisvad (2012) orthonormal basis of that
+// direction (model/utils.py, compute_orthonormal_basis), scaled by
+// 2 smoothing sqrt(omega / (pi N)) with omega the rectangle's solid angle seen from the light
+// (two triangles, Van Oosterom-Strackee, model/utils.py subtended_angle) and N the photon count
+// of all simulations and wavelengths. The reference computes omega on the device and reads it
+// back (sbt_angle.item(), caustics.py:60); here every thread computes it from the light's
+// parameters, so nothing waits on the host.
+
+struct V3f {
+    float x, y, z;
+};
+__device__ __forceinline__ V3f v3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ float dot3(V3f a, V3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3f cross3(V3f a, V3f b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ V3f scale3(float s, V3f a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ V3f add3(V3f a, V3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3f sub3(V3f a, V3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ float norm3(V3f a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ V3f unit3(V3f a) {
+    const float n = norm3(a);
+    return n > 0.f ? scale3(1.f / n, a) : a;
+}
+
+// slerp(p0, p1, t) = (sin((1 - t) w) p0 + sin(t w) p1) / sin(w), w = acos(clamp(p0.p1))
+__device__ __forceinline__ V3f slerp3(V3f p0, V3f p1, float t) {
+    const float w = acosf(fminf(fmaxf(dot3(p0, p1), -1.f), 1.f));
+    const float s = sinf(w);
+    return scale3(1.f / s, add3(scale3(sinf((1.f - t) * w), p0), scale3(sinf(t * w), p1)));
+}
+
+// Solid angle of triangle (v0, v1, v2) seen from o: 2 atan2(d0.(d2 x d1), |d0||d1||d2| +
+// |d0| d1.d2 + |d1| d0.d2 + |d2| d0.d1), negative values counted as zero (as the reference
+// sums relu of the per-triangle angles).
+__device__ __forceinline__ float tri_angle(V3f o, V3f v0, V3f v1, V3f v2) {
+    const V3f d0 = sub3(v0, o), d1 = sub3(v1, o), d2 = sub3(v2, o);
+    const float n0 = norm3(d0), n1 = norm3(d1), n2 = norm3(d2);
+    const float num = dot3(d0, cross3(d2, d1));
+    const float den = n0 * n1 * n2 + n0 * dot3(d1, d2) + n1 * dot3(d0, d2) + n2 * dot3(d0, d1);
+    const float a = (num == 0.f && den == 0.f) ? 0.f : 2.f * atan2f(num, den);
+    return fmaxf(a, 0.f);
+}
+
+__global__ __launch_bounds__(256) void point_light_kernel(pds_point_light L, int64_t n_dir,
+                                                          uint64_t seed, uint64_t offset,
+                                                          const float* __restrict__ coeffs,
+                                                          float* __restrict__ dir,
+                                                          float* __restrict__ dth,
+                                                          float* __restrict__ dph,
+                                                          float* __restrict__ flux) {
+    const V3f o = v3(L.position[0], L.position[1], L.position[2]);
+    const V3f p00 = v3(L.xmin, L.ymin, L.plane_z), p10 = v3(L.xmax, L.ymin, L.plane_z);
+    const V3f p01 = v3(L.xmin, L.ymax, L.plane_z), p11 = v3(L.xmax, L.ymax, L.plane_z);
+    const V3f c00 = unit3(sub3(p00, o)), c10 = unit3(sub3(p10, o));
+    const V3f c01 = unit3(sub3(p01, o)), c11 = unit3(sub3(p11, o));
+    const float omega = tri_angle(o, p00, p10, p01) + tri_angle(o, p01, p10, p11);
+    const int wl = L.wavelengths;
+    const double total = double(n_dir) * double(L.simulations) * double(wl);
+    const float scale = float(2.0 * double(L.smoothing) *
+                              sqrt(double(omega) / (3.141592653589793 * total)));
+    const float f = L.energy / float(int64_t(L.simulations) * L.inner);
+    const int64_t n = n_dir * wl;
+    const int64_t pairs = (n_dir + 1) >> 1;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < pairs;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        uint4 r = make_uint4(0u, 0u, 0u, 0u);
+        if (!coeffs) {
+            const uint64_t ctr = offset + uint64_t(k);
+            r = philox4x32_10(make_uint4(uint32_t(ctr), uint32_t(ctr >> 32), 0u, 0u),
+                              uint32_t(seed), uint32_t(seed >> 32));
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t i = 2 * k + h;
+            if (i >= n_dir) break;
+            const float u0 = coeffs ? coeffs[i] : unit24(h ? r.z : r.x);
+            const float u1 = coeffs ? coeffs[n_dir + i] : unit24(h ? r.w : r.y);
+            const V3f lower = slerp3(c00, c10, u0), upper = slerp3(c01, c11, u0);
+            const V3f d = slerp3(lower, upper, u1);
+            V3f b1, b2;
+            if (d.z < -1.f + 1e-5f) {
+                b1 = v3(0.f, -1.f, 0.f);
+                b2 = v3(-1.f, 0.f, 0.f);
+            } else {
+                const float a = 1.f / (1.f + d.z);
+                const float b = -d.x * d.y * a;
+                b1 = v3(1.f - a * d.x * d.x, b, -d.x);
+                b2 = v3(b, 1.f - a * d.y * d.y, -d.y);
+            }
+            for (int w = 0; w < wl; ++w) {
+                const int64_t j = i * wl + w;
+                dir[j] = d.x; dir[n + j] = d.y; dir[2 * n + j] = d.z;
+                dth[j] = scale * b1.x; dth[n + j] = scale * b1.y; dth[2 * n + j] = scale * b1.z;
+                dph[j] = scale * b2.x; dph[n + j] = scale * b2.y; dph[2 * n + j] = scale * b2.z;
+                flux[j] = f;
+            }
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_point_light(const pds_point_light& L, int64_t n_dir, uint64_t seed,
+                               uint64_t offset, const float* coeffs, float* dir, float* dth,
+                               float* dph, float* flux, cudaStream_t st) {
+    if (n_dir <= 0) return cudaSuccess;
+    const int64_t pairs = (n_dir + 1) / 2;
+    const int64_t blocks = (pairs + 255) / 256;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t cap = int64_t(sms) * 16;
+    point_light_kernel<<<unsigned(blocks < cap ? blocks : cap), 256, 0, st>>>(
+        L, n_dir, seed, offset, coeffs, dir, dth, dph, flux);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_source(int32_t rows, int32_t cols, int32_t per_texel, float texel,
                           uint64_t seed, uint64_t offset, int64_t n, float* px, float* py,

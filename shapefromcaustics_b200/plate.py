@@ -21,7 +21,8 @@ from . import _lib
 from ._lib import check, lib
 from .splatting import SplatPlan, _ptr, _stream
 
-__all__ = ["PlateParams", "plate_params", "refract_forward", "refract_backward", "PlateSplat"]
+__all__ = ["PlateParams", "plate_params", "refract_forward", "refract_backward", "PlateSplat",
+           "PointLight", "point_light", "point_light_source"]
 
 
 PlateParams = _lib.PdsPlate
@@ -118,3 +119,45 @@ class PlateSplat(torch.autograd.Function):
         gh = refract_backward(h, px, py, flux, ctx.params, gE, gX, gM)
         ctx.plan_ws = None
         return gh, None, None, None, None, None, None, None
+
+
+PointLight = _lib.PdsPointLight
+
+
+def point_light(position, rect, plane_z, smoothing, energy, simulations=1, inner=1,
+                wavelengths=1):
+    """``pds_point_light`` of a light at ``position`` whose photons spread over
+    ``rect = (xmin, ymin, xmax, ymax)`` on the plane ``z = plane_z`` (the reference's
+    ``compute_point_light_dirs`` arguments: smoothing, energy, num_simul, num_inner_simul and
+    the number of wavelengths)."""
+    L = PointLight()
+    for k in range(3):
+        L.position[k] = float(position[k])
+    L.plane_z = float(plane_z)
+    L.xmin, L.ymin, L.xmax, L.ymax = (float(v) for v in rect)
+    L.smoothing = float(smoothing)
+    L.energy = float(energy)
+    L.simulations = int(simulations)
+    L.inner = int(inner)
+    L.wavelengths = int(wavelengths)
+    return L
+
+
+def point_light_source(light, n_directions, device, seed=0, offset=0, coeffs=None):
+    """Photon directions of a point light on the device (``pds_point_light_source_f32``):
+    ``(direction [3, n], dtheta [3, n], dphi [3, n], flux [n], next_offset)`` with
+    ``n = n_directions * light.wavelengths``. The two uniform numbers of each direction come
+    from ``coeffs [2, n_directions]`` (float32, device) when given, else from the Philox
+    source keyed by ``seed`` at counter ``offset``; ``next_offset`` draws a disjoint stream."""
+    n = int(n_directions) * int(light.wavelengths)
+    dev = torch.device(device)
+    out = [torch.empty((3, n), device=dev) for _ in range(3)] + [torch.empty(n, device=dev)]
+    if coeffs is not None:
+        _check_f32(coeffs, "coeffs")
+        if tuple(coeffs.shape) != (2, int(n_directions)):
+            raise RuntimeError("coeffs must be [2, n_directions]")
+    with torch.cuda.device(dev):
+        check(_fn("pds_point_light_source_f32")(
+            ctypes.byref(light), int(n_directions), int(seed) & (2 ** 64 - 1), int(offset),
+            _ptr(coeffs) if coeffs is not None else None, *(_ptr(t) for t in out), _stream(dev)))
+    return (*out, int(offset) + (int(n_directions) + 1) // 2)

@@ -185,3 +185,37 @@ def test_config2_gpu_gradient_matches_fp64_central_differences(cuda):
     assert smooth.all() and skipped < 64
     err = np.linalg.norm(fd - an) / np.linalg.norm(fd)
     assert err < 1e-3, (err, fd, an)
+
+
+def test_point_light_source_matches_compute_point_light_dirs(cuda):
+    """pds_point_light_source_f32 with the reference's own uniform numbers reproduces the
+    reference's compute_point_light_dirs (tests/golden/refraction_ref.npz; float32 kernel,
+    float64 fixture), and with its Philox numbers the FP64 restatement."""
+    import os
+    from oracle import point_light as PLR
+    from shapefromcaustics_b200 import plate as PL
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                "refraction_ref.npz"))
+    coords = gold["plight_coords"]
+    z, _, sims, inner, smooth, energy = (float(v) for v in gold["plight_params"])
+    rect = (coords[0].min(), coords[1].min(), coords[0].max(), coords[1].max())
+    light = PL.point_light(gold["plight_light"], rect, z, smooth, energy, int(sims), int(inner))
+    coeffs = torch.from_numpy(gold["plight_coeffs"].reshape(2, -1)).float().cuda()
+    d, dt, dp, flux, _ = PL.point_light_source(light, coeffs.shape[1], "cuda", coeffs=coeffs)
+    torch.cuda.synchronize()
+    assert rel_l2(d.cpu().numpy().T, gold["plight_direction"]) < 1e-6
+    assert rel_l2(dt.cpu().numpy().T, gold["plight_Dtheta"]) < 1e-5
+    assert rel_l2(dp.cpu().numpy().T, gold["plight_Dphi"]) < 1e-5
+    assert rel_l2(flux.cpu().numpy(), gold["plight_flux"]) < 1e-6
+    # Philox numbers, three wavelengths per direction, against the restatement
+    light3 = PL.point_light((0.3, -0.1, 12.0), (-2.0, -1.5, 2.0, 1.5), 1.0, 4.0, 1e-4, 16, 32, 3)
+    n_dir = 5001
+    d, dt, dp, flux, nxt = PL.point_light_source(light3, n_dir, "cuda", seed=77, offset=5)
+    torch.cuda.synchronize()
+    u0, u1 = PLR.philox_coeffs(n_dir, 77, 5)
+    rd, rt, rp, rf = PLR.point_light((0.3, -0.1, 12.0), (-2.0, -1.5, 2.0, 1.5), 1.0, u0, u1, 4.0,
+                                     1e-4, 16, 32, 3)
+    assert nxt == 5 + (n_dir + 1) // 2 and d.shape == (3, 3 * n_dir)
+    assert rel_l2(d.cpu().numpy().T, rd) < 1e-6
+    assert rel_l2(dt.cpu().numpy().T, rt) < 1e-5
+    assert rel_l2(flux.cpu().numpy(), rf) < 1e-6

@@ -107,3 +107,26 @@ def test_fused_silica_dispersion_equals_the_reference():
     # tensors too
     nt = fused_silica(torch.from_numpy(lam))
     assert rel(nt.numpy(), GOLD["silica_n"]) < 1e-15
+
+
+def point_light_case():
+    coords = GOLD["plight_coords"]
+    plane_z, nwl, sims, inner, smooth, energy = (float(v) for v in GOLD["plight_params"])
+    rect = (coords[0].min(), coords[1].min(), coords[0].max(), coords[1].max())
+    coeffs = GOLD["plight_coeffs"].reshape(2, -1)
+    return GOLD["plight_light"], rect, plane_z, coeffs, smooth, energy, int(sims), int(inner)
+
+
+def test_point_light_restatement_equals_compute_point_light_dirs():
+    from oracle import point_light as PLR
+    light, rect, z, coeffs, smooth, energy, sims, inner = point_light_case()
+    d, dt, dp, flux = PLR.point_light(light, rect, z, coeffs[0], coeffs[1], smooth, energy, sims,
+                                      inner)
+    assert rel(d, GOLD["plight_direction"]) < TOL
+    assert rel(dt, GOLD["plight_Dtheta"]) < TOL
+    assert rel(dp, GOLD["plight_Dphi"]) < TOL
+    assert rel(flux, GOLD["plight_flux"]) < TOL
+    # the helpers on their own
+    assert rel(PLR.slerp(GOLD["slerp_p0"], GOLD["slerp_p1"], GOLD["slerp_t"]), GOLD["slerp_out"]) < TOL
+    b1, b2 = PLR.onb(GOLD["onb_n"].T)
+    assert rel(b1.T, GOLD["onb_b1"]) < TOL and rel(b2.T, GOLD["onb_b2"]) < TOL
