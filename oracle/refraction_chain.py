@@ -253,3 +253,81 @@ def receiver_splat_inputs(h, scene, photons, channel=None):
         channel = torch.zeros(px.shape[0], dtype=torch.int64, device=px.device)
     Ep, Mp, cp, radius = splat_inputs(Du, Dv, nrm, flux, channel)
     return Ep, xy.contiguous(), Mp, cp, radius
+
+
+def trace_height_field(h, scene, origin, d, plane_z, iterations=12):
+    """Ray parameter t of the first hit of rays ``origin + t d`` (``origin [3]``, ``d [3, N]``
+    unit, pointing down) with the bilinear height-field surface ``z = h(x, y)``: Newton steps on
+    ``f(t) = o_z + t d_z - h(o_xy + t d_xy)`` from the plane ``z = plane_z`` (the height field is
+    assumed to have no overhangs and no occluding bump before the hit, as the reference's
+    ``generate_from_point_light`` assumes for its samples). Differentiable in ``h``: at the
+    converged root the Newton map's derivative is the implicit one, ``dt/dh = w / f'(t)``.
+    -> (t [N], inside [N] bool: the hit lies over the field)."""
+    H, W = h.shape
+    o = torch.as_tensor(origin, dtype=h.dtype, device=h.device)[:, None]
+    t = (o[2] - plane_z) / (-d[2])
+    for _ in range(iterations):
+        p = o + t * d
+        fx = p[0] / scene.texel + (W - 1) / 2.0
+        fy = p[1] / scene.texel + (H - 1) / 2.0
+        hv, hdx, hdy = _bilinear(h[None], fx, fy)
+        f = p[2] - hv[0]
+        fp = d[2] - (hdx[0] * d[0] + hdy[0] * d[1]) / scene.texel
+        t = t - f / fp
+    p = o + t * d
+    fx = p[0] / scene.texel + (W - 1) / 2.0
+    fy = p[1] / scene.texel + (H - 1) / 2.0
+    inside = (fx >= 0) & (fx <= W - 1) & (fy >= 0) & (fy <= H - 1)
+    return t, inside
+
+
+def trace_point_light_to_receiver(h, scene, origin, d, Dth, Dph, plane_z):
+    """Receiver position (normalised, ``[2, N]``) and receiver-plane differentials ``[3, N]``
+    of point-light photons (``origin``, unit directions ``d [3, N]``, direction differentials
+    ``Dth, Dph [3, N]``): the traced hit on the height field, the positional differentials
+    carried from the light to the hit (``model/photon_differential.py:69-78`` with ``Du = Dv =
+    0`` at the light), refraction into the glass with the direction differentials, the flat
+    bottom face and the receiver plane as in ``trace_to_receiver``. -> (xy, Du, Dv, inside)."""
+    dt = h.dtype
+    n_ph = d.shape[1]
+    zero = torch.zeros((3, n_ph), dtype=dt, device=h.device)
+    t, inside = trace_height_field(h, scene, origin, d, plane_z)
+    o = torch.as_tensor(origin, dtype=dt, device=h.device)[:, None]
+    p1 = o + t * d
+    _, Nt, Ntx, Nty = sample_surface(h, scene, p1[0], p1[1])
+    Ntn = Nt / torch.sqrt(_dot(Nt, Nt))
+    Du1 = transfer(zero, Dth, t, Ntn, d)
+    Dv1 = transfer(zero, Dph, t, Ntn, d)
+    dNu = Ntx * Du1[0] + Nty * Du1[1]
+    dNv = Ntx * Dv1[0] + Nty * Dv1[1]
+    n, dnu = _unit_normal_and_derivative(Nt, dNu)
+    _, dnv = _unit_normal_and_derivative(Nt, dNv)
+    t1, Ddu = _refract(d, n, Dth, dnu, 1.0 / scene.ior)
+    _, Ddv = _refract(d, n, Dph, dnv, 1.0 / scene.ior)
+    s1 = -p1[2] / t1[2]
+    p2 = p1 + s1 * t1
+    nz = torch.zeros_like(zero)
+    nz[2] = 1.0
+    Du2 = transfer(Du1, Ddu, s1, nz, t1)
+    Dv2 = transfer(Dv1, Ddv, s1, nz, t1)
+    t2, Ddu2 = _refract(t1, nz, Ddu, zero, scene.ior)
+    _, Ddv2 = _refract(t1, nz, Ddv, zero, scene.ior)
+    s2 = (-scene.receiver_distance - p2[2]) / t2[2]
+    p3 = p2 + s2 * t2
+    Du3 = transfer(Du2, Ddu2, s2, nz, t2)
+    Dv3 = transfer(Dv2, Ddv2, s2, nz, t2)
+    inv = 1.0 / scene.receiver_half
+    return p3[:2] * inv, Du3 * inv, Dv3 * inv, inside
+
+
+def point_light_splat_inputs(h, scene, origin, d, Dth, Dph, flux, plane_z, channel=None):
+    """Splat inputs ``(Ep, xp, Mp, cp, radius)`` of point-light photons; photons whose hit
+    misses the field get channel -1."""
+    xy, Du, Dv, inside = trace_point_light_to_receiver(h, scene, origin, d, Dth, Dph, plane_z)
+    nrm = torch.zeros_like(Du)
+    nrm[2] = 1.0
+    if channel is None:
+        channel = torch.zeros(d.shape[1], dtype=torch.int64, device=d.device)
+    channel = torch.where(inside, channel, torch.full_like(channel, -1))
+    Ep, Mp, cp, radius = splat_inputs(Du, Dv, nrm, flux, channel)
+    return Ep, xy.contiguous(), Mp, cp, radius

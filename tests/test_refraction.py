@@ -104,3 +104,69 @@ def test_config2_gradient_matches_central_differences_on_64_texels():
     fd, smooth = PF.fd_gradient(h, target, scene, photons, texels)
     assert smooth.all() and skipped < 64
     assert np.linalg.norm(fd - an) / np.linalg.norm(an) < 1e-4, (fd, an)
+
+
+def point_light_setup(n=24, img=48, n_dir=4000, seed=4):
+    from oracle import point_light as PLR
+    scene = RF.PlateScene(texel=0.4, receiver_distance=30.0, receiver_half=7.0)
+    h = RF.height_field_bumps(n, n, seed=seed, bumps=6, amp=(0.0, 0.05), width=(2.0, 5.0))
+    half = 0.5 * (n - 1) * scene.texel
+    rect = (-half + 0.3, -half + 0.3, half - 0.3, half - 0.3)
+    light = (0.4, -0.3, 40.0)
+    g = np.random.default_rng(seed)
+    u0, u1 = g.random(n_dir), g.random(n_dir)
+    d, dt, dp, flux = PLR.point_light(light, rect, 1.0, u0, u1, 6.0, 1.0, 1, 1)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a.T))  # noqa: E731
+    return scene, h, light, (T(d), T(dt), T(dp), torch.from_numpy(flux)), (1, img, img)
+
+
+def test_point_light_trace_hits_the_surface():
+    scene, h, light, (d, dt, dp, flux), shape = point_light_setup()
+    t, inside = RF.trace_height_field(h, scene, light, d, 1.0)
+    p = torch.tensor(light, dtype=torch.float64)[:, None] + t * d
+    H, W = h.shape
+    fx = p[0] / scene.texel + (W - 1) / 2.0
+    fy = p[1] / scene.texel + (H - 1) / 2.0
+    hv, _, _ = RF._bilinear(h[None], fx, fy)
+    assert bool(inside.all())
+    assert float((p[2] - hv[0]).abs().max()) < 1e-12
+
+
+def test_point_light_height_gradient_matches_central_differences():
+    scene, h, light, (d, dt, dp, flux), shape = point_light_setup()
+
+    def render_pl(hh):
+        Ep, xp, Mp, cp, radius = RF.point_light_splat_inputs(hh, scene, light, d, dt, dp, flux,
+                                                             1.0)
+        return OraclePDS.apply(Ep, xp, Mp, cp, radius, shape, 20)
+
+    t2 = RF.height_field_bumps(24, 24, seed=9, bumps=6, amp=(0.0, 0.05), width=(2.0, 5.0))
+    target = render_pl(t2).detach()
+    hv = h.clone().requires_grad_(True)
+    loss = 0.5 * ((render_pl(hv) - target) ** 2).sum()
+    loss.backward()
+    grad = hv.grad.detach()
+    rng = np.random.default_rng(1)
+    eps = 1e-7
+
+    def L(hh):
+        with torch.no_grad():
+            return float(0.5 * ((render_pl(hh) - target) ** 2).sum())
+
+    def boxes(hh):
+        with torch.no_grad():
+            Ep, xp, Mp, cp, radius = RF.point_light_splat_inputs(hh, scene, light, d, dt, dp,
+                                                                 flux, 1.0)
+        return O.footprints(xp.numpy(), cp.numpy(), radius.numpy(), shape, 20)[0]
+
+    fd, an = [], []
+    while len(fd) < 12:
+        i, j = (int(v) for v in rng.integers(3, 21, 2))
+        hp = h.clone(); hp[i, j] += eps
+        hm = h.clone(); hm[i, j] -= eps
+        if not np.array_equal(boxes(hp), boxes(hm)):
+            continue  # a truncation box moves: the difference quotient measures a jump
+        fd.append((L(hp) - L(hm)) / (2 * eps))
+        an.append(float(grad[i, j]))
+    fd, an = np.array(fd), np.array(an)
+    assert np.linalg.norm(fd - an) / np.linalg.norm(an) < 1e-4, (fd, an)
