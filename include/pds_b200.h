@@ -250,6 +250,31 @@ int pds_point_light_source_f32(const pds_point_light* light, int64_t n_direction
                                uint64_t offset, const float* coeffs, float* direction,
                                float* dtheta, float* dphi, float* flux, void* stream);
 
+/* Splat inputs of n point-light photons (direction[3][n], dtheta[3][n], dphi[3][n], flux[n],
+ * e.g. from pds_point_light_source_f32; channel[n] or NULL for 0) on the plate: each photon's
+ * first hit with the bilinear height-field surface is traced from the light (Newton steps from
+ * the plane z = light->plane_z; the reference traces with OptiX, PyOptix/RayTrace.cpp:233-291,
+ * on the plate's mesh), its positional differentials are carried from the light to the hit
+ * (model/photon_differential.py:69-78, zero at the light), and the chain continues as in
+ * pds_refract_forward_f32 with the photon's direction differentials. plate->light_dir and
+ * plate->du0 are not used. Photons whose hit lies outside the field get channel -1. */
+int pds_refract_point_forward_f32(const float* height, int32_t rows, int32_t cols,
+                                  const pds_plate* plate, const pds_point_light* light,
+                                  const float* direction, const float* dtheta, const float* dphi,
+                                  const float* flux, const int64_t* channel, int64_t n_photons,
+                                  float* Ep, float* xp, float* Mp, int64_t* cp, float* radius,
+                                  void* stream);
+
+/* Adds d L / d height for point-light photons given their splat-input gradients; the trace and
+ * the chain are recomputed (nothing from the forward is needed), and the hit's dependence on
+ * the heights (dt/dh = w / f'(t) for the hit cell's bilinear weights w) is included. */
+int pds_refract_point_backward_f32(const float* height, int32_t rows, int32_t cols,
+                                   const pds_plate* plate, const pds_point_light* light,
+                                   const float* direction, const float* dtheta,
+                                   const float* dphi, const float* flux, int64_t n_photons,
+                                   const float* grad_Ep, const float* grad_xp,
+                                   const float* grad_Mp, float* grad_height, void* stream);
+
 /* ---- projected Landweber update of the height field ------------------------------- */
 /* One update of the reference's pixel-basis Landweber loop (shape_from_caustics.py:386-398):
  * d <- VconsHeur(mask * extShrink(d - tau * grad, shrink, lower, upper)), with extShrink

@@ -93,6 +93,12 @@ SIGNATURES = {
                                                _P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "pds_refract_backward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate), _P, _P,
                                                 _P, _I64, _P, _P, _P, _P, _P]),
+    "pds_refract_point_forward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate),
+                                                     ctypes.POINTER(PdsPointLight), _P, _P, _P,
+                                                     _P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    "pds_refract_point_backward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate),
+                                                      ctypes.POINTER(PdsPointLight), _P, _P, _P,
+                                                      _P, _I64, _P, _P, _P, _P, _P]),
     "pds_photon_source_f32": (ctypes.c_int, [_I32, _I32, _I32, ctypes.c_float, ctypes.c_uint64,
                                              ctypes.c_uint64, _P, _P, _P]),
     "pds_point_light_source_f32": (ctypes.c_int, [ctypes.POINTER(PdsPointLight), _I64,

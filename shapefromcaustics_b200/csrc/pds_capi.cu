@@ -550,6 +550,52 @@ int pds_refract_backward_f32(const float* h, int32_t rows, int32_t cols, const p
     return PDS_OK;
 }
 
+static int check_point(const pds_point_light* light, const float* dir, const float* dth,
+                       const float* dph, int64_t n) {
+    if (!light) return fail(PDS_ERR_INVALID_ARGUMENT, "null light");
+    if (n > 0 && (!dir || !dth || !dph))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null photon direction array");
+    return PDS_OK;
+}
+
+int pds_refract_point_forward_f32(const float* h, int32_t rows, int32_t cols,
+                                  const pds_plate* plate, const pds_point_light* light,
+                                  const float* dir, const float* dth, const float* dph,
+                                  const float* flux, const int64_t* channel, int64_t n, float* Ep,
+                                  float* xp, float* Mp, int64_t* cp, float* radius, void* stream) {
+    int rc = check_plate(h, rows, cols, plate, dir, dir, flux, n);
+    if (rc) return rc;
+    rc = check_point(light, dir, dth, dph, n);
+    if (rc) return rc;
+    if (n > 0 && (!Ep || !xp || !Mp || !cp || !radius))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
+    cudaError_t e = pds::launch_refract_point(false, h, rows, cols, *plate, *light, dir, dth, dph,
+                                              flux, channel, n, Ep, xp, Mp, cp, radius, nullptr,
+                                              nullptr, nullptr, nullptr,
+                                              static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "point_fwd_kernel");
+    return PDS_OK;
+}
+
+int pds_refract_point_backward_f32(const float* h, int32_t rows, int32_t cols,
+                                   const pds_plate* plate, const pds_point_light* light,
+                                   const float* dir, const float* dth, const float* dph,
+                                   const float* flux, int64_t n, const float* gE, const float* gX,
+                                   const float* gM, float* gh, void* stream) {
+    int rc = check_plate(h, rows, cols, plate, dir, dir, flux, n);
+    if (rc) return rc;
+    rc = check_point(light, dir, dth, dph, n);
+    if (rc) return rc;
+    if (n > 0 && (!gE || !gX || !gM || !gh))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
+    cudaError_t e = pds::launch_refract_point(true, h, rows, cols, *plate, *light, dir, dth, dph,
+                                              flux, nullptr, n, nullptr, nullptr, nullptr, nullptr,
+                                              nullptr, gE, gX, gM, gh,
+                                              static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "point_bwd_kernel");
+    return PDS_OK;
+}
+
 int pds_photon_source_f32(int32_t rows, int32_t cols, int32_t per_texel, float texel,
                           uint64_t seed, uint64_t offset, float* px, float* py, void* stream) {
     if (rows < 1 || cols < 1 || per_texel < 1)

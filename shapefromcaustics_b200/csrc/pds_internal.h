@@ -26,6 +26,14 @@ cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pd
                            int64_t* cp, float* radius, const float* gE, const float* gX,
                            const float* gM, float* gh, cudaStream_t st);
 
+cudaError_t launch_refract_point(bool backward, const float* h, int H, int W,
+                                 const pds_plate& plate, const pds_point_light& light,
+                                 const float* dir, const float* dth, const float* dph,
+                                 const float* flux, const int64_t* channel, int64_t n, float* Ep,
+                                 float* xp, float* Mp, int64_t* cp, float* radius,
+                                 const float* gE, const float* gX, const float* gM, float* gh,
+                                 cudaStream_t st);
+
 // photon source (pds_source.cu)
 cudaError_t launch_source(int32_t rows, int32_t cols, int32_t per_texel, float texel,
                           uint64_t seed, uint64_t offset, int64_t n, float* px, float* py,

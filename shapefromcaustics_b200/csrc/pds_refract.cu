@@ -215,9 +215,17 @@ __device__ __forceinline__ float hat(const float* h, int H, int W, int i, int j)
     return __ldg(h + int64_t(i) * W + j);
 }
 
-// The seven scalars of one photon: height, Sobel normal (x, y) and their x/y derivatives.
+// Position derivatives of the surface at a sample (for the traced hit).
+struct SurfGeo {
+    float hx, hy;        // slope of the bilinear height
+    float tw_nx, tw_ny;  // d2 Nx / dx dy, d2 Ny / dx dy of the bilinear normal field
+};
+
+// The seven scalars of one photon: height, Sobel normal (x, y) and their x/y derivatives;
+// with geo, also the position derivatives of the sample.
 __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, float texel,
-                                                const Bilin& b, float s[K]) {
+                                                const Bilin& b, float s[K],
+                                                SurfGeo* geo = nullptr) {
     const float c = -1.f / (8.f * texel);
     float hv[2][2], nx[2][2], ny[2][2];
 #pragma unroll
@@ -254,6 +262,15 @@ __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, fl
     s[4] = ddx(ny);  // dNy/dx
     s[5] = ddy(nx);  // dNx/dy
     s[6] = ddy(ny);  // dNy/dy
+    if (geo) {
+        // the height's slope and the normal field's twist d2/dxdy (the x derivatives above
+        // vary along y and the y derivatives along x by it)
+        geo->hx = ddx(hv);
+        geo->hy = ddy(hv);
+        const float it2 = 1.f / (texel * texel);
+        geo->tw_nx = ((nx[1][1] - nx[1][0]) - (nx[0][1] - nx[0][0])) * it2;
+        geo->tw_ny = ((ny[1][1] - ny[1][0]) - (ny[0][1] - ny[0][0])) * it2;
+    }
 }
 
 struct RefractArgs {
@@ -307,6 +324,57 @@ __global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
     }
 }
 
+// Adds d L / d height of one photon to its 4x4 texel patch (x0-1..x0+2, y0-1..y0+2) from the
+// derivatives c[k] of L with respect to its seven surface scalars: the transposed bilinear
+// stencil for the height (k = 0) and the transposed bilinear and Sobel stencils for the normal
+// scalars (k = 1..6). Patch texels outside the field fold onto the border (replicate padding).
+__device__ __forceinline__ void scatter_patch(float* gh, int H, int W, float texel,
+                                          const Bilin& b, const float c[K]) {
+    float patch[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) patch[r][q] = 0.f;
+    const float sob = -1.f / (8.f * texel);
+    const float it = 1.f / texel;
+    const float wv[2][2] = {{(1.f - b.ay) * (1.f - b.ax), (1.f - b.ay) * b.ax},
+                            {b.ay * (1.f - b.ax), b.ay * b.ax}};
+    const float wx[2][2] = {{-(1.f - b.ay) * it, (1.f - b.ay) * it}, {-b.ay * it, b.ay * it}};
+    const float wy[2][2] = {{-(1.f - b.ax) * it, -b.ax * it}, {(1.f - b.ax) * it, b.ax * it}};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            patch[r + 1][q + 1] += c[0] * wv[r][q];
+            const float gnx = sob * (c[1] * wv[r][q] + c[3] * wx[r][q] + c[5] * wy[r][q]);
+            const float gny = sob * (c[2] * wv[r][q] + c[4] * wx[r][q] + c[6] * wy[r][q]);
+            // Sobel x at (r, q): +(r-1,q+1) -(r-1,q-1) +2(r,q+1) -2(r,q-1) +(r+1,q+1) -(r+1,q-1)
+            patch[r][q + 2] += gnx;
+            patch[r][q] -= gnx;
+            patch[r + 1][q + 2] += 2.f * gnx;
+            patch[r + 1][q] -= 2.f * gnx;
+            patch[r + 2][q + 2] += gnx;
+            patch[r + 2][q] -= gnx;
+            // Sobel y: +(r+1,q-1) -(r-1,q-1) +2(r+1,q) -2(r-1,q) +(r+1,q+1) -(r-1,q+1)
+            patch[r + 2][q] += gny;
+            patch[r][q] -= gny;
+            patch[r + 2][q + 1] += 2.f * gny;
+            patch[r][q + 1] -= 2.f * gny;
+            patch[r + 2][q + 2] += gny;
+            patch[r][q + 2] -= gny;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int ii = min(max(b.y0 - 1 + r, 0), H - 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int jj = min(max(b.x0 - 1 + q, 0), W - 1);
+            if (patch[r][q] != 0.f) atomicAdd(gh + int64_t(ii) * W + jj, patch[r][q]);
+        }
+    }
+}
+
 __global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
     const int64_t n = a.n;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -333,50 +401,208 @@ __global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
         Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
         L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
         L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
-        // map d L / d scalars onto the 4x4 texel patch (x0-1..x0+2, y0-1..y0+2)
-        float patch[4][4];
+        float c[K];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) patch[r][q] = 0.f;
-        const float c = -1.f / (8.f * a.P.texel);
-        const float it = 1.f / a.P.texel;
-        const float wv[2][2] = {{(1.f - b.ay) * (1.f - b.ax), (1.f - b.ay) * b.ax},
-                                {b.ay * (1.f - b.ax), b.ay * b.ax}};
-        const float wx[2][2] = {{-(1.f - b.ay) * it, (1.f - b.ay) * it}, {-b.ay * it, b.ay * it}};
-        const float wy[2][2] = {{-(1.f - b.ax) * it, -b.ax * it}, {(1.f - b.ax) * it, b.ax * it}};
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                patch[r + 1][q + 1] += L.d[0] * wv[r][q];
-                const float gnx = c * (L.d[1] * wv[r][q] + L.d[3] * wx[r][q] + L.d[5] * wy[r][q]);
-                const float gny = c * (L.d[2] * wv[r][q] + L.d[4] * wx[r][q] + L.d[6] * wy[r][q]);
-                // Sobel x at (r, q): +(r-1,q+1) -(r-1,q-1) +2(r,q+1) -2(r,q-1) +(r+1,q+1) -(r+1,q-1)
-                patch[r][q + 2] += gnx;
-                patch[r][q] -= gnx;
-                patch[r + 1][q + 2] += 2.f * gnx;
-                patch[r + 1][q] -= 2.f * gnx;
-                patch[r + 2][q + 2] += gnx;
-                patch[r + 2][q] -= gnx;
-                // Sobel y: +(r+1,q-1) -(r-1,q-1) +2(r+1,q) -2(r-1,q) +(r+1,q+1) -(r-1,q+1)
-                patch[r + 2][q] += gny;
-                patch[r][q] -= gny;
-                patch[r + 2][q + 1] += 2.f * gny;
-                patch[r][q + 1] -= 2.f * gny;
-                patch[r + 2][q + 2] += gny;
-                patch[r][q + 2] -= gny;
-            }
+        for (int k = 0; k < K; ++k) c[k] = L.d[k];
+        scatter_patch(a.gh, a.H, a.W, a.P.texel, b, c);
+    }
+}
+
+// ---- point light: traced hit on the height field ----------------------------------------
+// Photons leave the light at o with unit direction d and direction differentials (Dth, Dph)
+// (pds_point_light_source_f32). Their first hit with the bilinear height-field surface is found
+// by Newton steps on f(t) = o_z + t d_z - h(o_xy + t d_xy) from the plane z = plane_z (no
+// overhangs and no occluding bump before the hit, as the reference's generate_from_point_light
+// assumes, model/caustics.py:119). At the hit the positional differentials are the light's
+// carried over the length t (model/photon_differential.py:69-78 with Du = Dv = 0 at the light),
+// and the chain continues as for the collimated plate with the direction differentials.
+
+struct Ray {
+    float ox, oy, oz;
+    float dx, dy, dz;
+};
+
+// Newton iterations of the trace; false when the ray grazes the surface or its hit lies
+// outside the field. b, s, geo: the surface at the hit; t: the ray parameter; fp: f'(t).
+__device__ __forceinline__ bool trace_hit(const float* h, int H, int W, float texel,
+                                          float plane_z, const Ray& r, float& t, Bilin& b,
+                                          float s[K], SurfGeo& geo, float& fp) {
+    t = (r.oz - plane_z) / (-r.dz);
+    const float cx = 0.5f * float(W - 1), cy = 0.5f * float(H - 1);
+    for (int it = 0; it < 10; ++it) {
+        const float px = r.ox + t * r.dx, py = r.oy + t * r.dy, pz = r.oz + t * r.dz;
+        b = bilin(px, py, texel, H, W);
+        surface_scalars(h, H, W, texel, b, s, &geo);
+        fp = r.dz - (geo.hx * r.dx + geo.hy * r.dy);
+        if (!(fabsf(fp) > 1e-6f)) return false;
+        const float step = (pz - s[0]) / fp;
+        t -= step;
+        if (fabsf(step) <= 1e-7f * fabsf(t)) break;
+    }
+    const float px = r.ox + t * r.dx, py = r.oy + t * r.dy;
+    const float fx = px / texel + cx, fy = py / texel + cy;
+    if (!(fx >= 0.f && fx <= float(W - 1) && fy >= 0.f && fy <= float(H - 1))) return false;
+    b = bilin(px, py, texel, H, W);
+    surface_scalars(h, H, W, texel, b, s, &geo);
+    fp = r.dz - (geo.hx * r.dx + geo.hy * r.dy);
+    return fabsf(fp) > 1e-6f;
+}
+
+// The refraction chain of one point-light photon from its hit parameter t and the six normal
+// scalars at the hit (Nx, Ny, dNx/dx, dNy/dx, dNx/dy, dNy/dy).
+template <class T>
+__device__ __forceinline__ void point_chain(const T& t, const T& Nx, const T& Ny, const T& Nxx,
+                                            const T& Nyx, const T& Nxy, const T& Nyy,
+                                            const Ray& r, const V3<float>& Dth,
+                                            const V3<float>& Dph, const PlateParams& P, T& xr,
+                                            T& yr, T& Dux, T& Duy, T& Dvx, T& Dvy) {
+    const V3<T> d = {cst<T>(r.dx), cst<T>(r.dy), cst<T>(r.dz)};
+    const V3<T> Dt = {cst<T>(Dth.x), cst<T>(Dth.y), cst<T>(Dth.z)};
+    const V3<T> Dp = {cst<T>(Dph.x), cst<T>(Dph.y), cst<T>(Dph.z)};
+    const V3<T> p1 = {cst<T>(r.ox) + t * d.x, cst<T>(r.oy) + t * d.y, cst<T>(r.oz) + t * d.z};
+    const V3<T> Nt = {Nx, Ny, cst<T>(1.f)};
+    const T nn = vdot(Nt, Nt);
+    const T nlen = dsqrt(nn);
+    const V3<T> n = vscale(cst<T>(1.f) / nlen, Nt);
+    const T nd = vdot(n, d);
+    // positional differentials carried from the light over t onto the tangent plane
+    const V3<T> Du1 = vscale(t, vsub(Dt, vscale(vdot(n, Dt) / nd, d)));
+    const V3<T> Dv1 = vscale(t, vsub(Dp, vscale(vdot(n, Dp) / nd, d)));
+    const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
+    const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
+    const T nl3 = nn * nlen;
+    const V3<T> dnu = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
+    const V3<T> dnv = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
+    V3<T> t1, Ddu, Ddv, tmp;
+    refract(d, n, Dt, dnu, 1.f / P.ior, t1, Ddu);
+    refract(d, n, Dp, dnv, 1.f / P.ior, tmp, Ddv);
+    const T s1 = -p1.z / t1.z;
+    const V3<T> p2 = {p1.x + s1 * t1.x, p1.y + s1 * t1.y, cst<T>(0.f)};
+    const V3<T> Du2 = transfer_z(Du1, Ddu, s1, t1);
+    const V3<T> Dv2 = transfer_z(Dv1, Ddv, s1, t1);
+    const V3<T> ez = {cst<T>(0.f), cst<T>(0.f), cst<T>(1.f)};
+    const V3<T> zero = {cst<T>(0.f), cst<T>(0.f), cst<T>(0.f)};
+    V3<T> t2, Ddu2, Ddv2;
+    refract(t1, ez, Ddu, zero, P.ior, t2, Ddu2);
+    refract(t1, ez, Ddv, zero, P.ior, tmp, Ddv2);
+    const T s2 = cst<T>(-P.dist) / t2.z;
+    const V3<T> Du3 = transfer_z(Du2, Ddu2, s2, t2);
+    const V3<T> Dv3 = transfer_z(Dv2, Ddv2, s2, t2);
+    xr = P.inv_half * (p2.x + s2 * t2.x);
+    yr = P.inv_half * (p2.y + s2 * t2.y);
+    Dux = P.inv_half * Du3.x;
+    Duy = P.inv_half * Du3.y;
+    Dvx = P.inv_half * Dv3.x;
+    Dvy = P.inv_half * Dv3.y;
+}
+
+struct PointArgs {
+    const float* h;
+    int H, W;
+    PlateParams P;
+    float ox, oy, oz, plane_z;
+    const float* dir;   // [3][n]
+    const float* dth;   // [3][n]
+    const float* dph;   // [3][n]
+    const float* flux;
+    const int64_t* channel;
+    int64_t n;
+    float* Ep;
+    float* xp;
+    float* Mp;
+    int64_t* cp;
+    float* radius;
+    const float* gE;
+    const float* gX;
+    const float* gM;
+    float* gh;
+};
+
+__device__ __forceinline__ Ray photon_ray(const PointArgs& a, int64_t i) {
+    Ray r;
+    r.ox = a.ox; r.oy = a.oy; r.oz = a.oz;
+    r.dx = a.dir[i]; r.dy = a.dir[a.n + i]; r.dz = a.dir[2 * a.n + i];
+    return r;
+}
+
+__global__ __launch_bounds__(256) void point_fwd_kernel(PointArgs a) {
+    const int64_t n = a.n;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const Ray r = photon_ray(a, i);
+        float t, fp, s[K];
+        Bilin b;
+        SurfGeo geo;
+        const bool hit = trace_hit(a.h, a.H, a.W, a.P.texel, a.plane_z, r, t, b, s, geo, fp);
+        float xr = 0.f, yr = 0.f, Dux = 0.f, Duy = 0.f, Dvx = 0.f, Dvy = 0.f;
+        if (hit) {
+            const V3<float> Dt = {a.dth[i], a.dth[n + i], a.dth[2 * n + i]};
+            const V3<float> Dp = {a.dph[i], a.dph[n + i], a.dph[2 * n + i]};
+            point_chain<float>(t, s[1], s[2], s[3], s[4], s[5], s[6], r, Dt, Dp, a.P, xr, yr, Dux,
+                               Duy, Dvx, Dvy);
         }
+        const float den = Dux * Dvy - Duy * Dvx;
+        const bool good = hit && den != 0.f;
+        const float f = 2.f / (good ? den : 1.f);
+        a.Mp[i] = f * Dvy;
+        a.Mp[n + i] = -f * Dvx;
+        a.Mp[2 * n + i] = 0.f;
+        a.Mp[3 * n + i] = -f * Duy;
+        a.Mp[4 * n + i] = f * Dux;
+        a.Mp[5 * n + i] = 0.f;
+        a.xp[i] = xr;
+        a.xp[n + i] = yr;
+        a.radius[i] = 0.5f * fmaxf(sqrtf(Dux * Dux + Duy * Duy), sqrtf(Dvx * Dvx + Dvy * Dvy));
+        a.Ep[i] = 4.f * a.flux[i] / (good ? fabsf(den) : 1.f);
+        const int64_t ch = a.channel ? a.channel[i] : 0;
+        a.cp[i] = good ? ch : -1;
+    }
+}
+
+__global__ __launch_bounds__(256) void point_bwd_kernel(PointArgs a) {
+    const int64_t n = a.n;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const Ray r = photon_ray(a, i);
+        float t, fp, s[K];
+        Bilin b;
+        SurfGeo geo;
+        if (!trace_hit(a.h, a.H, a.W, a.P.texel, a.plane_z, r, t, b, s, geo, fp)) continue;
+        // component 0: the hit parameter t (the scalars follow the hit along the ray: their
+        // position derivatives times d); components 1-6: the normal scalars at a fixed position
+        Dual v[K];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int ii = min(max(b.y0 - 1 + r, 0), a.H - 1);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int jj = min(max(b.x0 - 1 + q, 0), a.W - 1);
-                if (patch[r][q] != 0.f) atomicAdd(a.gh + int64_t(ii) * a.W + jj, patch[r][q]);
-            }
+        for (int k = 0; k < K; ++k) {
+            v[k] = dconst(s[k]);
+            v[k].d[k] = 1.f;
         }
+        v[0].v = t;
+        v[1].d[0] = s[3] * r.dx + s[5] * r.dy;
+        v[2].d[0] = s[4] * r.dx + s[6] * r.dy;
+        v[3].d[0] = geo.tw_nx * r.dy;
+        v[4].d[0] = geo.tw_ny * r.dy;
+        v[5].d[0] = geo.tw_nx * r.dx;
+        v[6].d[0] = geo.tw_ny * r.dx;
+        const V3<float> Dt = {a.dth[i], a.dth[n + i], a.dth[2 * n + i]};
+        const V3<float> Dp = {a.dph[i], a.dph[n + i], a.dph[2 * n + i]};
+        Dual xr, yr, Dux, Duy, Dvx, Dvy;
+        point_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], r, Dt, Dp, a.P, xr, yr, Dux,
+                          Duy, Dvx, Dvy);
+        const Dual den = Dux * Dvy - Duy * Dvx;
+        if (den.v == 0.f) continue;
+        const Dual f = dconst(2.f) / den;
+        const float gE = a.gE[i];
+        const float g0 = a.gM[i], g1 = a.gM[n + i], g3 = a.gM[3 * n + i], g4 = a.gM[4 * n + i];
+        Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
+        L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
+        L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
+        // the hit moves with the heights: dt / dh_j = w_j / f'(t) for the bilinear weights w_j
+        // of the hit's cell
+        float c[K];
+        c[0] = L.d[0] / fp;
+#pragma unroll
+        for (int k = 1; k < K; ++k) c[k] = L.d[k];
+        scatter_patch(a.gh, a.H, a.W, a.P.texel, b, c);
     }
 }
 
@@ -390,6 +616,50 @@ int grid_for(int64_t n) {
 }
 
 }  // namespace
+
+cudaError_t launch_refract_point(bool backward, const float* h, int H, int W,
+                                 const pds_plate& plate, const pds_point_light& light,
+                                 const float* dir, const float* dth, const float* dph,
+                                 const float* flux, const int64_t* channel, int64_t n, float* Ep,
+                                 float* xp, float* Mp, int64_t* cp, float* radius,
+                                 const float* gE, const float* gX, const float* gM, float* gh,
+                                 cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    PointArgs a;
+    a.h = h;
+    a.H = H;
+    a.W = W;
+    a.P.texel = plate.texel;
+    a.P.ior = plate.ior;
+    a.P.dist = plate.receiver_distance;
+    a.P.inv_half = 1.f / plate.receiver_half;
+    a.P.du0 = 0.f;
+    a.P.lx = a.P.ly = a.P.lz = 0.f;
+    a.ox = light.position[0];
+    a.oy = light.position[1];
+    a.oz = light.position[2];
+    a.plane_z = light.plane_z;
+    a.dir = dir;
+    a.dth = dth;
+    a.dph = dph;
+    a.flux = flux;
+    a.channel = channel;
+    a.n = n;
+    a.Ep = Ep;
+    a.xp = xp;
+    a.Mp = Mp;
+    a.cp = cp;
+    a.radius = radius;
+    a.gE = gE;
+    a.gX = gX;
+    a.gM = gM;
+    a.gh = gh;
+    if (backward)
+        point_bwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+    else
+        point_fwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
                            const float* px, const float* py, const float* flux,

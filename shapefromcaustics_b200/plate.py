@@ -22,7 +22,8 @@ from ._lib import check, lib
 from .splatting import SplatPlan, _ptr, _stream
 
 __all__ = ["PlateParams", "plate_params", "refract_forward", "refract_backward", "PlateSplat",
-           "PointLight", "point_light", "point_light_source"]
+           "PointLight", "point_light", "point_light_source", "refract_point_forward",
+           "refract_point_backward", "PointPlateSplat"]
 
 
 PlateParams = _lib.PdsPlate
@@ -161,3 +162,70 @@ def point_light_source(light, n_directions, device, seed=0, offset=0, coeffs=Non
             ctypes.byref(light), int(n_directions), int(seed) & (2 ** 64 - 1), int(offset),
             _ptr(coeffs) if coeffs is not None else None, *(_ptr(t) for t in out), _stream(dev)))
     return (*out, int(offset) + (int(n_directions) + 1) // 2)
+
+
+def refract_point_forward(height, light, params, direction, dtheta, dphi, flux, channel=None):
+    """Splat inputs ``(Ep, xp, Mp, cp, radius)`` of point-light photons traced onto the plate
+    (``pds_refract_point_forward_f32``)."""
+    for t, nm in ((height, "height"), (direction, "direction"), (dtheta, "dtheta"),
+                  (dphi, "dphi"), (flux, "flux")):
+        _check_f32(t, nm)
+    n = flux.numel()
+    dev = height.device
+    Ep = torch.empty(n, device=dev)
+    xp = torch.empty((2, n), device=dev)
+    Mp = torch.empty((2, 3, n), device=dev)
+    cp = torch.empty((1, n), dtype=torch.int64, device=dev)
+    radius = torch.empty(n, device=dev)
+    with torch.cuda.device(dev):
+        check(_fn("pds_refract_point_forward_f32")(
+            _ptr(height), height.shape[0], height.shape[1], ctypes.byref(params),
+            ctypes.byref(light), _ptr(direction), _ptr(dtheta), _ptr(dphi), _ptr(flux),
+            _ptr(channel) if channel is not None else None, n, _ptr(Ep), _ptr(xp), _ptr(Mp),
+            _ptr(cp), _ptr(radius), _stream(dev)))
+    return Ep, xp, Mp, cp, radius
+
+
+def refract_point_backward(height, light, params, direction, dtheta, dphi, flux, gE, gX, gM,
+                           grad_height=None):
+    """Adds d L / d height for point-light photons (``pds_refract_point_backward_f32``)."""
+    n = flux.numel()
+    if grad_height is None:
+        grad_height = torch.zeros_like(height)
+    with torch.cuda.device(height.device):
+        check(_fn("pds_refract_point_backward_f32")(
+            _ptr(height), height.shape[0], height.shape[1], ctypes.byref(params),
+            ctypes.byref(light), _ptr(direction), _ptr(dtheta), _ptr(dphi), _ptr(flux), n,
+            _ptr(gE.contiguous()), _ptr(gX.contiguous()), _ptr(gM.contiguous()),
+            _ptr(grad_height), _stream(height.device)))
+    return grad_height
+
+
+class PointPlateSplat(torch.autograd.Function):
+    """Caustic image of the plate lit by a point light (photons traced onto the height-field
+    surface); differentiable in the height field. ``photons`` = ``(direction, dtheta, dphi,
+    flux)`` as from ``point_light_source``."""
+
+    @staticmethod
+    def forward(ctx, height, direction, dtheta, dphi, flux, light, params, output_size,
+                max_pixel_radius):
+        h = height.detach().contiguous()
+        inputs = refract_point_forward(h, light, params, direction, dtheta, dphi, flux)
+        plan = SplatPlan(*inputs, output_size, max_pixel_radius)
+        img = plan.forward()
+        ctx.save_for_backward(h, direction, dtheta, dphi, flux)
+        ctx.light, ctx.params = light, params
+        ctx.shape = tuple(int(v) for v in output_size)
+        ctx.mpr = int(max_pixel_radius)
+        ctx.cfg = plan.cfg
+        return img
+
+    @staticmethod
+    def backward(ctx, grad_img):
+        h, direction, dtheta, dphi, flux = ctx.saved_tensors
+        inputs = refract_point_forward(h, ctx.light, ctx.params, direction, dtheta, dphi, flux)
+        plan = SplatPlan(*inputs, ctx.shape, ctx.mpr, config=ctx.cfg)
+        gE, gX, gM = plan.backward(grad_img.contiguous())
+        gh = refract_point_backward(h, ctx.light, ctx.params, direction, dtheta, dphi, flux, gE,
+                                    gX, gM)
+        return gh, None, None, None, None, None, None, None, None

@@ -219,3 +219,80 @@ def test_point_light_source_matches_compute_point_light_dirs(cuda):
     assert rel_l2(d.cpu().numpy().T, rd) < 1e-6
     assert rel_l2(dt.cpu().numpy().T, rt) < 1e-5
     assert rel_l2(flux.cpu().numpy(), rf) < 1e-6
+
+
+def point_scene(n=48, n_dir=20000, seed=2):
+    """A point light 40 mm above a 48 x 48 plate (texel 0.4 mm), photons from the device
+    source, evaluated in float64 on their float32 values."""
+    from shapefromcaustics_b200 import plate as PL
+    scene = RF.PlateScene(texel=0.4, receiver_distance=30.0, receiver_half=12.0)
+    h = RF.height_field_bumps(n, n, seed=seed, bumps=10, base=1.0, amp=(0.0, 0.05),
+                              width=(2.0, 6.0)).float()
+    half = 0.5 * (n - 1) * scene.texel
+    rect = (-half + 0.2, -half + 0.2, half - 0.2, half - 0.2)
+    light = PL.point_light((0.5, -0.4, 40.0), rect, 1.0, 3.0, 1.0, 1, 1, 1)
+    d, dt, dp, flux, _ = PL.point_light_source(light, n_dir, "cuda", seed=seed)
+    return scene, h, light, (d, dt, dp, flux)
+
+
+def test_point_light_refract_forward_matches_float64_chain(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, light, (d, dt, dp, flux) = point_scene()
+    params = PL.plate_params(scene, 0.0)
+    Ep, xp, Mp, cp, radius = PL.refract_point_forward(h.cuda(), light, params, d, dt, dp, flux)
+    torch.cuda.synchronize()
+    pos = tuple(light.position)
+    rE, rx, rM, rc, rr = RF.point_light_splat_inputs(
+        h.double(), scene, pos, d.double().cpu(), dt.double().cpu(), dp.double().cpu(),
+        flux.double().cpu(), float(light.plane_z))
+    assert torch.equal(cp.cpu(), rc) and bool((rc >= 0).all())
+    assert rel_l2(xp.cpu(), rx) < 1e-6
+    assert rel_l2(Ep.cpu(), rE) < 1e-4
+    assert rel_l2(Mp.cpu(), rM) < 1e-4
+    assert rel_l2(radius.cpu(), rr) < 1e-4
+
+
+def test_point_light_refract_backward_matches_float64_autograd(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, light, (d, dt, dp, flux) = point_scene(seed=3)
+    params = PL.plate_params(scene, 0.0)
+    n = flux.numel()
+    g = torch.Generator().manual_seed(0)
+    gE = torch.randn(n, generator=g, dtype=torch.float64)
+    gX = torch.randn((2, n), generator=g, dtype=torch.float64)
+    gM = torch.randn((2, 3, n), generator=g, dtype=torch.float64) * 1e-3
+    gM[:, 2] = 0
+    gh = PL.refract_point_backward(h.cuda(), light, params, d, dt, dp, flux, gE.float().cuda(),
+                                   gX.float().cuda(), gM.float().cuda())
+    hd = h.double().requires_grad_(True)
+    Ep, xp, Mp, cp, radius = RF.point_light_splat_inputs(
+        hd, scene, tuple(light.position), d.double().cpu(), dt.double().cpu(), dp.double().cpu(),
+        flux.double().cpu(), float(light.plane_z))
+    L = (Ep * gE).sum() + (xp * gX).sum() + (Mp * gM).sum()
+    (ref,) = torch.autograd.grad(L, hd)
+    torch.cuda.synchronize()
+    assert rel_l2(gh.cpu(), ref) < 1e-3
+
+
+def test_point_plate_splat_end_to_end_gradient(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, light, (d, dt, dp, flux) = point_scene(seed=5)
+    params = PL.plate_params(scene, 0.0)
+    shape = (1, 128, 128)
+    G = torch.randn(shape, generator=torch.Generator().manual_seed(1), dtype=torch.float64)
+    hv = h.cuda().requires_grad_(True)
+    img = PL.PointPlateSplat.apply(hv, d, dt, dp, flux, light, params, shape, 20)
+    (img * G.float().cuda()).sum().backward()
+    hd = h.double().requires_grad_(True)
+    Ep, xp, Mp, cp, radius = RF.point_light_splat_inputs(
+        hd, scene, tuple(light.position), d.double().cpu(), dt.double().cpu(), dp.double().cpu(),
+        flux.double().cpu(), float(light.plane_z))
+    a = [t.detach().numpy() for t in (Ep, xp, Mp, cp, radius)]
+    rimg = O.forward(*a, shape, 20)
+    gE, gX, gM = O.backward(G.numpy(), *a, 20)
+    L = (Ep * torch.from_numpy(gE)).sum() + (xp * torch.from_numpy(gX)).sum() + \
+        (Mp * torch.from_numpy(gM)).sum()
+    (ref,) = torch.autograd.grad(L, hd)
+    torch.cuda.synchronize()
+    assert rel_l2(img.detach().cpu(), rimg) < 1e-4
+    assert rel_l2(hv.grad.cpu(), ref) < 1e-3
