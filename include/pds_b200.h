@@ -149,14 +149,23 @@ int pds_plan_export(const void* workspace, size_t workspace_bytes, int64_t n_pho
  * n_total); images live in one flat buffer at each simulation's image_offset. */
 
 /* Fills tiles_x, tiles_y, tile_base of sims[0..n_sims) (host memory) for cfg and returns
- * the total tile count in *n_tiles_total. */
+ * the total tile count in *n_tiles_total. Each simulation's image range
+ * [image_offset, image_offset + C*H*W) must be identical to or disjoint from every other's
+ * (simulations that share an image are summed into it); PDS_ERR_INVALID_ARGUMENT otherwise. */
 int pds_batch_layout(pds_sim* sims, int32_t n_sims, const pds_config* cfg,
                      int64_t* n_tiles_total);
+
+/* The element count the batch's image buffers (the forward's out, the backward's grad) must
+ * hold: the end of the last image range of sims[0..n_sims) (host memory), after the same range
+ * checks as pds_batch_layout. */
+int pds_batch_image_elems(const pds_sim* sims, int32_t n_sims, int64_t* image_elems);
 
 size_t pds_batch_workspace_bytes(int64_t n_total, int64_t n_tiles_total, const pds_config* cfg);
 
 /* sims_dev: the laid-out table in device memory. out: flat image buffer, overwritten over
- * [0, image_elems) where image_elems = max(image_offset + C*H*W). */
+ * [0, image_elems) where image_elems = max(image_offset + C*H*W) (pds_batch_image_elems).
+ * Image planes of a table that reach past image_elems are not written (their photons add
+ * nothing), so an inconsistent device table cannot write outside the buffer. */
 int pds_batch_plan_f32(const float* Ep, const float* xp, const float* Mp, const int64_t* cp,
                        const float* radius, int64_t n_total, const pds_sim* sims_dev,
                        int32_t n_sims, int64_t n_tiles_total, int32_t max_pixel_radius,
@@ -168,10 +177,13 @@ int pds_batch_forward_planned_f32(const float* Ep, const float* xp, const float*
                                   int64_t n_tiles_total, int64_t image_elems,
                                   int32_t max_pixel_radius, float* out, void* workspace,
                                   size_t workspace_bytes, const pds_config* cfg, void* stream);
+/* grad: the flat upstream gradient of the batch's images, image_elems elements (image planes
+ * past it are not read: their photons get zero gradients). */
 int pds_batch_backward_planned_f32(const float* grad, const float* Ep, const float* xp,
                                    const float* Mp, const int64_t* cp, const float* radius,
                                    int64_t n_total, const pds_sim* sims_dev, int32_t n_sims,
-                                   int64_t n_tiles_total, int32_t max_pixel_radius,
+                                   int64_t n_tiles_total, int64_t image_elems,
+                                   int32_t max_pixel_radius,
                                    float* grad_Ep, float* grad_xp, float* grad_Mp,
                                    void* workspace, size_t workspace_bytes,
                                    const pds_config* cfg, void* stream);

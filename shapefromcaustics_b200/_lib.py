@@ -82,13 +82,16 @@ SIGNATURES = {
                                                 _I32, _P, _P, _P, _P, _SZ, _CFG, _P]),
     "pds_batch_layout": (ctypes.c_int, [ctypes.POINTER(PdsSim), _I32, _CFG,
                                         ctypes.POINTER(_I64)]),
+    "pds_batch_image_elems": (ctypes.c_int, [ctypes.POINTER(PdsSim), _I32,
+                                             ctypes.POINTER(_I64)]),
     "pds_batch_workspace_bytes": (_SZ, [_I64, _I64, _CFG]),
     "pds_batch_plan_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P, _I32, _I64, _I32, _P, _SZ,
                                           _CFG, _P]),
     "pds_batch_forward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P, _I32, _I64,
                                                      _I64, _I32, _P, _P, _SZ, _CFG, _P]),
     "pds_batch_backward_planned_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _P, _I32,
-                                                      _I64, _I32, _P, _P, _P, _P, _SZ, _CFG, _P]),
+                                                      _I64, _I64, _I32, _P, _P, _P, _P, _SZ, _CFG,
+                                                      _P]),
     "pds_refract_forward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate), _P, _P,
                                                _P, _P, _I64, _P, _P, _P, _P, _P, _P]),
     "pds_refract_backward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate), _P, _P,

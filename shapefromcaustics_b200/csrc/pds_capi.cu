@@ -10,9 +10,13 @@
 // on the caller's stream. It allocates nothing and never synchronises. Failures return a
 // PDS_ERR_* code and leave a message for pds_last_error() (the reference raises through
 // TORCH_CHECK and does not check its launches, photon_differentials.cu:125, :234).
+#include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "pds_internal.h"
 #include "pds_splat.h"
@@ -316,6 +320,7 @@ int forward_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tile
     int rc = tile_args(ph, st, n_tiles, mpr, cfg, ws, ws_bytes, a);
     if (rc) return rc;
     a.out = out;
+    a.image_elems = image_elems;
     cudaError_t e = cudaMemsetAsync(out, 0, size_t(image_elems) * sizeof(float), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return cuda_fail(e, "forward: output reset");
@@ -326,8 +331,8 @@ int forward_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tile
 }
 
 int backward_impl(const float* grad, const pds::Photons& ph, const pds::SimTable& st,
-                  int64_t n_tiles, int32_t mpr, float* gE, float* gX, float* gM,
-                  const pds_config* cfg, void* ws, size_t ws_bytes, cudaStream_t s) {
+                  int64_t n_tiles, int64_t image_elems, int32_t mpr, float* gE, float* gX,
+                  float* gM, const pds_config* cfg, void* ws, size_t ws_bytes, cudaStream_t s) {
     if (ph.n > 0 && (!grad || !gE || !gX || !gM))
         return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
     pds::TileArgs a;
@@ -335,6 +340,7 @@ int backward_impl(const float* grad, const pds::Photons& ph, const pds::SimTable
     if (rc) return rc;
     if (ph.n == 0) return PDS_OK;
     a.grad = grad;
+    a.image_elems = image_elems;
     a.gE = gE;
     a.gX = gX;
     a.gM = gM;
@@ -420,8 +426,8 @@ int pds_backward_planned_f32(const float* G, const float* E, const float* X, con
     int64_t nt;
     rc = single_tiles(cfg, C, H, W, &nt, &sim, n);
     if (rc) return rc;
-    return backward_impl(G, photons(E, X, M, cp, R, n), table_one(sim), nt, mpr, gE, gX, gM,
-                         cfg, ws, ws_bytes, static_cast<cudaStream_t>(stream));
+    return backward_impl(G, photons(E, X, M, cp, R, n), table_one(sim), nt, C * H * W, mpr, gE,
+                         gX, gM, cfg, ws, ws_bytes, static_cast<cudaStream_t>(stream));
 }
 
 int pds_forward_f32(const float* E, const float* X, const float* M, const int64_t* cp,
@@ -443,6 +449,42 @@ int pds_backward_f32(const float* G, const float* E, const float* X, const float
                                     ws_bytes, cfg, stream);
 }
 
+// The simulations' image ranges [image_offset, image_offset + C*H*W): each must be identical
+// to or disjoint from every other (simulations that share an image are summed into it, as the
+// reference's caller sums its simulations); the end of the last range in *elems.
+static int check_image_ranges(const pds_sim* sims, int32_t n_sims, int64_t* elems) {
+    std::vector<std::pair<int64_t, int64_t>> r;
+    r.reserve(size_t(n_sims));
+    for (int32_t s = 0; s < n_sims; ++s) {
+        const pds_sim& d = sims[s];
+        if (d.image_offset < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative image_offset");
+        const int64_t size = int64_t(d.channels) * d.height * d.width;
+        if (d.image_offset > INT64_MAX - size)
+            return fail(PDS_ERR_INVALID_ARGUMENT, "image range overflows");
+        r.emplace_back(d.image_offset, d.image_offset + size);
+    }
+    std::sort(r.begin(), r.end());
+    int64_t end = 0;
+    for (size_t k = 0; k < r.size(); ++k) {
+        if (k > 0 && r[k].first < r[k - 1].second && r[k] != r[k - 1])
+            return fail(PDS_ERR_INVALID_ARGUMENT,
+                        "simulation image ranges overlap without being the same image");
+        end = r[k].second > end ? r[k].second : end;
+    }
+    *elems = end;
+    return PDS_OK;
+}
+
+int pds_batch_image_elems(const pds_sim* sims, int32_t n_sims, int64_t* image_elems) {
+    if (!sims || n_sims < 1 || !image_elems)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "pds_batch_image_elems: empty or null table");
+    for (int32_t s = 0; s < n_sims; ++s) {
+        int rc = check_image(sims[s].channels, sims[s].height, sims[s].width);
+        if (rc) return rc;
+    }
+    return check_image_ranges(sims, n_sims, image_elems);
+}
+
 int pds_batch_layout(pds_sim* sims, int32_t n_sims, const pds_config* cfg, int64_t* n_tiles) {
     pds_config c;
     int rc = resolve_cfg(cfg, c);
@@ -457,7 +499,6 @@ int pds_batch_layout(pds_sim* sims, int32_t n_sims, const pds_config* cfg, int64
         if (d.n_photons < 0 || d.photon_begin != next_photon)
             return fail(PDS_ERR_INVALID_ARGUMENT,
                         "simulations must cover the photon arrays contiguously and in order");
-        if (d.image_offset < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative image_offset");
         next_photon += d.n_photons;
         d.tiles_x = int32_t((d.width + c.tile - 1) / c.tile);
         d.tiles_y = int32_t((d.height + c.tile - 1) / c.tile);
@@ -465,6 +506,9 @@ int pds_batch_layout(pds_sim* sims, int32_t n_sims, const pds_config* cfg, int64
         base += int64_t(d.channels) * d.tiles_x * d.tiles_y;
         if (base >= (int64_t(1) << 30)) return fail(PDS_ERR_UNSUPPORTED, "too many tiles");
     }
+    int64_t elems = 0;
+    rc = check_image_ranges(sims, n_sims, &elems);
+    if (rc) return rc;
     *n_tiles = base;
     return PDS_OK;
 }
@@ -497,14 +541,15 @@ int pds_batch_forward_planned_f32(const float* E, const float* X, const float* M
 int pds_batch_backward_planned_f32(const float* G, const float* E, const float* X,
                                    const float* M, const int64_t* cp, const float* R,
                                    int64_t n_total, const pds_sim* sims_dev, int32_t n_sims,
-                                   int64_t n_tiles, int32_t mpr, float* gE, float* gX, float* gM,
-                                   void* ws, size_t ws_bytes, const pds_config* cfg,
-                                   void* stream) {
+                                   int64_t n_tiles, int64_t image_elems, int32_t mpr, float* gE,
+                                   float* gX, float* gM, void* ws, size_t ws_bytes,
+                                   const pds_config* cfg, void* stream) {
     int rc = check_photons(E, X, M, cp, R, n_total);
     if (rc) return rc;
     if (!sims_dev || n_sims < 1) return fail(PDS_ERR_INVALID_ARGUMENT, "null simulation table");
+    if (image_elems < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative image_elems");
     return backward_impl(G, photons(E, X, M, cp, R, n_total), table_dev(sims_dev, n_sims),
-                         n_tiles, mpr, gE, gX, gM, cfg, ws, ws_bytes,
+                         n_tiles, image_elems, mpr, gE, gX, gM, cfg, ws, ws_bytes,
                          static_cast<cudaStream_t>(stream));
 }
 

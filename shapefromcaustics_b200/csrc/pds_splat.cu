@@ -43,6 +43,7 @@ __device__ __forceinline__ int64_t wide_count(const TileArgs& a) {
 
 struct TileInfo {
     int64_t img_off;  // element offset of the (simulation, channel) image plane
+    bool in_image;    // the plane lies inside the caller's image buffer
     int32_t W, H;
     int32_t ox, oy;   // pixel coordinates of the accumulator's (0, 0)
     float sx, sy;     // 2 / W, 2 / H
@@ -53,7 +54,8 @@ struct TileInfo {
 __device__ __forceinline__ double img_wd(const TileInfo& t) { return double(float(t.W)); }
 __device__ __forceinline__ double img_hd(const TileInfo& t) { return double(float(t.H)); }
 
-__device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t tile, const Cfg& cfg) {
+__device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t tile, const Cfg& cfg,
+                                                int64_t image_elems) {
     const int s = find_sim_of_tile(st, tile);
     const pds_sim sim = load_sim(st, s);
     const int32_t local = int32_t(tile) - sim.tile_base;
@@ -65,6 +67,7 @@ __device__ __forceinline__ TileInfo decode_tile(const SimTable& st, uint32_t til
     t.W = sim.width;
     t.H = sim.height;
     t.img_off = sim.image_offset + int64_t(ch) * sim.height * sim.width;
+    t.in_image = t.img_off >= 0 && t.img_off + int64_t(sim.height) * sim.width <= image_elems;
     t.ox = tx * cfg.tile - cfg.apron;
     t.oy = ty * cfg.tile - cfg.apron;
     t.sx = float(2.0 / double(sim.width));
@@ -502,7 +505,13 @@ __device__ __forceinline__ void flush_tile(float* acc, int sw, const TileInfo& t
     if (threadIdx.x == 0) {
         sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
     }
-    if (x0 <= x1) {
+    if (x0 <= x1 && !ti.in_image) {
+        // a plane outside the caller's buffer (an inconsistent simulation table): clear only
+        for (int gy = y0 + int(threadIdx.x >> 5); gy <= y1; gy += int(blockDim.x >> 5)) {
+            float* arow = acc + (gy - ti.oy) * sw - ti.ox;
+            for (int gx = x0 + int(threadIdx.x & 31); gx <= x1; gx += 32) arow[gx] = 0.f;
+        }
+    } else if (x0 <= x1) {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int nw = blockDim.x >> 5;
         float* img = out + ti.img_off;
@@ -614,7 +623,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
          c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
         Segment sg = first_segment(a, c, p0);
-        TileInfo ti = decode_tile(a.sims, sg.tile, cfg);
+        TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
         for (int64_t base = p0; base < p1; base += NT) {
             const int64_t i = base + threadIdx.x;
             const bool have = i < p1;
@@ -656,7 +665,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
                 if (sg.end >= bend) break;
                 flush_tile(acc, sw, ti, a.out, sb);
                 sg = next_segment(a, sg);
-                ti = decode_tile(a.sims, sg.tile, cfg);
+                ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
             }
         }
         flush_tile(acc, sw, ti, a.out, sb);
@@ -675,7 +684,8 @@ __device__ __forceinline__ void load_region(float* tg, int sw, const TileInfo& t
     for (int gy = gy0 + warp; gy < gy1; gy += nw) {
         float* trow = tg + (gy - ti.oy) * sw - ti.ox;
         const float* grow = img + int64_t(gy) * ti.W;
-        for (int gx = gx0 + lane; gx < gx1; gx += 32) trow[gx] = __ldg(grow + gx);
+        for (int gx = gx0 + lane; gx < gx1; gx += 32)
+            trow[gx] = ti.in_image ? __ldg(grow + gx) : 0.f;
     }
 }
 
@@ -991,7 +1001,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
          c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
         Segment sg = first_segment(a, c, p0);
-        TileInfo ti = decode_tile(a.sims, sg.tile, cfg);
+        TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
         // next_chunk's barrier ends the previous chunk's reads of the staged tile
         load_region(tg, sw, ti, a.grad);
         __syncthreads();
@@ -1032,7 +1042,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
                 }
                 if (sg.end >= bend) break;
                 sg = next_segment(a, sg);
-                ti = decode_tile(a.sims, sg.tile, cfg);
+                ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
                 __syncthreads();
                 load_region(tg, sw, ti, a.grad);
                 __syncthreads();
@@ -1078,6 +1088,7 @@ __device__ __forceinline__ bool direct_setup(const TileArgs& a, uint32_t rid, Di
     d.wd = double(float(sim.width));
     d.hd = double(float(sim.height));
     d.img_off = sim.image_offset + ch * sim.height * sim.width;
+    if (d.img_off < 0 || d.img_off + int64_t(sim.height) * sim.width > a.image_elems) return false;
     d.W = sim.width;
     return true;
 }

@@ -63,6 +63,7 @@ struct TileArgs {
     uint32_t* queue;             // chunk work counter of the tile kernel (zeroed before launch)
     float* out;                  // forward: flat image buffer (zeroed by caller)
     const float* grad;           // backward: flat upstream gradient buffer
+    int64_t image_elems;         // elements of out / grad: image planes past it are not touched
     float* gE;                   // backward outputs
     float* gX;
     float* gM;

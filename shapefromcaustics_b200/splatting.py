@@ -266,7 +266,8 @@ class BatchedSplat:
         with torch.cuda.device(self.device):
             check(lib().pds_batch_backward_planned_f32(_ptr(grad_flat),
                                                        *(_ptr(t) for t in self.inputs),
-                                                       *self._common(), self.mpr, _ptr(gE),
+                                                       *self._common(), self.image_elems,
+                                                       self.mpr, _ptr(gE),
                                                        _ptr(gx), _ptr(gM), _ptr(self.ws),
                                                        self.ws.numel(), ctypes.byref(self.cfg),
                                                        _stream(self.device)))

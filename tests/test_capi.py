@@ -66,11 +66,13 @@ def test_batch_layout_on_host():
     lib = _lib.lib()
     t = (_lib.PdsSim * 3)()
     shapes = [(1, 512, 512), (2, 100, 70), (1, 16, 16)]
-    b = 0
+    b = off = 0
     for k, (c, h, w) in enumerate(shapes):
         t[k].photon_begin, t[k].n_photons = b, 10 + k
         t[k].channels, t[k].height, t[k].width = c, h, w
+        t[k].image_offset = off
         b += 10 + k
+        off += c * h * w
     nt = ctypes.c_int64()
     cfg = _lib.config(tile=32)
     _lib.check(lib.pds_batch_layout(t, 3, ctypes.byref(cfg), ctypes.byref(nt)))
@@ -81,3 +83,30 @@ def test_batch_layout_on_host():
     t[1].photon_begin = 3  # not contiguous
     with pytest.raises(_lib.PdsError):
         _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))
+
+
+def test_batch_image_ranges_are_checked_on_host():
+    lib = _lib.lib()
+    t = (_lib.PdsSim * 3)()
+    for k in range(3):
+        t[k].photon_begin, t[k].n_photons = 5 * k, 5
+        t[k].channels, t[k].height, t[k].width = 1, 32, 32
+    # all three summed into one image
+    n = ctypes.c_int64()
+    _lib.check(lib.pds_batch_image_elems(t, 3, ctypes.byref(n)))
+    assert n.value == 32 * 32
+    # separate images with a gap
+    t[1].image_offset, t[2].image_offset = 1024, 4096
+    _lib.check(lib.pds_batch_image_elems(t, 3, ctypes.byref(n)))
+    assert n.value == 4096 + 1024
+    nt = ctypes.c_int64()
+    _lib.check(lib.pds_batch_layout(t, 3, None, ctypes.byref(nt)))
+    # a range that overlaps another without being the same image
+    t[2].image_offset = 1500
+    for call in (lambda: lib.pds_batch_image_elems(t, 3, ctypes.byref(n)),
+                 lambda: lib.pds_batch_layout(t, 3, None, ctypes.byref(nt))):
+        with pytest.raises(_lib.PdsError, match="overlap"):
+            _lib.check(call())
+    t[2].image_offset = -1
+    with pytest.raises(_lib.PdsError, match="negative"):
+        _lib.check(lib.pds_batch_image_elems(t, 3, ctypes.byref(n)))
