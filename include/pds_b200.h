@@ -223,6 +223,26 @@ int pds_refract_backward_f32(const float* height, int32_t rows, int32_t cols,
                              const float* grad_xp, const float* grad_Mp, float* grad_height,
                              void* stream);
 
+/* The two calls above for a batch of simulations that share one height field but each have
+ * their own plate parameters (light direction, refractive index for its wavelength, initial
+ * differential length, receiver), in one launch: simulation k holds the photons
+ * begins_dev[k] .. begins_dev[k + 1] - 1 (the last ends at n_photons; begins_dev[0] = 0,
+ * ascending) and uses plates_dev[k]; both tables live in device memory. The reference runs
+ * its simulations, each with its own light sample and wavelengths, one after another
+ * (shape_from_caustics.py:351-353). Every plate must have the field's texel. */
+int pds_batch_refract_forward_f32(const float* height, int32_t rows, int32_t cols,
+                                  const pds_plate* plates_dev, const int64_t* begins_dev,
+                                  int32_t n_sims, const float* px, const float* py,
+                                  const float* flux, const int64_t* channel, int64_t n_photons,
+                                  float* Ep, float* xp, float* Mp, int64_t* cp, float* radius,
+                                  void* stream);
+int pds_batch_refract_backward_f32(const float* height, int32_t rows, int32_t cols,
+                                   const pds_plate* plates_dev, const int64_t* begins_dev,
+                                   int32_t n_sims, const float* px, const float* py,
+                                   const float* flux, int64_t n_photons, const float* grad_Ep,
+                                   const float* grad_xp, const float* grad_Mp,
+                                   float* grad_height, void* stream);
+
 /* Entry points of rows * cols * per_texel photons (per_texel per texel of a rows x cols
  * height field of edge `texel`, centred on the origin), each jittered uniformly inside its
  * texel (the reference's per-pixel random surface samples, model/caustics.py:78-83):

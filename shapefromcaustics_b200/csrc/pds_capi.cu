@@ -573,7 +573,8 @@ int pds_refract_forward_f32(const float* h, int32_t rows, int32_t cols, const pd
     if (rc) return rc;
     if (n > 0 && (!Ep || !xp || !Mp || !cp || !radius))
         return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
-    cudaError_t e = pds::launch_refract(false, h, rows, cols, *plate, px, py, flux, channel, n, Ep,
+    cudaError_t e = pds::launch_refract(false, h, rows, cols, *plate, nullptr, nullptr, 0, px, py,
+                                        flux, channel, n, Ep,
                                         xp, Mp, cp, radius, nullptr, nullptr, nullptr, nullptr,
                                         static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "refract_fwd_kernel");
@@ -588,10 +589,58 @@ int pds_refract_backward_f32(const float* h, int32_t rows, int32_t cols, const p
     if (rc) return rc;
     if (n > 0 && (!gE || !gX || !gM || !gh))
         return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
-    cudaError_t e = pds::launch_refract(true, h, rows, cols, *plate, px, py, flux, nullptr, n,
+    cudaError_t e = pds::launch_refract(true, h, rows, cols, *plate, nullptr, nullptr, 0, px, py,
+                                        flux, nullptr, n,
                                         nullptr, nullptr, nullptr, nullptr, nullptr, gE, gX, gM,
                                         gh, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel");
+    return PDS_OK;
+}
+
+int pds_batch_refract_forward_f32(const float* h, int32_t rows, int32_t cols,
+                                  const pds_plate* plates_dev, const int64_t* begins_dev,
+                                  int32_t n_sims, const float* px, const float* py,
+                                  const float* flux, const int64_t* channel, int64_t n,
+                                  float* Ep, float* xp, float* Mp, int64_t* cp, float* radius,
+                                  void* stream) {
+    if (!plates_dev || !begins_dev || n_sims < 1)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null or empty plate table");
+    if (rows < 1 || cols < 1 || !h) return fail(PDS_ERR_INVALID_ARGUMENT, "empty height field");
+    if (n < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative photon count");
+    if (n > 0 && (!px || !py || !flux)) return fail(PDS_ERR_INVALID_ARGUMENT, "null photon array");
+    if (n > 0 && (!Ep || !xp || !Mp || !cp || !radius))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null output array");
+    pds_plate unused;
+    std::memset(&unused, 0, sizeof(unused));
+    unused.receiver_half = 1.f;
+    cudaError_t e = pds::launch_refract(false, h, rows, cols, unused, plates_dev, begins_dev,
+                                        n_sims, px, py, flux, channel, n, Ep, xp, Mp, cp, radius,
+                                        nullptr, nullptr, nullptr, nullptr,
+                                        static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "refract_fwd_kernel (batch)");
+    return PDS_OK;
+}
+
+int pds_batch_refract_backward_f32(const float* h, int32_t rows, int32_t cols,
+                                   const pds_plate* plates_dev, const int64_t* begins_dev,
+                                   int32_t n_sims, const float* px, const float* py,
+                                   const float* flux, int64_t n, const float* gE, const float* gX,
+                                   const float* gM, float* gh, void* stream) {
+    if (!plates_dev || !begins_dev || n_sims < 1)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null or empty plate table");
+    if (rows < 1 || cols < 1 || !h) return fail(PDS_ERR_INVALID_ARGUMENT, "empty height field");
+    if (n < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative photon count");
+    if (n > 0 && (!px || !py || !flux)) return fail(PDS_ERR_INVALID_ARGUMENT, "null photon array");
+    if (n > 0 && (!gE || !gX || !gM || !gh))
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
+    pds_plate unused;
+    std::memset(&unused, 0, sizeof(unused));
+    unused.receiver_half = 1.f;
+    cudaError_t e = pds::launch_refract(true, h, rows, cols, unused, plates_dev, begins_dev,
+                                        n_sims, px, py, flux, nullptr, n, nullptr, nullptr,
+                                        nullptr, nullptr, nullptr, gE, gX, gM, gh,
+                                        static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel (batch)");
     return PDS_OK;
 }
 

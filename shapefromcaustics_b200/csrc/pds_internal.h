@@ -21,6 +21,7 @@ void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st);
 
 // refraction to the receiver (pds_refract.cu)
 cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
+                           const pds_plate* plates, const int64_t* begins, int32_t n_sims,
                            const float* px, const float* py, const float* flux,
                            const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
                            int64_t* cp, float* radius, const float* gE, const float* gX,

@@ -115,6 +115,19 @@ struct PlateParams {
     float lx, ly, lz;  // light direction
 };
 
+__host__ __device__ __forceinline__ PlateParams to_params(const pds_plate& p) {
+    PlateParams q;
+    q.texel = p.texel;
+    q.ior = p.ior;
+    q.dist = p.receiver_distance;
+    q.inv_half = 1.f / p.receiver_half;
+    q.du0 = p.du0;
+    q.lx = p.light_dir[0];
+    q.ly = p.light_dir[1];
+    q.lz = p.light_dir[2];
+    return q;
+}
+
 // Snell refraction of direction d and its differential Dd at unit normal n facing the
 // incident side (d.n < 0), with normal derivative dn (model/caustics.py:176-189).
 template <class T>
@@ -277,6 +290,10 @@ struct RefractArgs {
     const float* h;
     int H, W;
     PlateParams P;
+    // batches: simulation k (photons begins[k] .. begins[k + 1] - 1) uses plates[k]; NULL: P
+    const pds_plate* plates;
+    const int64_t* begins;
+    int32_t n_sims;
     const float* px;
     const float* py;
     const float* flux;
@@ -295,16 +312,29 @@ struct RefractArgs {
     float* gh;
 };
 
+// The plate of photon i: its simulation's in a batch (photons of a simulation are
+// contiguous; bisection over the simulations' first photons), else the call's.
+__device__ __forceinline__ PlateParams photon_params(const RefractArgs& a, int64_t i) {
+    if (!a.plates) return a.P;
+    int lo = 0, hi = a.n_sims - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(a.begins + mid) <= i) lo = mid; else hi = mid - 1;
+    }
+    return to_params(a.plates[lo]);
+}
+
 __global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
     const int64_t n = a.n;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x) {
         const float px = a.px[i], py = a.py[i];
-        const Bilin b = bilin(px, py, a.P.texel, a.H, a.W);
+        const PlateParams P = photon_params(a, i);
+        const Bilin b = bilin(px, py, P.texel, a.H, a.W);
         float s[K];
-        surface_scalars(a.h, a.H, a.W, a.P.texel, b, s);
+        surface_scalars(a.h, a.H, a.W, P.texel, b, s);
         float xr, yr, Dux, Duy, Dvx, Dvy;
-        plate_chain<float>(s[0], s[1], s[2], s[3], s[4], s[5], s[6], px, py, a.P, xr, yr, Dux,
+        plate_chain<float>(s[0], s[1], s[2], s[3], s[4], s[5], s[6], px, py, P, xr, yr, Dux,
                            Duy, Dvx, Dvy);
         const float den = Dux * Dvy - Duy * Dvx;
         const bool good = den != 0.f;
@@ -380,9 +410,10 @@ __global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x) {
         const float px = a.px[i], py = a.py[i];
-        const Bilin b = bilin(px, py, a.P.texel, a.H, a.W);
+        const PlateParams P = photon_params(a, i);
+        const Bilin b = bilin(px, py, P.texel, a.H, a.W);
         float s[K];
-        surface_scalars(a.h, a.H, a.W, a.P.texel, b, s);
+        surface_scalars(a.h, a.H, a.W, P.texel, b, s);
         Dual v[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -390,7 +421,7 @@ __global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
             v[k].d[k] = 1.f;
         }
         Dual xr, yr, Dux, Duy, Dvx, Dvy;
-        plate_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], px, py, a.P, xr, yr, Dux,
+        plate_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], px, py, P, xr, yr, Dux,
                           Duy, Dvx, Dvy);
         const Dual den = Dux * Dvy - Duy * Dvx;
         if (den.v == 0.f) continue;  // degenerate photon: skipped by the splat, no gradient
@@ -404,7 +435,7 @@ __global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
         float c[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) c[k] = L.d[k];
-        scatter_patch(a.gh, a.H, a.W, a.P.texel, b, c);
+        scatter_patch(a.gh, a.H, a.W, P.texel, b, c);
     }
 }
 
@@ -662,6 +693,7 @@ cudaError_t launch_refract_point(bool backward, const float* h, int H, int W,
 }
 
 cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
+                           const pds_plate* plates, const int64_t* begins, int32_t n_sims,
                            const float* px, const float* py, const float* flux,
                            const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
                            int64_t* cp, float* radius, const float* gE, const float* gX,
@@ -671,14 +703,10 @@ cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pd
     a.h = h;
     a.H = H;
     a.W = W;
-    a.P.texel = plate.texel;
-    a.P.ior = plate.ior;
-    a.P.dist = plate.receiver_distance;
-    a.P.inv_half = 1.f / plate.receiver_half;
-    a.P.du0 = plate.du0;
-    a.P.lx = plate.light_dir[0];
-    a.P.ly = plate.light_dir[1];
-    a.P.lz = plate.light_dir[2];
+    a.P = to_params(plate);
+    a.plates = plates;
+    a.begins = begins;
+    a.n_sims = n_sims;
     a.px = px;
     a.py = py;
     a.flux = flux;

@@ -23,7 +23,7 @@ from .splatting import SplatPlan, _ptr, _stream
 
 __all__ = ["PlateParams", "plate_params", "refract_forward", "refract_backward", "PlateSplat",
            "PointLight", "point_light", "point_light_source", "refract_point_forward",
-           "refract_point_backward", "PointPlateSplat"]
+           "refract_point_backward", "PointPlateSplat", "BatchedPlate", "BatchedPlateSplat"]
 
 
 PlateParams = _lib.PdsPlate
@@ -229,3 +229,100 @@ class PointPlateSplat(torch.autograd.Function):
         gh = refract_point_backward(h, ctx.light, ctx.params, direction, dtheta, dphi, flux, gE,
                                     gX, gM)
         return gh, None, None, None, None, None, None, None, None
+
+
+class BatchedPlate:
+    """Many simulations of one height-field plate in one launch sequence: each simulation has
+    its own photon count, image size and plate parameters (light direction, the refractive
+    index of its wavelength, initial differential length), and all share the height field.
+
+    ``sims`` is a list of ``(n_photons, (C, H, W), pds_plate)``; photons are the simulations'
+    entry points concatenated in order. The forward refracts every photon in one batched launch
+    (``pds_batch_refract_forward_f32``) and splats all simulations through one plan and one
+    forward (``BatchedSplat``); the backward runs the batched splat backward and one batched
+    refraction backward into the height field's gradient (refracted photons recomputed, not
+    stored). The reference runs its simulations one after another and sums them
+    (``shape_from_caustics.py:351-353``); ``images(flat)`` gives the per-simulation images."""
+
+    def __init__(self, sims, max_pixel_radius, device, config=None):
+        from .splatting import BatchedSplat
+        self.device = torch.device(device)
+        self.splat = BatchedSplat([(n, shape) for n, shape, _ in sims], max_pixel_radius,
+                                  self.device, config=config)
+        n_sims = len(sims)
+        table = (PlateParams * n_sims)()
+        begins = []
+        b = 0
+        for k, (n, _, p) in enumerate(sims):
+            ctypes.memmove(ctypes.byref(table, k * ctypes.sizeof(PlateParams)), ctypes.byref(p),
+                           ctypes.sizeof(PlateParams))
+            begins.append(b)
+            b += int(n)
+        self.n_sims = n_sims
+        self.n_total = b
+        self.plates_dev = torch.frombuffer(bytearray(bytes(table)), dtype=torch.uint8).to(
+            self.device)
+        self.begins_dev = torch.tensor(begins, dtype=torch.int64, device=self.device)
+        self.image_elems = self.splat.image_elems
+
+    def _inputs(self, height, px, py, flux):
+        n = self.n_total
+        if px.numel() != n or py.numel() != n or flux.numel() != n:
+            raise RuntimeError(f"batch expects {n} photons")
+        for t, nm in ((height, "height"), (px, "px"), (py, "py"), (flux, "flux")):
+            _check_f32(t, nm)
+        dev = self.device
+        Ep = torch.empty(n, device=dev)
+        xp = torch.empty((2, n), device=dev)
+        Mp = torch.empty((2, 3, n), device=dev)
+        cp = torch.empty((1, n), dtype=torch.int64, device=dev)
+        radius = torch.empty(n, device=dev)
+        with torch.cuda.device(dev):
+            check(_fn("pds_batch_refract_forward_f32")(
+                _ptr(height), height.shape[0], height.shape[1], _ptr(self.plates_dev),
+                _ptr(self.begins_dev), self.n_sims, _ptr(px), _ptr(py), _ptr(flux), None, n,
+                _ptr(Ep), _ptr(xp), _ptr(Mp), _ptr(cp), _ptr(radius), _stream(dev)))
+        return Ep, xp, Mp, cp, radius
+
+    def forward(self, height, px, py, flux, out=None):
+        """Flat images of all simulations (plans the splat; keeps the plan for backward)."""
+        inputs = self._inputs(height, px, py, flux)
+        self.splat.plan(*inputs)
+        return self.splat.forward(out)
+
+    def backward(self, height, px, py, flux, grad_flat, grad_height=None):
+        """Adds d L / d height for the flat images' gradient (after ``forward`` on the same
+        height field and photons)."""
+        inputs = self._inputs(height, px, py, flux)
+        self.splat.inputs = inputs
+        gE, gX, gM = self.splat.backward(grad_flat)
+        if grad_height is None:
+            grad_height = torch.zeros_like(height)
+        with torch.cuda.device(self.device):
+            check(_fn("pds_batch_refract_backward_f32")(
+                _ptr(height), height.shape[0], height.shape[1], _ptr(self.plates_dev),
+                _ptr(self.begins_dev), self.n_sims, _ptr(px), _ptr(py), _ptr(flux),
+                self.n_total, _ptr(gE), _ptr(gX), _ptr(gM), _ptr(grad_height),
+                _stream(self.device)))
+        return grad_height
+
+    def images(self, flat):
+        return self.splat.images(flat)
+
+
+class BatchedPlateSplat(torch.autograd.Function):
+    """Flat images of a ``BatchedPlate``'s simulations; differentiable in the height field."""
+
+    @staticmethod
+    def forward(ctx, height, px, py, flux, batch):
+        h = height.detach().contiguous()
+        img = batch.forward(h, px, py, flux)
+        ctx.save_for_backward(h, px, py, flux)
+        ctx.batch = batch
+        return img
+
+    @staticmethod
+    def backward(ctx, grad_flat):
+        h, px, py, flux = ctx.saved_tensors
+        gh = ctx.batch.backward(h, px, py, flux, grad_flat.contiguous())
+        return gh, None, None, None, None

@@ -296,3 +296,52 @@ def test_point_plate_splat_end_to_end_gradient(cuda):
     torch.cuda.synchronize()
     assert rel_l2(img.detach().cpu(), rimg) < 1e-4
     assert rel_l2(hv.grad.cpu(), ref) < 1e-3
+
+
+def plate_batch(n_field=48, seed=7):
+    """Five simulations of one plate, each with its own tilt, wavelength, photon count and
+    image size."""
+    from shapefromcaustics_b200 import plate as PL
+    from shapefromcaustics_b200.landweber import photon_source
+    from shapefromcaustics_b200.scene import fused_silica
+    rng = np.random.default_rng(seed)
+    scene = RF.PlateScene(texel=0.4, receiver_distance=30.0, receiver_half=14.0)
+    h = RF.height_field_bumps(n_field, n_field, seed=seed, bumps=10, base=1.0,
+                              amp=(0.0, 0.05), width=(2.0, 8.0)).float().cuda()
+    sims, photons = [], []
+    offset = 0
+    for k, (per, img) in enumerate([(2, 64), (1, 128), (4, 96), (3, 64), (1, 256)]):
+        th, ph = np.radians(5.0) * rng.random(), 2 * np.pi * rng.random()
+        light = (np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), -np.cos(th))
+        s = RF.PlateScene(texel=0.4, ior=float(fused_silica(0.45 + 0.2 * rng.random())),
+                          receiver_distance=30.0, receiver_half=14.0, light_dir=light)
+        p = PL.plate_params(s, 3.0 * 2.0 * s.receiver_half / img)
+        px, py, offset = photon_source(n_field, n_field, per, s.texel, 11, offset, "cuda")
+        n = px.numel()
+        sims.append((n, (1, img, img), p))
+        photons.append((px, py, torch.full((n,), 1.0 / n, device="cuda")))
+    return h, sims, photons
+
+
+def test_batched_plate_equals_the_per_simulation_plates(cuda):
+    from shapefromcaustics_b200 import plate as PL
+    h, sims, photons = plate_batch()
+    batch = PL.BatchedPlate(sims, 20, "cuda")
+    cat = [torch.cat([p[k] for p in photons]).contiguous() for k in range(3)]
+    hv = h.clone().requires_grad_(True)
+    flat = PL.BatchedPlateSplat.apply(hv, *cat, batch)
+    g = torch.randn(flat.shape, generator=torch.Generator("cuda").manual_seed(3), device="cuda")
+    (flat * g).sum().backward()
+    imgs = batch.images(flat.detach())
+    gsum = torch.zeros_like(h)
+    off = 0
+    for (n, shape, p), (px, py, flux), img in zip(sims, photons, imgs):
+        hs = h.clone().requires_grad_(True)
+        ref = PL.PlateSplat.apply(hs, px, py, flux, p, shape, 20, True)
+        gs = g[off:off + ref.numel()].view(shape)
+        (ref * gs).sum().backward()
+        gsum += hs.grad
+        off += ref.numel()
+        assert rel_l2(img.cpu(), ref.detach().cpu()) < 1e-5
+    torch.cuda.synchronize()
+    assert rel_l2(hv.grad.cpu(), gsum.cpu()) < 1e-5
