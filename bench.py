@@ -512,6 +512,8 @@ def run_ours(args, rank, world, device):
         "parity_batched_vs_plain_relL2": parity_plain,
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1 and not args.no_plate_batch and args.workload == "batch64":
+        result["landweber_plate_batch"] = run_plate_batch(args, device, args.steps, args.warmup)
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         result["reference_gpu"] = reference_gpu_subprocess(args, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -748,6 +750,143 @@ def plate_setup(n_field, image, per_texel, device, seed=0, texel=0.1, dist=50.0)
     return scene, h, t
 
 
+def plate_batch_setup(device, seed=1000, n_sims=64, n_field=256, footprint_px=3.0):
+    """The uneven batch of Landweber simulations: one 256^2 height field (the 256^2 Landweber
+    workload's generator), 64 simulations with the batch's photon counts ~ logU[2^16, 2^22]
+    (rounded to whole photons per texel) and image sizes {256, 512, 1024}^2, each with its own
+    light tilt (up to 5 degrees, uniform azimuth) and wavelength (U[450, 650] nm, the fused
+    silica index at it); initial footprints of footprint_px receiver pixels."""
+    import numpy as np
+    from shapefromcaustics_b200 import plate as PL
+    from shapefromcaustics_b200 import scene as SC
+    scene, h_true, h_tgt = plate_setup(n_field, 512, 4, device, seed=0)
+    rng = np.random.default_rng(seed)
+    specs = S.batch_specs(n_sims, seed=seed)
+    sims, per_texel = [], []
+    for n, shape in specs:
+        per = max(1, int(round(n / float(n_field * n_field))))
+        th, ph = np.radians(5.0) * rng.random(), 2 * np.pi * rng.random()
+        light = (np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), -np.cos(th))
+        lam = 0.45 + 0.2 * rng.random()
+        s = SC.PlateScene(texel=scene.texel, ior=float(SC.fused_silica(lam)),
+                          receiver_distance=scene.receiver_distance,
+                          receiver_half=scene.receiver_half, light_dir=light)
+        p = PL.plate_params(s, footprint_px * 2.0 * s.receiver_half / shape[1])
+        sims.append((per * n_field * n_field, shape, p))
+        per_texel.append(per)
+    return scene, h_true, h_tgt, sims, per_texel
+
+
+def run_plate_batch(args, device, steps, warmup):
+    """One Landweber iteration over the uneven batch of simulations with refraction
+    (plate_batch_setup), batched (one CUDA graph: photon sources, one batched refraction, one
+    splat plan / forward / backward, one batched refraction backward, the fused update) against
+    plain (the reference's per-simulation loop, shape_from_caustics.py:351-353: each
+    simulation's source, refraction, plan, forward, backward and refraction backward launched
+    in turn from Python). -> dict of iterations per second and the batch's size."""
+    from shapefromcaustics_b200 import plate as PL
+    from shapefromcaustics_b200.landweber import LandweberParams, landweber_update, photon_source
+    from shapefromcaustics_b200.splatting import SplatPlan
+    scene, h_true, h_tgt, sims, per_texel = plate_batch_setup(device)
+    nf = h_true.shape[0]
+    batch = PL.BatchedPlate(sims, MPR, device)
+    n_total = batch.n_total
+    px = torch.empty(n_total, device=device)
+    py = torch.empty(n_total, device=device)
+    flux = torch.cat([torch.full((n,), 1.0 / n, device=device) for n, _, _ in sims])
+    views, b = [], 0
+    for n, _, _ in sims:
+        views.append((px[b:b + n], py[b:b + n], flux[b:b + n]))
+        b += n
+
+    def sources(offset0):
+        off = offset0
+        for per, (vx, vy, _) in zip(per_texel, views):
+            _, _, off = photon_source(nf, nf, per, scene.texel, 7, off, device, out=(vx, vy))
+        return off
+
+    sources(0)
+    target = batch.forward(h_tgt.contiguous(), px, py, flux).clone()
+    base = 1.0
+    d = (h_true - base).clone()
+    h = (base + d).contiguous()
+    mask = torch.ones_like(d)
+    vol = float(d.sum())
+    params = LandweberParams(tau=1e-4, d1=0.75 * vol, d2=1.25 * vol)
+    ws = torch.empty(1 << 22, dtype=torch.uint8, device=device)
+    img = torch.empty(batch.image_elems, device=device)
+    gimg = torch.empty_like(img)
+    gh = torch.zeros_like(d)
+
+    def batched_step():
+        sources(0)
+        batch.forward(h, px, py, flux, out=img)
+        torch.sub(img, target, out=gimg)
+        gh.zero_()
+        batch.backward(h, px, py, flux, gimg, grad_height=gh)
+        landweber_update(d, gh, mask, params, ws)
+        torch.add(d, base, out=h)
+
+    t_views = batch.images(target)
+
+    def plain_step():
+        gh.zero_()
+        off = 0
+        for k, ((n, shape, p), per, (vx, vy, vf)) in enumerate(zip(sims, per_texel, views)):
+            _, _, off = photon_source(nf, nf, per, scene.texel, 7, off, device, out=(vx, vy))
+            inputs = PL.refract_forward(h, vx, vy, vf, p)
+            plan = SplatPlan(*inputs, shape, MPR)
+            g = plan.forward() - t_views[k]
+            inputs = PL.refract_forward(h, vx, vy, vf, p)
+            plan.inputs = inputs
+            gE, gX, gM = plan.backward(g)
+            PL.refract_backward(h, vx, vy, vf, p, gE, gX, gM, grad_height=gh)
+        landweber_update(d, gh, mask, params, ws)
+        torch.add(d, base, out=h)
+
+    stream = torch.cuda.Stream(device)
+    stream.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(stream):
+        for _ in range(max(warmup, 3)):
+            batched_step()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        batched_step()
+    torch.cuda.synchronize()
+    for _ in range(max(warmup, 3)):
+        graph.replay()
+    torch.cuda.synchronize()
+    per = time_graph(graph, steps, stream)
+    ms_b = sum(per) / steps
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            plain_step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        k = max(2, min(steps, 5))
+        e0.record(stream)
+        for _ in range(k):
+            plain_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_p = e0.elapsed_time(e1) / k
+    del graph
+    return {"batched_it_per_s": 1e3 / ms_b, "plain_it_per_s": 1e3 / ms_p,
+            "batched_over_plain": ms_p / ms_b, "batched_ms": ms_b, "plain_ms": ms_p,
+            "photons_per_iteration": n_total, "simulations": len(sims),
+            "workload": "uneven batch with refraction: 256^2 height field, 64 simulations, "
+                        "N_i ~ logU[2^16, 2^22] (whole photons per texel), images "
+                        "{256,512,1024}^2, light tilt <= 5 deg, wavelength U[450,650] nm "
+                        "(fused silica), 3-pixel footprints; one Landweber iteration "
+                        "(sources, refraction, splat, backward, update)",
+            "batched": "one CUDA graph: 64 source launches, one batched refraction, one plan / "
+                       "forward / backward, one batched refraction backward, the update",
+            "plain": "per simulation from Python: source, refraction, plan, forward, "
+                     "refraction (recomputed), backward, refraction backward; then the update"}
+
+
 def run_landweber_step(args, rank, world, device):
     """One Landweber iteration on a 256^2 field, 4 photons per texel (262,144), 512^2
     image: refraction + splat forward, L2 discrepancy against a target rendered from a second
@@ -861,6 +1000,8 @@ def main():
                     choices=["batch64", "uniform1m", "medium", "contention", "contention24",
                              "landweber256", "recon1024"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plate-batch", action="store_true",
+                    help="skip the batched-vs-plain Landweber iteration with refraction")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the reference CUDA extension's run on the same workload")
     ap.add_argument("--no-autotune", action="store_true",

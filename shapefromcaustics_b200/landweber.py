@@ -67,14 +67,20 @@ def render_plate(height, scene, px, py, flux, params, shape, max_pixel_radius=20
         return PlateSplat.apply(height, px, py, flux, params, shape, max_pixel_radius, False)
 
 
-def photon_source(H, W, per_texel, texel, seed, offset, device):
+def photon_source(H, W, per_texel, texel, seed, offset, device, out=None):
     """Entry points of ``per_texel`` uniformly jittered photons per texel from the device
     source (``pds_photon_source_f32``: Philox4x32-10 keyed by ``seed``, counter blocks from
     ``offset``, two photons a block). Returns ``(px, py, next_offset)``; passing
-    ``next_offset`` to the next call draws a disjoint stream."""
+    ``next_offset`` to the next call draws a disjoint stream. ``out``: optional ``(px, py)``
+    float32 device tensors of ``H * W * per_texel`` elements to write into."""
     n = H * W * per_texel
-    px = torch.empty(n, dtype=torch.float32, device=device)
-    py = torch.empty(n, dtype=torch.float32, device=device)
+    if out is not None:
+        px, py = out
+        if px.numel() != n or py.numel() != n:
+            raise RuntimeError(f"out must hold {n} photons")
+    else:
+        px = torch.empty(n, dtype=torch.float32, device=device)
+        py = torch.empty(n, dtype=torch.float32, device=device)
     with torch.cuda.device(px.device):
         check(lib().pds_photon_source_f32(H, W, per_texel, float(texel), int(seed) & (2 ** 64 - 1),
                                           int(offset), _ptr(px), _ptr(py), _stream(px.device)))

@@ -53,3 +53,15 @@ def test_bench_line_carries_every_key(cuda):
     # the reference's own CUDA extension on the same workload (when it is built)
     rg = r["reference_gpu"]
     assert "unavailable" in rg or (rg["value"] > 0 and rg["ours_over_reference_gpu"] > 0)
+
+
+def test_plate_batch_iteration_runs_batched_and_plain(cuda):
+    """The batched-vs-plain Landweber iteration with refraction that the benchmark line carries
+    (64 simulations with their own tilt, wavelength, photon count and image size)."""
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    r = bench.run_plate_batch(None, torch.device("cuda:0"), 2, 1)
+    assert r["simulations"] == 64 and r["photons_per_iteration"] > 2 ** 24
+    assert r["batched_it_per_s"] > 0 and r["plain_it_per_s"] > 0
+    assert r["batched_over_plain"] > 1.0
