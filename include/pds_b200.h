@@ -343,13 +343,6 @@ int pds_landweber_update_noalloc_f32(float* d, const float* grad, const float* m
                                      int64_t rows, int64_t cols, const pds_landweber* params,
                                      void* stream);
 
-/* ---- device radix sort (exposed for its bit-exactness tests) ----------------------- */
-/* Stable ascending sort of keys[n] (only the low key_bits bits are compared) carrying the
- * original index: perm_out[k] = index of the k-th smallest key, keys_out the sorted keys. */
-size_t pds_sort_workspace_bytes(int64_t n);
-int pds_sort_u32(const uint32_t* keys, int64_t n, int32_t key_bits, uint32_t* keys_out,
-                 uint32_t* perm_out, void* workspace, size_t workspace_bytes, void* stream);
-
 #ifdef __cplusplus
 }
 #endif

@@ -48,8 +48,6 @@ def lib():
         l.pds_oracle_backward.restype = None
         l.pds_oracle_footprints.argtypes = [p, p, p, i64, i64, i64, i64, i32, p, p]
         l.pds_oracle_footprints.restype = None
-        l.pds_oracle_stable_sort_u32.argtypes = [p, i64, p]
-        l.pds_oracle_stable_sort_u32.restype = None
         _lib = l
     return _lib
 
@@ -110,11 +108,3 @@ def footprints(xp, cp, radius, output_size, max_pixel_radius):
     lib().pds_oracle_footprints(_ptr(X), _ptr(C), _ptr(R), N, nc, h, w, int(max_pixel_radius),
                                 _ptr(out5), _ptr(box))
     return out5, box
-
-
-def stable_sort_u32(keys):
-    """Stable ascending order of uint32 keys (the CPU sort the device sort must equal)."""
-    k = np.ascontiguousarray(np.asarray(keys, dtype=np.uint32))
-    perm = np.empty(k.shape[0], dtype=np.int64)
-    lib().pds_oracle_stable_sort_u32(_ptr(k), k.shape[0], _ptr(perm))
-    return perm

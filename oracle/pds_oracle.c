@@ -318,21 +318,3 @@ void pds_oracle_footprints(const double* X, const int64_t* cp, const double* R, 
         box_pixels[i] = n;
     }
 }
-
-/* Stable LSD ordering check helper: counting sort of 32-bit keys (stable), the CPU sort the
- * device radix sort is compared with bit for bit. perm[k] = index of the k-th smallest. */
-void pds_oracle_stable_sort_u32(const uint32_t* keys, int64_t n, int64_t* perm) {
-    int64_t* tmp = (int64_t*)malloc((size_t)(n > 0 ? n : 1) * sizeof(int64_t));
-    int64_t* cnt = (int64_t*)malloc(65537 * sizeof(int64_t));
-    for (int64_t i = 0; i < n; ++i) perm[i] = i;
-    for (int pass = 0; pass < 2; ++pass) {
-        const int shift = 16 * pass;
-        memset(cnt, 0, 65537 * sizeof(int64_t));
-        for (int64_t i = 0; i < n; ++i) cnt[((keys[perm[i]] >> shift) & 0xFFFF) + 1]++;
-        for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
-        for (int64_t i = 0; i < n; ++i) tmp[cnt[(keys[perm[i]] >> shift) & 0xFFFF]++] = perm[i];
-        memcpy(perm, tmp, (size_t)n * sizeof(int64_t));
-    }
-    free(tmp);
-    free(cnt);
-}

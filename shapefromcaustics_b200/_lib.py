@@ -117,8 +117,6 @@ SIGNATURES = {
     "pds_landweber_update_noalloc_f32": (ctypes.c_int, [_P, _P, _P, _I64, _I64,
                                                         ctypes.POINTER(PdsLandweber), _P]),
     "pds_plan_export": (ctypes.c_int, [_P, _SZ, _I64, _I64, _I32, _CFG, _P, _P, _P]),
-    "pds_sort_workspace_bytes": (_SZ, [_I64]),
-    "pds_sort_u32": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P, _SZ, _P]),
 }
 
 _lib = None

@@ -795,39 +795,4 @@ int pds_plan_export(const void* ws, size_t ws_bytes, int64_t n, int64_t n_tiles,
     return PDS_OK;
 }
 
-size_t pds_sort_workspace_bytes(int64_t n) {
-    const size_t nn = size_t(n > 0 ? n : 1);
-    return 2 * pds::align_up(nn * 4, 256) + pds::sort_aux_bytes(n);
-}
-
-int pds_sort_u32(const uint32_t* keys, int64_t n, int32_t key_bits, uint32_t* keys_out,
-                 uint32_t* perm_out, void* ws, size_t ws_bytes, void* stream) {
-    if (n < 0 || n >= int64_t(0xFFFFFFFFll))
-        return fail(PDS_ERR_INVALID_ARGUMENT, "sort size outside [0, 2^32 - 1)");
-    if (key_bits < 0 || key_bits > 32)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "key_bits outside [0, 32]");
-    if (n == 0) return PDS_OK;
-    if (!keys || !keys_out || !perm_out)
-        return fail(PDS_ERR_INVALID_ARGUMENT, "null sort array");
-    int rc = check_ws(ws, ws_bytes, pds_sort_workspace_bytes(n));
-    if (rc) return rc;
-    const size_t nn = size_t(n);
-    char* b = static_cast<char*>(ws);
-    uint32_t* kt = reinterpret_cast<uint32_t*>(b);
-    uint32_t* vt = reinterpret_cast<uint32_t*>(b + pds::align_up(nn * 4, 256));
-    void* aux = b + 2 * pds::align_up(nn * 4, 256);
-    const int passes = pds::sort_passes(key_bits);
-    // the last pass must land in the caller's buffers
-    const bool last_in0 = passes == 0 || ((passes - 1) & 1) == 0;
-    uint32_t* k0 = last_in0 ? keys_out : kt;
-    uint32_t* k1 = last_in0 ? kt : keys_out;
-    uint32_t* v0 = last_in0 ? perm_out : vt;
-    uint32_t* v1 = last_in0 ? vt : perm_out;
-    uint32_t *ko, *vo;
-    cudaError_t e = pds::radix_sort(keys, k0, k1, v0, v1, n, key_bits, aux,
-                                    static_cast<cudaStream_t>(stream), &ko, &vo);
-    if (e != cudaSuccess) return cuda_fail(e, "radix sort");
-    return PDS_OK;
-}
-
 }  // extern "C"

@@ -11,14 +11,6 @@ namespace pds {
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// radix sort (pds_sort.cu)
-int sort_passes(int key_bits);
-size_t sort_aux_bytes(int64_t n);
-cudaError_t radix_sort(const uint32_t* keys_in, uint32_t* k0, uint32_t* k1, uint32_t* v0,
-                       uint32_t* v1, int64_t n, int key_bits, void* aux, cudaStream_t st,
-                       uint32_t** keys_out, uint32_t** vals_out);
-void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st);
-
 // refraction to the receiver (pds_refract.cu)
 cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
                            const pds_plate* plates, const int64_t* begins, int32_t n_sims,

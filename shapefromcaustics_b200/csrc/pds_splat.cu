@@ -1264,11 +1264,6 @@ __global__ __launch_bounds__(256) void grad_scatter4_kernel(TileArgs a) {
     }
 }
 
-__global__ void iota_kernel(uint32_t* dst, int64_t n) {
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * blockDim.x)
-        dst[i] = uint32_t(i);
-}
 
 constexpr int kTileThreads = 256;
 
@@ -1298,11 +1293,6 @@ cudaError_t set_smem(K kernel, size_t smem) {
 
 }  // namespace
 
-void iota_u32(uint32_t* dst, int64_t n, cudaStream_t st) {
-    if (n <= 0) return;
-    const int64_t blocks = (n + 255) / 256;
-    iota_kernel<<<unsigned(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(dst, n);
-}
 
 template <int MINB, bool ROWS>
 cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {

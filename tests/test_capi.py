@@ -26,7 +26,7 @@ def declared_functions():
 def test_header_declares_the_entry_points():
     names = declared_functions()
     for n in ("pds_forward_f32", "pds_backward_f32", "pds_plan_f32", "pds_batch_layout",
-              "pds_sort_u32", "pds_last_error", "pds_workspace_bytes"):
+              "pds_plan_export", "pds_last_error", "pds_workspace_bytes"):
         assert n in names
 
 
@@ -58,8 +58,10 @@ def test_argument_errors_without_a_device():
     assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"positive" in lib.pds_last_error()
     rc = lib.pds_plan_f32(p, p, p, p, p, 5, 1, 8, 8, 20, p, 10, None, None)
     assert rc == _lib.PDS_ERR_WORKSPACE
-    rc = lib.pds_sort_u32(p, 10, 40, p, p, p, 1 << 20, None)
-    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT
+    rc = lib.pds_plan_export(p, 10, 5, 1, 20, None, p, p, None)
+    assert rc == _lib.PDS_ERR_WORKSPACE
+    rc = lib.pds_plan_export(p, 1 << 20, 5, 1, 20, None, None, None, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"null" in lib.pds_last_error()
 
 
 def test_batch_layout_on_host():

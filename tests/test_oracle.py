@@ -159,11 +159,6 @@ def test_ref32_and_fp64_agree_to_float_precision():
     assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-4
 
 
-def test_oracle_stable_sort_matches_numpy():
-    rng = np.random.default_rng(1)
-    keys = rng.integers(0, 300, 10000).astype(np.uint32)
-    assert np.array_equal(O.stable_sort_u32(keys), np.argsort(keys, kind="stable"))
-
 
 def test_philox_known_answers():
     """The numpy Philox4x32-10 (checker of the device photon source) against the published
