@@ -76,41 +76,48 @@ __global__ __launch_bounds__(256) void source_kernel(int32_t rows, int32_t cols,
 // back (sbt_angle.item(), caustics.py:60); here every thread computes it from the light's
 // parameters, so nothing waits on the host.
 
-struct V3f {
-    float x, y, z;
+// The directions and their bases are formed in double: the basis divides by 1 + d_z, which
+// cancels for near-vertical directions (about 7e-4 for a light 10 units above a unit plate),
+// so a float32 direction would carry ~1e-4 relative error into the differentials. Each photon
+// costs a few hundred double operations once per simulation, outside the splat's hot path.
+struct V3d {
+    double x, y, z;
 };
-__device__ __forceinline__ V3f v3(float x, float y, float z) { return {x, y, z}; }
-__device__ __forceinline__ float dot3(V3f a, V3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ V3f cross3(V3f a, V3f b) {
+__device__ __forceinline__ V3d v3(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ double dot3(V3d a, V3d b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3d cross3(V3d a, V3d b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
-__device__ __forceinline__ V3f scale3(float s, V3f a) { return {s * a.x, s * a.y, s * a.z}; }
-__device__ __forceinline__ V3f add3(V3f a, V3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ V3f sub3(V3f a, V3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ float norm3(V3f a) { return sqrtf(dot3(a, a)); }
-__device__ __forceinline__ V3f unit3(V3f a) {
-    const float n = norm3(a);
-    return n > 0.f ? scale3(1.f / n, a) : a;
+__device__ __forceinline__ V3d scale3(double s, V3d a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ V3d add3(V3d a, V3d b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3d sub3(V3d a, V3d b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ double norm3(V3d a) { return sqrt(dot3(a, a)); }
+__device__ __forceinline__ V3d unit3(V3d a) {
+    const double n = norm3(a);
+    return n > 0.0 ? scale3(1.0 / n, a) : a;
 }
 
 // slerp(p0, p1, t) = (sin((1 - t) w) p0 + sin(t w) p1) / sin(w), w = acos(clamp(p0.p1))
-__device__ __forceinline__ V3f slerp3(V3f p0, V3f p1, float t) {
-    const float w = acosf(fminf(fmaxf(dot3(p0, p1), -1.f), 1.f));
-    const float s = sinf(w);
-    return scale3(1.f / s, add3(scale3(sinf((1.f - t) * w), p0), scale3(sinf(t * w), p1)));
+__device__ __forceinline__ V3d slerp3(V3d p0, V3d p1, double t) {
+    const double w = acos(fmin(fmax(dot3(p0, p1), -1.0), 1.0));
+    const double s = sin(w);
+    return scale3(1.0 / s, add3(scale3(sin((1.0 - t) * w), p0), scale3(sin(t * w), p1)));
 }
 
 // Solid angle of triangle (v0, v1, v2) seen from o: 2 atan2(d0.(d2 x d1), |d0||d1||d2| +
 // |d0| d1.d2 + |d1| d0.d2 + |d2| d0.d1), negative values counted as zero (as the reference
 // sums relu of the per-triangle angles).
-__device__ __forceinline__ float tri_angle(V3f o, V3f v0, V3f v1, V3f v2) {
-    const V3f d0 = sub3(v0, o), d1 = sub3(v1, o), d2 = sub3(v2, o);
-    const float n0 = norm3(d0), n1 = norm3(d1), n2 = norm3(d2);
-    const float num = dot3(d0, cross3(d2, d1));
-    const float den = n0 * n1 * n2 + n0 * dot3(d1, d2) + n1 * dot3(d0, d2) + n2 * dot3(d0, d1);
-    const float a = (num == 0.f && den == 0.f) ? 0.f : 2.f * atan2f(num, den);
-    return fmaxf(a, 0.f);
+__device__ __forceinline__ double tri_angle(V3d o, V3d v0, V3d v1, V3d v2) {
+    const V3d d0 = sub3(v0, o), d1 = sub3(v1, o), d2 = sub3(v2, o);
+    const double n0 = norm3(d0), n1 = norm3(d1), n2 = norm3(d2);
+    const double num = dot3(d0, cross3(d2, d1));
+    const double den = n0 * n1 * n2 + n0 * dot3(d1, d2) + n1 * dot3(d0, d2) + n2 * dot3(d0, d1);
+    const double a = (num == 0.0 && den == 0.0) ? 0.0 : 2.0 * atan2(num, den);
+    return fmax(a, 0.0);
 }
+
+// [0, 1) from the top 24 bits, in double (exact)
+__device__ __forceinline__ double unit24d(uint32_t u) { return double(u >> 8) * (1.0 / 16777216.0); }
 
 __global__ __launch_bounds__(256) void point_light_kernel(pds_point_light L, int64_t n_dir,
                                                           uint64_t seed, uint64_t offset,
@@ -119,16 +126,15 @@ __global__ __launch_bounds__(256) void point_light_kernel(pds_point_light L, int
                                                           float* __restrict__ dth,
                                                           float* __restrict__ dph,
                                                           float* __restrict__ flux) {
-    const V3f o = v3(L.position[0], L.position[1], L.position[2]);
-    const V3f p00 = v3(L.xmin, L.ymin, L.plane_z), p10 = v3(L.xmax, L.ymin, L.plane_z);
-    const V3f p01 = v3(L.xmin, L.ymax, L.plane_z), p11 = v3(L.xmax, L.ymax, L.plane_z);
-    const V3f c00 = unit3(sub3(p00, o)), c10 = unit3(sub3(p10, o));
-    const V3f c01 = unit3(sub3(p01, o)), c11 = unit3(sub3(p11, o));
-    const float omega = tri_angle(o, p00, p10, p01) + tri_angle(o, p01, p10, p11);
+    const V3d o = v3(L.position[0], L.position[1], L.position[2]);
+    const V3d p00 = v3(L.xmin, L.ymin, L.plane_z), p10 = v3(L.xmax, L.ymin, L.plane_z);
+    const V3d p01 = v3(L.xmin, L.ymax, L.plane_z), p11 = v3(L.xmax, L.ymax, L.plane_z);
+    const V3d c00 = unit3(sub3(p00, o)), c10 = unit3(sub3(p10, o));
+    const V3d c01 = unit3(sub3(p01, o)), c11 = unit3(sub3(p11, o));
+    const double omega = tri_angle(o, p00, p10, p01) + tri_angle(o, p01, p10, p11);
     const int wl = L.wavelengths;
     const double total = double(n_dir) * double(L.simulations) * double(wl);
-    const float scale = float(2.0 * double(L.smoothing) *
-                              sqrt(double(omega) / (3.141592653589793 * total)));
+    const double scale = 2.0 * double(L.smoothing) * sqrt(omega / (3.141592653589793 * total));
     const float f = L.energy / float(int64_t(L.simulations) * L.inner);
     const int64_t n = n_dir * wl;
     const int64_t pairs = (n_dir + 1) >> 1;
@@ -144,25 +150,27 @@ __global__ __launch_bounds__(256) void point_light_kernel(pds_point_light L, int
         for (int h = 0; h < 2; ++h) {
             const int64_t i = 2 * k + h;
             if (i >= n_dir) break;
-            const float u0 = coeffs ? coeffs[i] : unit24(h ? r.z : r.x);
-            const float u1 = coeffs ? coeffs[n_dir + i] : unit24(h ? r.w : r.y);
-            const V3f lower = slerp3(c00, c10, u0), upper = slerp3(c01, c11, u0);
-            const V3f d = slerp3(lower, upper, u1);
-            V3f b1, b2;
-            if (d.z < -1.f + 1e-5f) {
-                b1 = v3(0.f, -1.f, 0.f);
-                b2 = v3(-1.f, 0.f, 0.f);
+            const double u0 = coeffs ? double(coeffs[i]) : unit24d(h ? r.z : r.x);
+            const double u1 = coeffs ? double(coeffs[n_dir + i]) : unit24d(h ? r.w : r.y);
+            const V3d lower = slerp3(c00, c10, u0), upper = slerp3(c01, c11, u0);
+            const V3d d = slerp3(lower, upper, u1);
+            V3d b1, b2;
+            if (d.z < -1.0 + 1e-5) {
+                b1 = v3(0.0, -1.0, 0.0);
+                b2 = v3(-1.0, 0.0, 0.0);
             } else {
-                const float a = 1.f / (1.f + d.z);
-                const float b = -d.x * d.y * a;
-                b1 = v3(1.f - a * d.x * d.x, b, -d.x);
-                b2 = v3(b, 1.f - a * d.y * d.y, -d.y);
+                const double a = 1.0 / (1.0 + d.z);
+                const double b = -d.x * d.y * a;
+                b1 = v3(1.0 - a * d.x * d.x, b, -d.x);
+                b2 = v3(b, 1.0 - a * d.y * d.y, -d.y);
             }
             for (int w = 0; w < wl; ++w) {
                 const int64_t j = i * wl + w;
-                dir[j] = d.x; dir[n + j] = d.y; dir[2 * n + j] = d.z;
-                dth[j] = scale * b1.x; dth[n + j] = scale * b1.y; dth[2 * n + j] = scale * b1.z;
-                dph[j] = scale * b2.x; dph[n + j] = scale * b2.y; dph[2 * n + j] = scale * b2.z;
+                dir[j] = float(d.x); dir[n + j] = float(d.y); dir[2 * n + j] = float(d.z);
+                dth[j] = float(scale * b1.x); dth[n + j] = float(scale * b1.y);
+                dth[2 * n + j] = float(scale * b1.z);
+                dph[j] = float(scale * b2.x); dph[n + j] = float(scale * b2.y);
+                dph[2 * n + j] = float(scale * b2.z);
                 flux[j] = f;
             }
         }

@@ -149,7 +149,7 @@ __device__ __forceinline__ void deposit_band(const Rec& r, const Band& bd, const
 // add exactly zero in the reference (value > 0 fails, :106). Photons that fail the
 // reference's image-half-size ellipse test somewhere in their box (tiny images only) take
 // the per-pixel test path.
-__device__ __noinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
+__device__ __forceinline__ void deposit(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                         bool band, float* acc, int& bx0, int& bx1, int& by0,
                                         int& by1) {
     const uint32_t p = r.packed;
@@ -457,7 +457,7 @@ __device__ __forceinline__ void rec_box(const Rec& r, const TileInfo& ti, int& p
 }
 
 // Forward deposit of one photon by the whole warp (see use_coop).
-__device__ __noinline__ void deposit_coop(const Rec& r, const TileInfo& ti, int sw,
+__device__ __forceinline__ void deposit_coop(const Rec& r, const TileInfo& ti, int sw,
                                              uint32_t acc_base, int lane) {
     int pxc, pyc, x0, x1, y0, y1;
     rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
@@ -604,7 +604,7 @@ __device__ __forceinline__ int64_t next_chunk(uint32_t* queue, uint32_t* slot) {
     return int64_t(*slot);
 }
 
-template <int NT, int MINB, bool ROWS>
+template <int NT, int MINB>
 __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     extern __shared__ float acc[];
     __shared__ int sb[4];
@@ -637,22 +637,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
                 const bool mine = have && i >= sg.begin && i < sg.end;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
                 int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
-                if constexpr (ROWS) {
-                    // padded-row walk; photons without a band take the generic walk below
-                    RowGeo g;
-                    int rows = 0;
-                    bool generic = false;
-                    if (mine && !coop && !(rec_flags(r.packed) & kFlagFwdSkip)) {
-                        int pxc, pyc;
-                        rec_clip(r, ti, pxc, pyc, x0, x1, y0, y1);
-                        generic = !prep_rows(r, ti, sw, pxc, pyc, x0, x1, y0, y1, g);
-                        rows = generic ? 0 : g.rows;
-                    }
-                    deposit_rows(g, rows, r.e * kThreeOverPi, acc_base, sw);
-                    if (generic) deposit(r, ti, sw, cfg.spans, false, acc, x0, x1, y0, y1);
-                } else if (mine && !coop) {
-                    deposit(r, ti, sw, cfg.spans, cfg.band, acc, x0, x1, y0, y1);
-                }
+                if (mine && !coop) deposit(r, ti, sw, cfg.spans, cfg.band, acc, x0, x1, y0, y1);
                 if (coop) {
                     int pxc, pyc;
                     rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
@@ -856,7 +841,7 @@ __device__ __forceinline__ BandMoments gather_band_rows(const Band& bd, const Ba
 __device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const TileInfo& ti,
                                             int sw, const float* tg, uint32_t slot, int pxc,
                                             int pyc, int ky0, int ky1, int kxb0, int kxb1,
-                                            const TileArgs& a) {
+                                            GradRec* stage) {
     const float a00 = r.m00 * ti.sx, a10 = r.m10 * ti.sx;
     const float m01sy = r.m01 * ti.sy, m11sy = r.m11 * ti.sy;
     const float c00 = fmaf(r.m00, r.dx0, r.m01 * r.dy0), c10 = fmaf(r.m10, r.dx0, r.m11 * r.dy0);
@@ -869,7 +854,7 @@ __device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const 
     const float Sx = fmaf(ti.sx, m.B1t, r.dx0 * m.A0t);
     const float Sxx = fmaf(ti.sx * ti.sx, m.B2,
                            fmaf(2.f * ti.sx * r.dx0, m.B1t, r.dx0 * r.dx0 * m.A0t));
-    finish_grad(a.stage, slot, r.e, r.m00, r.m01, r.m10, r.m11, m.sE, Sx, m.Sy, Sxx, m.Sxy,
+    finish_grad(stage, slot, r.e, r.m00, r.m01, r.m10, r.m11, m.sE, Sx, m.Sy, Sxx, m.Sxy,
                 m.Syy);
 }
 
@@ -877,9 +862,9 @@ __device__ __forceinline__ void gather_band(const Rec& r, const Band& bd, const 
 // Pixels outside the support contribute 0 * g in the reference; with spans on they are not
 // visited. The offset d of pixel (kx, ky) is (kx sx + dx0, ky sy + dy0); moments in x are
 // kept in the integer offset kx and converted once per photon.
-__device__ __noinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
+__device__ __forceinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bool spans,
                                        bool band, const float* tg, uint32_t rid,
-                                       const TileArgs& a) {
+                                       GradRec* stage) {
     const uint32_t p = r.packed;
     const uint32_t fl = rec_flags(p);
     const int pxc = ti.ox + rec_lx(p), pyc = ti.oy + rec_ly(p);
@@ -892,7 +877,7 @@ __device__ __noinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bo
                                   float(rx) + 1.f);
         if (bd.on) {
             const int ky0 = max(bd.ky0, y0 - pyc), ky1 = min(bd.ky1, y1 - pyc);
-            gather_band(r, bd, ti, sw, tg, rid, pxc, pyc, ky0, ky1, x0 - pxc, x1 - pxc, a);
+            gather_band(r, bd, ti, sw, tg, rid, pxc, pyc, ky0, ky1, x0 - pxc, x1 - pxc, stage);
             return;
         }
     }
@@ -937,14 +922,14 @@ __device__ __noinline__ void gather(const Rec& r, const TileInfo& ti, int sw, bo
     }
     const float Sx = fmaf(ti.sx, B1t, r.dx0 * A0t);
     const float Sxx = fmaf(ti.sx * ti.sx, B2, fmaf(2.f * ti.sx * r.dx0, B1t, r.dx0 * r.dx0 * A0t));
-    finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+    finish_grad(stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
 }
 
 // Backward gather of one photon by the whole warp (see use_coop): lanes take rows and walk
 // their support spans, and a warp reduction hands the moments to the owning lane.
-__device__ __noinline__ void gather_coop(const Rec& r, const TileInfo& ti, int sw,
+__device__ __forceinline__ void gather_coop(const Rec& r, const TileInfo& ti, int sw,
                                             const float* tg, uint32_t rid, int owner,
-                                            const TileArgs& a) {
+                                            GradRec* stage) {
     const int lane = threadIdx.x & 31;
     int pxc, pyc, x0, x1, y0, y1;
     rec_box(r, ti, pxc, pyc, x0, x1, y0, y1);
@@ -984,16 +969,15 @@ __device__ __noinline__ void gather_coop(const Rec& r, const TileInfo& ti, int s
     if (lane == owner) {
         const float Sx = fmaf(ti.sx, B1t, r.dx0 * A0t);
         const float Sxx = fmaf(ti.sx * ti.sx, B2, fmaf(2.f * ti.sx * r.dx0, B1t, r.dx0 * r.dx0 * A0t));
-        finish_grad(a.stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
+        finish_grad(stage, rid, r.e, r.m00, r.m01, r.m10, r.m11, sE, Sx, Sy, Sxx, Sxy, Syy);
     }
 }
 
-template <int NT, int MINB, bool ROWS>
+template <int NT, int MINB>
 __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
     extern __shared__ float tg[];
     const Cfg cfg = a.cfg;
     const int sw = cfg.sw;
-    const uint32_t tg_base = static_cast<uint32_t>(__cvta_generic_to_shared(tg));
     const int64_t n_tile = tile_count(a);
     const int64_t nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
     __shared__ uint32_t chunk_slot;
@@ -1016,29 +1000,162 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
             for (int pass = 0; pass <= NT; ++pass) {
                 const bool mine = have && i >= sg.begin && i < sg.end;
                 const bool coop = mine && use_coop(r, cfg.coop_r);
-                if constexpr (ROWS) {
-                    // padded-row walk; photons without a band take the generic gather below
-                    RowGeo g;
-                    int rows = 0;
-                    bool walk = false, generic = false;
-                    if (mine && !coop) {
+                if (mine && !coop) gather(r, ti, sw, cfg.spans, cfg.band, tg, uint32_t(i), a.stage);
+                for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
+                    const int src = __ffs(cm) - 1;
+                    const Rec rb = shfl_rec(r, src);
+                    const uint32_t slot = uint32_t(base) + (threadIdx.x & ~31u) + uint32_t(src);
+                    gather_coop(rb, ti, sw, tg, slot, src, a.stage);
+                }
+                if (sg.end >= bend) break;
+                sg = next_segment(a, sg);
+                ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
+                __syncthreads();
+                load_region(tg, sw, ti, a.grad);
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// ---- the padded-row walk's kernels (walk 4) ---------------------------------------------
+// The same persistent chunk and segment loop as fwd_tiles_kernel / bwd_tiles_kernel, with the
+// padded-row walk for the photons that have a band. A lane loads its record in the pass of its
+// segment only, and keeps just the row walk's constants across the walk; the rare paths (no
+// band, warp-cooperative splat) reload the record out of line, so their registers do not
+// burden the walk.
+
+__device__ __noinline__ void deposit_generic(const Rec* rp, TileInfo ti, int sw, bool spans,
+                                             float* acc) {
+    const Rec r = *rp;
+    int x0, x1, y0, y1;
+    deposit(r, ti, sw, spans, false, acc, x0, x1, y0, y1);
+}
+
+__device__ __noinline__ void deposit_coop_at(const Rec* rp, TileInfo ti, int sw, uint32_t acc_base,
+                                             int lane) {
+    deposit_coop(*rp, ti, sw, acc_base, lane);
+}
+
+__device__ __noinline__ void gather_generic(const Rec* rp, TileInfo ti, int sw, bool spans,
+                                            const float* tg, uint32_t rid, GradRec* stage) {
+    gather(*rp, ti, sw, spans, false, tg, rid, stage);
+}
+
+__device__ __noinline__ void gather_coop_at(const Rec* rp, TileInfo ti, int sw, const float* tg,
+                                            uint32_t rid, int owner, GradRec* stage) {
+    gather_coop(*rp, ti, sw, tg, rid, owner, stage);
+}
+
+template <int NT, int MINB>
+__global__ __launch_bounds__(NT, MINB) void fwd_rows_kernel(TileArgs a) {
+    extern __shared__ float acc[];
+    __shared__ int sb[4];
+    __shared__ uint32_t chunk_slot;
+    const Cfg cfg = a.cfg;
+    const int sw = cfg.sw;
+    for (int k = threadIdx.x; k < sw * sw; k += NT) acc[k] = 0.f;
+    if (threadIdx.x == 0) {
+        sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
+    }
+    __syncthreads();
+    const uint32_t acc_base = static_cast<uint32_t>(__cvta_generic_to_shared(acc));
+    const int lane = threadIdx.x & 31;
+    // photon positions fit in 31 bits (the entry points reject larger calls)
+    const int n_tile = int(tile_count(a));
+    const int nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
+    for (int c = int(next_chunk(a.queue, &chunk_slot)); c < nchunks;
+         c = int(next_chunk(a.queue, &chunk_slot))) {
+        const int p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
+        Segment sg = first_segment(a, c, p0);
+        TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
+        for (int base = p0; base < p1; base += NT) {
+            const int i = base + int(threadIdx.x);
+            const int bend = min(base + NT, p1);
+            for (int pass = 0; pass <= NT; ++pass) {
+                const bool mine = i < p1 && i >= sg.begin && i < sg.end;
+                RowGeo g;
+                int rows = 0;
+                float e3 = 0.f;
+                bool generic = false, coop = false;
+                int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
+                if (mine) {
+                    const Rec r = a.srecs[i];
+                    coop = use_coop(r, cfg.coop_r);
+                    if (coop || !(rec_flags(r.packed) & kFlagFwdSkip)) {
+                        int pxc, pyc;
+                        rec_clip(r, ti, pxc, pyc, x0, x1, y0, y1);
+                        if (!coop) {
+                            generic = !prep_rows(r, ti, sw, pxc, pyc, x0, x1, y0, y1, g);
+                            rows = generic ? 0 : g.rows;
+                            e3 = r.e * kThreeOverPi;
+                        }
+                    }
+                }
+                deposit_rows(g, rows, e3, acc_base, sw);
+                if (generic) deposit_generic(a.srecs + i, ti, sw, cfg.spans, acc);
+                for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
+                    const int src = __ffs(cm) - 1;
+                    deposit_coop_at(a.srecs + (base + int(threadIdx.x & ~31u) + src), ti, sw,
+                                    acc_base, lane);
+                }
+                bbox_publish(sb, x0, x1, y0, y1);
+                if (sg.end >= bend) break;
+                flush_tile(acc, sw, ti, a.out, sb);
+                sg = next_segment(a, sg);
+                ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
+            }
+        }
+        flush_tile(acc, sw, ti, a.out, sb);
+    }
+}
+
+template <int NT, int MINB>
+__global__ __launch_bounds__(NT, MINB) void bwd_rows_kernel(TileArgs a) {
+    extern __shared__ float tg[];
+    __shared__ uint32_t chunk_slot;
+    const Cfg cfg = a.cfg;
+    const int sw = cfg.sw;
+    const uint32_t tg_base = static_cast<uint32_t>(__cvta_generic_to_shared(tg));
+    const int n_tile = int(tile_count(a));
+    const int nchunks = (n_tile + cfg.chunk - 1) / cfg.chunk;
+    for (int c = int(next_chunk(a.queue, &chunk_slot)); c < nchunks;
+         c = int(next_chunk(a.queue, &chunk_slot))) {
+        const int p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
+        Segment sg = first_segment(a, c, p0);
+        TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
+        // next_chunk's barrier ends the previous chunk's reads of the staged tile
+        load_region(tg, sw, ti, a.grad);
+        __syncthreads();
+        for (int base = p0; base < p1; base += NT) {
+            const int i = base + int(threadIdx.x);
+            const int bend = min(base + NT, p1);
+            for (int pass = 0; pass <= NT; ++pass) {
+                const bool mine = i < p1 && i >= sg.begin && i < sg.end;
+                RowGeo g;
+                int rows = 0;
+                float dy0 = 0.f;
+                bool walk = false, generic = false, coop = false;
+                if (mine) {
+                    const Rec r = a.srecs[i];
+                    coop = use_coop(r, cfg.coop_r);
+                    if (!coop) {
                         int pxc, pyc, x0, x1, y0, y1;
                         rec_clip(r, ti, pxc, pyc, x0, x1, y0, y1);
                         walk = prep_rows(r, ti, sw, pxc, pyc, x0, x1, y0, y1, g);
                         generic = !walk;
                         rows = walk ? g.rows : 0;
+                        dy0 = r.dy0;
                     }
-                    const RowMoments m = gather_rows(g, rows, tg_base, sw, ti.sy, r.dy0);
-                    if (walk) finish_rows(a.stage, uint32_t(i), r, ti, m);
-                    if (generic) gather(r, ti, sw, cfg.spans, false, tg, uint32_t(i), a);
-                } else if (mine && !coop) {
-                    gather(r, ti, sw, cfg.spans, cfg.band, tg, uint32_t(i), a);
                 }
+                const RowMoments m = gather_rows(g, rows, tg_base, sw, ti.sy, dy0);
+                if (walk) finish_rows(a.stage, uint32_t(i), a.srecs[i], ti, m);
+                if (generic)
+                    gather_generic(a.srecs + i, ti, sw, cfg.spans, tg, uint32_t(i), a.stage);
                 for (uint32_t cm = __ballot_sync(0xFFFFFFFFu, coop); cm; cm &= cm - 1) {
                     const int src = __ffs(cm) - 1;
-                    const Rec rb = shfl_rec(r, src);
-                    const uint32_t slot = uint32_t(base) + (threadIdx.x & ~31u) + uint32_t(src);
-                    gather_coop(rb, ti, sw, tg, slot, src, a);
+                    const int slot = base + int(threadIdx.x & ~31u) + src;
+                    gather_coop_at(a.srecs + slot, ti, sw, tg, uint32_t(slot), src, a.stage);
                 }
                 if (sg.end >= bend) break;
                 sg = next_segment(a, sg);
@@ -1297,7 +1414,7 @@ cudaError_t set_smem(K kernel, size_t smem) {
 template <int MINB, bool ROWS>
 cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
     const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
-    auto kern = fwd_tiles_kernel<kTileThreads, MINB, ROWS>;
+    auto kern = ROWS ? fwd_rows_kernel<kTileThreads, MINB> : fwd_tiles_kernel<kTileThreads, MINB>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;
@@ -1316,7 +1433,7 @@ cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
 template <int MINB, bool ROWS>
 cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
     const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
-    auto kern = bwd_tiles_kernel<kTileThreads, MINB, ROWS>;
+    auto kern = ROWS ? bwd_rows_kernel<kTileThreads, MINB> : bwd_tiles_kernel<kTileThreads, MINB>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t chunks = (a.ph.n + a.cfg.chunk - 1) / a.cfg.chunk;

@@ -246,9 +246,9 @@ class BatchedPlate:
 
     def __init__(self, sims, max_pixel_radius, device, config=None):
         from .splatting import BatchedSplat
-        self.device = torch.device(device)
         self.splat = BatchedSplat([(n, shape) for n, shape, _ in sims], max_pixel_radius,
-                                  self.device, config=config)
+                                  device, config=config)
+        self.device = self.splat.device
         n_sims = len(sims)
         table = (PlateParams * n_sims)()
         begins = []

@@ -190,6 +190,8 @@ class BatchedSplat:
         self.cfg = config if config is not None else _default_cfg
         self.mpr = int(max_pixel_radius)
         self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         n_sims = len(sims)
         table = (_lib.PdsSim * n_sims)()
         begin, off = 0, 0
