@@ -52,13 +52,16 @@ typedef struct pds_config {
     int32_t class_bits; /* footprint-size bits appended to the sort key (photons of a tile
                            are then grouped by footprint size; with the band walk, classes
                            of 1/k octave of the band's area, k = 1 up to 3 bits, 2 for 4,
-                           3 for 5): 1..5, or -1 for none (default 5) */
+                           3 for 5; 6: the row walk's classes, 3 bits of band rows and 3
+                           of row width inside the box): 1..6, or -1 for none (default 5) */
     int32_t apron_max;  /* largest footprint radius (px) the tile path holds (default 32);
                            larger footprints take the direct path */
     int32_t walk;       /* pixels visited per photon: 1 = the reference's whole box,
                            2 = only the rows / row spans that can hold the kernel's support,
-                           3 = a sheared band of equal-width rows around the support
-                           (2 and 3 give the same result: pixels outside the support add
+                           3 = a sheared band of equal-width rows around the support,
+                           4 = the band's rows inside the box, each warp's photons padded to a
+                           common row count and width (best with class_bits 6)
+                           (2, 3 and 4 give the same result: pixels outside the support add
                            exactly zero); default 3 */
     int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2, 3 or 4
                            (fewer: more registers per thread; more: more warps); default 3 */

@@ -24,6 +24,9 @@ DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=3, coop_rad
 CANDIDATES = [dict(tile=t, chunk=2048, class_bits=b, walk=w, min_blocks=m, coop_radius=k)
               for t, b, w, m, k in itertools.product((64, 32), (5, 3), (3, 1), (3, 4), (-1, 8))]
 CANDIDATES += [dict(DEFAULT, chunk=c) for c in (1024, 4096)]
+# the padded-row walk with its row classes, at both tile sizes and CTA counts
+CANDIDATES += [dict(tile=t, chunk=2048, class_bits=6, walk=4, min_blocks=m, coop_radius=-1)
+               for t, m in itertools.product((64, 32), (3, 4))]
 
 _cache = {}
 

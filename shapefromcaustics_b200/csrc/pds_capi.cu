@@ -44,10 +44,10 @@ struct Resolved {
 int resolve_cfg(const pds_config* in, pds_config& out) {
     out.tile = (in && in->tile) ? in->tile : 64;
     out.chunk = (in && in->chunk) ? in->chunk : 2048;
-    out.class_bits = (in && in->class_bits) ? in->class_bits : 6;
+    out.class_bits = (in && in->class_bits) ? in->class_bits : 5;
     if (out.class_bits == -1) out.class_bits = 0;
     out.apron_max = (in && in->apron_max) ? in->apron_max : 32;
-    out.walk = (in && in->walk) ? in->walk : 4;
+    out.walk = (in && in->walk) ? in->walk : 3;
     out.min_blocks = (in && in->min_blocks) ? in->min_blocks : 3;
     out.coop_radius = (in && in->coop_radius) ? in->coop_radius : -1;
     if (out.coop_radius < -1 || out.coop_radius > 63)

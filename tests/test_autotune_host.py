@@ -9,13 +9,13 @@ DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=3, coop_rad
 def test_first_candidate_is_the_library_default_and_all_are_valid():
     assert AT.CANDIDATES[0] == DEFAULT == AT.DEFAULT
     keys = {tuple(sorted(c.items())) for c in AT.CANDIDATES}
-    assert len(keys) == len(AT.CANDIDATES) == 34
+    assert len(keys) == len(AT.CANDIDATES) == 38
     assert {c["chunk"] for c in AT.CANDIDATES} == {1024, 2048, 4096}
     for c in AT.CANDIDATES:
         assert c["tile"] in (16, 32, 64)
         assert c["chunk"] % 256 == 0
-        assert 1 <= c["class_bits"] <= 5
-        assert c["walk"] in (1, 2, 3)
+        assert 1 <= c["class_bits"] <= 6
+        assert c["walk"] in (1, 2, 3, 4)
         assert 2 <= c["min_blocks"] <= 4
         assert c["coop_radius"] == -1 or c["coop_radius"] >= 1
 
