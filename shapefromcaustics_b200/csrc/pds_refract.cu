@@ -19,6 +19,7 @@
 // N~x, N~y and their x/y derivatives), contracts with the splat-input gradients, and maps
 // the result back onto the photon's 4x4 texel patch through the transposed bilinear and
 // Sobel stencils. Patches are accumulated with global float adds.
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -358,8 +359,10 @@ __global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
 // derivatives c[k] of L with respect to its seven surface scalars: the transposed bilinear
 // stencil for the height (k = 0) and the transposed bilinear and Sobel stencils for the normal
 // scalars (k = 1..6). Patch texels outside the field fold onto the border (replicate padding).
-__device__ __forceinline__ void scatter_patch(float* gh, int H, int W, float texel,
-                                          const Bilin& b, const float c[K]) {
+// add(row, col, value) receives the non-zero patch entries.
+template <class Add>
+__device__ __forceinline__ void scatter_patch(int H, int W, float texel, const Bilin& b,
+                                              const float c[K], Add add) {
     float patch[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
@@ -400,42 +403,136 @@ __device__ __forceinline__ void scatter_patch(float* gh, int H, int W, float tex
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int jj = min(max(b.x0 - 1 + q, 0), W - 1);
-            if (patch[r][q] != 0.f) atomicAdd(gh + int64_t(ii) * W + jj, patch[r][q]);
+            if (patch[r][q] != 0.f) add(ii, jj, patch[r][q]);
         }
     }
 }
 
-__global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
-    const int64_t n = a.n;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * blockDim.x) {
-        const float px = a.px[i], py = a.py[i];
-        const PlateParams P = photon_params(a, i);
-        const Bilin b = bilin(px, py, P.texel, a.H, a.W);
-        float s[K];
-        surface_scalars(a.h, a.H, a.W, P.texel, b, s);
-        Dual v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            v[k] = dconst(s[k]);
-            v[k].d[k] = 1.f;
+// The height-field gradient of a CTA's photons: where the CTA's photons share a compact patch
+// of the field (the photon source emits photons texel by texel, so a CTA's 256 consecutive
+// photons sit in a few texel rows), their patches are summed in shared memory and added to the
+// field once per texel; otherwise (scattered hits) each patch entry is a global atomic add.
+// Without it, every photon's 16 patch entries were global atomics on a few hot texels.
+constexpr int kPatchSmem = 8192;  // floats of the CTA's shared patch region (32 KB)
+
+struct PatchAcc {
+    float* buf;   // shared region, rw x rh floats, or nullptr: global atomics
+    int x0, y0, rw;
+    float* gh;
+    int W;
+    __device__ __forceinline__ void operator()(int ii, int jj, float v) const {
+        if (buf)
+            atomicAdd(buf + (ii - y0) * rw + (jj - x0), v);
+        else
+            atomicAdd(gh + int64_t(ii) * W + jj, v);
+    }
+};
+
+// Sets up the CTA's region from its active photons' cells (bx0, by0; ignored when !active):
+// all threads call it. Returns the accumulator (shared region zeroed, or global).
+__device__ __forceinline__ PatchAcc patch_begin(float* smem, int* bb, bool active, int bx0,
+                                                int by0, float* gh, int H, int W) {
+    if (threadIdx.x == 0) {
+        bb[0] = INT_MAX; bb[1] = INT_MIN; bb[2] = INT_MAX; bb[3] = INT_MIN;
+    }
+    __syncthreads();
+    int lx0 = active ? bx0 : INT_MAX, lx1 = active ? bx0 : INT_MIN;
+    int ly0 = active ? by0 : INT_MAX, ly1 = active ? by0 : INT_MIN;
+    lx0 = __reduce_min_sync(0xFFFFFFFFu, lx0);
+    lx1 = __reduce_max_sync(0xFFFFFFFFu, lx1);
+    ly0 = __reduce_min_sync(0xFFFFFFFFu, ly0);
+    ly1 = __reduce_max_sync(0xFFFFFFFFu, ly1);
+    if ((threadIdx.x & 31) == 0 && lx0 <= lx1) {
+        atomicMin(bb + 0, lx0);
+        atomicMax(bb + 1, lx1);
+        atomicMin(bb + 2, ly0);
+        atomicMax(bb + 3, ly1);
+    }
+    __syncthreads();
+    PatchAcc acc;
+    acc.gh = gh;
+    acc.W = W;
+    acc.buf = nullptr;
+    acc.x0 = acc.y0 = acc.rw = 0;
+    if (bb[0] <= bb[1]) {
+        // patch texels: cell - 1 .. cell + 2, clamped into the field (replicate padding)
+        const int x0 = max(bb[0] - 1, 0), x1 = min(bb[1] + 2, W - 1);
+        const int y0 = max(bb[2] - 1, 0), y1 = min(bb[3] + 2, H - 1);
+        const int rw = x1 - x0 + 1, rh = y1 - y0 + 1;
+        if (int64_t(rw) * rh <= kPatchSmem) {
+            acc.buf = smem;
+            acc.x0 = x0;
+            acc.y0 = y0;
+            acc.rw = rw;
+            for (int k = threadIdx.x; k < rw * rh; k += blockDim.x) smem[k] = 0.f;
         }
-        Dual xr, yr, Dux, Duy, Dvx, Dvy;
-        plate_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], px, py, P, xr, yr, Dux,
-                          Duy, Dvx, Dvy);
-        const Dual den = Dux * Dvy - Duy * Dvx;
-        if (den.v == 0.f) continue;  // degenerate photon: skipped by the splat, no gradient
-        const Dual f = dconst(2.f) / den;
-        const float gE = a.gE[i];
-        const float g0 = a.gM[i], g1 = a.gM[n + i], g3 = a.gM[3 * n + i], g4 = a.gM[4 * n + i];
-        // L = gE Ep + gx xr + gy yr + sum gM Mp, as a dual over the seven scalars
-        Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
-        L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
-        L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
+    }
+    __syncthreads();
+    return acc;
+}
+
+// Adds the CTA's shared region to the field (all threads call it).
+__device__ __forceinline__ void patch_end(const PatchAcc& acc, int* bb, int H, int W) {
+    __syncthreads();
+    if (acc.buf) {
+        const int x1 = min(bb[1] + 2, W - 1), y1 = min(bb[3] + 2, H - 1);
+        const int rh = y1 - acc.y0 + 1;
+        for (int k = threadIdx.x; k < acc.rw * rh; k += blockDim.x) {
+            const float v = acc.buf[k];
+            if (v != 0.f)
+                atomicAdd(acc.gh + int64_t(acc.y0 + k / acc.rw) * W + acc.x0 + k % acc.rw, v);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
+    __shared__ float smem[kPatchSmem];
+    __shared__ int bb[4];
+    const int64_t n = a.n;
+    // CTA-contiguous blocks of 256 photons (their patches share a shared-memory region)
+    for (int64_t blk = int64_t(blockIdx.x) * blockDim.x; blk < n;
+         blk += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = blk + threadIdx.x;
+        bool active = i < n;
+        Bilin b = {0, 0, 0.f, 0.f};
         float c[K];
+        float texel = a.P.texel;
+        if (active) {
+            const float px = a.px[i], py = a.py[i];
+            const PlateParams P = photon_params(a, i);
+            texel = P.texel;
+            b = bilin(px, py, P.texel, a.H, a.W);
+            float s[K];
+            surface_scalars(a.h, a.H, a.W, P.texel, b, s);
+            Dual v[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) c[k] = L.d[k];
-        scatter_patch(a.gh, a.H, a.W, P.texel, b, c);
+            for (int k = 0; k < K; ++k) {
+                v[k] = dconst(s[k]);
+                v[k].d[k] = 1.f;
+            }
+            Dual xr, yr, Dux, Duy, Dvx, Dvy;
+            plate_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], px, py, P, xr, yr, Dux,
+                              Duy, Dvx, Dvy);
+            const Dual den = Dux * Dvy - Duy * Dvx;
+            if (den.v == 0.f) {
+                active = false;  // degenerate photon: skipped by the splat, no gradient
+            } else {
+                const Dual f = dconst(2.f) / den;
+                const float gE = a.gE[i];
+                const float g0 = a.gM[i], g1 = a.gM[n + i], g3 = a.gM[3 * n + i],
+                            g4 = a.gM[4 * n + i];
+                // L = gE Ep + gx xr + gy yr + sum gM Mp, as a dual over the seven scalars
+                Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
+                L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
+                L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
+#pragma unroll
+                for (int k = 0; k < K; ++k) c[k] = L.d[k];
+            }
+        }
+        const PatchAcc acc = patch_begin(smem, bb, active, b.x0, b.y0, a.gh, a.H, a.W);
+        if (active) scatter_patch(a.H, a.W, texel, b, c, acc);
+        patch_end(acc, bb, a.H, a.W);
     }
 }
 
@@ -633,7 +730,14 @@ __global__ __launch_bounds__(256) void point_bwd_kernel(PointArgs a) {
         c[0] = L.d[0] / fp;
 #pragma unroll
         for (int k = 1; k < K; ++k) c[k] = L.d[k];
-        scatter_patch(a.gh, a.H, a.W, a.P.texel, b, c);
+        // traced hits follow the photons' random directions, not the field's texel order:
+        // global adds
+        PatchAcc acc;
+        acc.buf = nullptr;
+        acc.x0 = acc.y0 = acc.rw = 0;
+        acc.gh = a.gh;
+        acc.W = a.W;
+        scatter_patch(a.H, a.W, a.P.texel, b, c, acc);
     }
 }
 
