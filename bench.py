@@ -779,6 +779,17 @@ def plate_batch_setup(device, seed=1000, n_sims=64, n_field=256, footprint_px=3.
     return scene, h_true, h_tgt, sims, per_texel
 
 
+def check_refract_backward(batch, h, px, py, flux, gE, gX, gM, gh):
+    """The batched refraction backward alone (the last step of BatchedPlate.backward)."""
+    from shapefromcaustics_b200._lib import check, lib
+    from shapefromcaustics_b200.splatting import _ptr, _stream
+    with torch.cuda.device(batch.device):
+        check(lib().pds_batch_refract_backward_f32(
+            _ptr(h), h.shape[0], h.shape[1], _ptr(batch.plates_dev), _ptr(batch.begins_dev),
+            batch.n_sims, _ptr(px), _ptr(py), _ptr(flux), batch.n_total, _ptr(gE), _ptr(gX),
+            _ptr(gM), _ptr(gh), _stream(batch.device)))
+
+
 def run_plate_batch(args, device, steps, warmup):
     """One Landweber iteration over the uneven batch of simulations with refraction
     (plate_batch_setup), batched (one CUDA graph: photon sources, one batched refraction, one
@@ -875,8 +886,42 @@ def run_plate_batch(args, device, steps, warmup):
         torch.cuda.synchronize()
     ms_p = e0.elapsed_time(e1) / k
     del graph
+    # phases of the batched step (eager, CUDA events on the stream)
+    names = ["sources", "refract_fwd", "plan", "splat_fwd", "data_grad", "refract_fwd_again",
+             "splat_bwd", "refract_bwd", "update"]
+    acc = {k: [] for k in names}
+    splat = batch.splat
+    with torch.cuda.stream(stream):
+        for rep in range(3):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
+            ev[0].record(stream)
+            sources(0)
+            ev[1].record(stream)
+            inputs = batch._inputs(h, px, py, flux)
+            ev[2].record(stream)
+            splat.plan(*inputs)
+            ev[3].record(stream)
+            splat.forward(img)
+            ev[4].record(stream)
+            torch.sub(img, target, out=gimg)
+            ev[5].record(stream)
+            inputs = batch._inputs(h, px, py, flux)
+            ev[6].record(stream)
+            splat.inputs = inputs
+            gE, gX, gM = splat.backward(gimg)
+            ev[7].record(stream)
+            gh.zero_()
+            check_refract_backward(batch, h, px, py, flux, gE, gX, gM, gh)
+            ev[8].record(stream)
+            landweber_update(d, gh, mask, params, ws)
+            ev[9].record(stream)
+            torch.cuda.synchronize()
+            for k, nm in enumerate(names):
+                acc[nm].append(ev[k].elapsed_time(ev[k + 1]))
+    phases = {k: statistics.median(v) for k, v in acc.items()}
     return {"batched_it_per_s": 1e3 / ms_b, "plain_it_per_s": 1e3 / ms_p,
             "batched_over_plain": ms_p / ms_b, "batched_ms": ms_b, "plain_ms": ms_p,
+            "batched_phase_ms": phases,
             "photons_per_iteration": n_total, "simulations": len(sims),
             "workload": "uneven batch with refraction: 256^2 height field, 64 simulations, "
                         "N_i ~ logU[2^16, 2^22] (whole photons per texel), images "
@@ -971,7 +1016,8 @@ def run_reconstruction(args, rank, world, device):
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
     peak = torch.cuda.max_memory_allocated(device)
-    phases = iteration_phases(1.0, res["target"], scene, res["d"].clone(),
+    # the phases of an iteration at the start (flat field), whatever the step size did later
+    phases = iteration_phases(1.0, res["target"], scene, torch.zeros_like(h_true),
                               torch.ones_like(h_true), params, sims=16, per_texel=4, image=nf,
                               footprint_px=args.recon_footprint, seed=rank + 99,
                               objective=args.recon_objective)
@@ -1017,8 +1063,9 @@ def main():
     ap.add_argument("--ref-sample", type=float, default=2 ** 21)
     ap.add_argument("--recon-objective", default="l2_sq", choices=["l2_sq", "normalized"],
                     help="recon1024: the reference's 0.5 |I - T|^2 or it divided by |T|^2")
-    ap.add_argument("--recon-tau", type=float, default=0.1,
-                    help="recon1024: gradient step (the reference's tau_pixel)")
+    ap.add_argument("--recon-tau", type=float, default=1e-7,
+                    help="recon1024: gradient step (the reference's tau_pixel; its default "
+                         "0.1 diverges on this scene with the l2_sq data term)")
     ap.add_argument("--recon-footprint", type=float, default=3.0,
                     help="recon1024: initial photon footprint in receiver pixels")
     args = ap.parse_args()
