@@ -790,7 +790,7 @@ def check_refract_backward(batch, h, px, py, flux, gE, gX, gM, gh):
             _ptr(gM), _ptr(gh), _stream(batch.device)))
 
 
-def run_plate_batch(args, device, steps, warmup):
+def run_plate_batch(args, device, steps, warmup, config=None):
     """One Landweber iteration over the uneven batch of simulations with refraction
     (plate_batch_setup), batched (one CUDA graph: photon sources, one batched refraction, one
     splat plan / forward / backward, one batched refraction backward, the fused update) against
@@ -802,7 +802,9 @@ def run_plate_batch(args, device, steps, warmup):
     from shapefromcaustics_b200.splatting import SplatPlan
     scene, h_true, h_tgt, sims, per_texel = plate_batch_setup(device)
     nf = h_true.shape[0]
-    batch = PL.BatchedPlate(sims, MPR, device)
+    from shapefromcaustics_b200 import _lib
+    batch = PL.BatchedPlate(sims, MPR, device,
+                            config=_lib.config(**config) if config else None)
     n_total = batch.n_total
     px = torch.empty(n_total, device=device)
     py = torch.empty(n_total, device=device)
