@@ -203,6 +203,206 @@ __device__ __forceinline__ void plate_chain(const T& hz, const T& Nx, const T& N
     Dvy = P.inv_half * Dv3.y;
 }
 
+// ---- reverse mode of the collimated chain ------------------------------------------------
+// The backward needs the seven derivatives dL/dS_k of one scalar L; forward-mode duals carry
+// seven tangents through every operation (eight times the arithmetic, and a register count
+// that leaves one CTA per SM), reverse mode one adjoint sweep. plate_chain_adjoint runs the
+// chain of plate_chain<float> forward, keeping its intermediates, then propagates the adjoints
+// of the outputs back to the seven scalars, operation by operation (the derivative of each
+// step written out below, from the formulas of plate_chain, refract and transfer_z).
+
+struct V3a {
+    float x, y, z;
+};
+__device__ __forceinline__ V3a va(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ float da(const V3a& a, const V3a& b) {
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+__device__ __forceinline__ V3a sa(float s, const V3a& a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ V3a pa(const V3a& a, const V3a& b) {
+    return {a.x + b.x, a.y + b.y, a.z + b.z};
+}
+__device__ __forceinline__ V3a ma(const V3a& a, const V3a& b) {
+    return {a.x - b.x, a.y - b.y, a.z - b.z};
+}
+__device__ __forceinline__ void acc3(V3a& a, const V3a& b) {
+    a.x += b.x; a.y += b.y; a.z += b.z;
+}
+
+// transfer_z: out = D - (D.z / t.z) t + s (Dd - (Dd.z / t.z) t)
+__device__ __forceinline__ V3a tz_fwd(const V3a& D, const V3a& Dd, float s, const V3a& t) {
+    const float a = D.z / t.z, b = Dd.z / t.z;
+    return pa(ma(D, sa(a, t)), sa(s, ma(Dd, sa(b, t))));
+}
+
+// adjoint of tz_fwd: accumulates into Db (D), Ddb (Dd), sb (s) and tb (t) from ob (out)
+__device__ __forceinline__ void tz_adj(const V3a& D, const V3a& Dd, float s, const V3a& t,
+                                       const V3a& ob, V3a& Db, V3a& Ddb, float& sb, V3a& tb) {
+    const float itz = 1.f / t.z;
+    const float a = D.z * itz, b = Dd.z * itz;
+    acc3(Db, ob);
+    const float ab = -da(ob, t);
+    Db.z += ab * itz;
+    tb.z -= ab * a * itz;
+    acc3(tb, sa(-(a + s * b), ob));
+    sb += da(ob, ma(Dd, sa(b, t)));
+    acc3(Ddb, sa(s, ob));
+    const float bb = -s * da(ob, t);
+    Ddb.z += bb * itz;
+    tb.z -= bb * b * itz;
+}
+
+// d L / d S for the collimated chain; L from the splat-input gradients (as in the backward
+// kernels): gx xr + gy yr + sum of gM times Mp + 4 flux gE / |den|. False for a degenerate
+// photon (den == 0: no gradient).
+__device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, float py,
+                                                    const PlateParams& P, float gx, float gy,
+                                                    float g0, float g1, float g3, float g4,
+                                                    float cE, float Sb[K]) {
+    const float Nx = S[1], Ny = S[2], Nxx = S[3], Nyx = S[4], Nxy = S[5], Nyy = S[6];
+    const float hz = S[0];
+    const V3a d = va(P.lx, P.ly, P.lz);
+    // ---- forward
+    const V3a Nt = va(Nx, Ny, 1.f);
+    const float nn = Nx * Nx + Ny * Ny + 1.f;
+    const float nlen = sqrtf(nn);
+    const float inl = 1.f / nlen;
+    const V3a n = sa(inl, Nt);
+    const float nd = da(n, d);
+    const float au = P.du0 * n.x / nd, av = P.du0 * n.y / nd;
+    const V3a Du1 = ma(va(P.du0, 0.f, 0.f), sa(au, d));
+    const V3a Dv1 = ma(va(0.f, P.du0, 0.f), sa(av, d));
+    const V3a dNu = va(Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, 0.f);
+    const V3a dNv = va(Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, 0.f);
+    const float nl3 = nn * nlen;
+    const float inl3 = 1.f / nl3;
+    const float wu = da(Nt, dNu), wv = da(Nt, dNv);
+    const V3a dnu = sa(inl3, ma(sa(nn, dNu), sa(wu, Nt)));
+    const V3a dnv = sa(inl3, ma(sa(nn, dNv), sa(wv, Nt)));
+    const float e1 = 1.f / P.ior;
+    const float cosi = da(d, n);
+    const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
+    const float ng1 = -sqrtf(k1);
+    const float coso = e1 * cosi - ng1;
+    const V3a t1 = ma(sa(e1, d), sa(coso, n));
+    const float f1 = e1 - (e1 * e1) * cosi / ng1;
+    const float ddu = da(d, dnu), ddv = da(d, dnv);
+    const float qu = f1 * ddu, qv = f1 * ddv;
+    const V3a Ddu = sa(-1.f, pa(sa(coso, dnu), sa(qu, n)));
+    const V3a Ddv = sa(-1.f, pa(sa(coso, dnv), sa(qv, n)));
+    const float s1 = -hz / t1.z;
+    const V3a Du2 = tz_fwd(Du1, Ddu, s1, t1);
+    const V3a Dv2 = tz_fwd(Dv1, Ddv, s1, t1);
+    const float e2 = P.ior;
+    const float c2 = t1.z;
+    const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
+    const float ng2 = -sqrtf(k2);
+    const float coso2 = e2 * c2 - ng2;
+    const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
+    const float f2 = e2 - (e2 * e2) * c2 / ng2;
+    const float q2u = f2 * Ddu.z, q2v = f2 * Ddv.z;
+    const V3a Ddu2 = ma(sa(e2, Ddu), va(0.f, 0.f, q2u));
+    const V3a Ddv2 = ma(sa(e2, Ddv), va(0.f, 0.f, q2v));
+    const float s2 = -P.dist / t2.z;
+    const V3a Du3 = tz_fwd(Du2, Ddu2, s2, t2);
+    const V3a Dv3 = tz_fwd(Dv2, Ddv2, s2, t2);
+    const float Dux = P.inv_half * Du3.x, Duy = P.inv_half * Du3.y;
+    const float Dvx = P.inv_half * Dv3.x, Dvy = P.inv_half * Dv3.y;
+    const float den = Dux * Dvy - Duy * Dvx;
+    if (den == 0.f) return false;
+    // ---- output adjoints: L = gx xr + gy yr + (2 / den) A + cE / |den|
+    const float f = 2.f / den;
+    const float A = g0 * Dvy - g1 * Dvx - g3 * Duy + g4 * Dux;
+    const float denb = -f * A / den - cE * copysignf(1.f, den) / (den * den);
+    const float Duxb = f * g4 + denb * Dvy, Duyb = -f * g3 - denb * Dvx;
+    const float Dvxb = -f * g1 - denb * Duy, Dvyb = f * g0 + denb * Dux;
+    const float p2xb = P.inv_half * gx, p2yb = P.inv_half * gy;
+    // ---- reverse sweep
+    V3a t2b = va(P.inv_half * gx * s2, P.inv_half * gy * s2, 0.f);
+    float s2b = P.inv_half * (gx * t2.x + gy * t2.y);
+    V3a Du2b = va(0.f, 0.f, 0.f), Dv2b = Du2b, Ddu2b = Du2b, Ddv2b = Du2b;
+    tz_adj(Du2, Ddu2, s2, t2, va(P.inv_half * Duxb, P.inv_half * Duyb, 0.f), Du2b, Ddu2b, s2b,
+           t2b);
+    tz_adj(Dv2, Ddv2, s2, t2, va(P.inv_half * Dvxb, P.inv_half * Dvyb, 0.f), Dv2b, Ddv2b, s2b,
+           t2b);
+    t2b.z += s2b * P.dist / (t2.z * t2.z);
+    // bottom refraction
+    V3a Dub = sa(e2, Ddu2b), Dvb = sa(e2, Ddv2b);  // adjoints of Ddu, Ddv
+    const float q2ub = -Ddu2b.z, q2vb = -Ddv2b.z;
+    Dub.z += f2 * q2ub;
+    Dvb.z += f2 * q2vb;
+    const float f2b = Ddu.z * q2ub + Ddv.z * q2vb;
+    V3a t1b = sa(e2, t2b);
+    const float coso2b = -t2b.z;
+    float c2b = e2 * coso2b - (e2 * e2) / ng2 * f2b;
+    float ng2b = -coso2b + (e2 * e2) * c2 / (ng2 * ng2) * f2b;
+    const float k2b = ng2b / (2.f * ng2);
+    c2b += 2.f * e2 * e2 * c2 * k2b;
+    t1b.z += c2b;
+    // bottom transfer
+    V3a Du1b = va(0.f, 0.f, 0.f), Dv1b = Du1b;
+    float s1b = p2xb * t1.x + p2yb * t1.y;
+    t1b.x += p2xb * s1;
+    t1b.y += p2yb * s1;
+    tz_adj(Du1, Ddu, s1, t1, Du2b, Du1b, Dub, s1b, t1b);
+    tz_adj(Dv1, Ddv, s1, t1, Dv2b, Dv1b, Dvb, s1b, t1b);
+    const float hzb = -s1b / t1.z;
+    t1b.z += s1b * hz / (t1.z * t1.z);
+    // top refraction (Dd = 0): Ddu = -(coso dnu + qu n), qu = f1 (d . dnu)
+    V3a nb = va(0.f, 0.f, 0.f);
+    float cosob = -da(Dub, dnu) - da(Dvb, dnv) - da(t1b, n);
+    V3a dnub = sa(-coso, Dub), dnvb = sa(-coso, Dvb);
+    const float qub = -da(Dub, n), qvb = -da(Dvb, n);
+    acc3(nb, sa(-qu, Dub));
+    acc3(nb, sa(-qv, Dvb));
+    acc3(nb, sa(-coso, t1b));
+    const float f1b = qub * ddu + qvb * ddv;
+    acc3(dnub, sa(qub * f1, d));
+    acc3(dnvb, sa(qvb * f1, d));
+    float cosib = e1 * cosob - (e1 * e1) / ng1 * f1b;
+    const float ng1b = -cosob + (e1 * e1) * cosi / (ng1 * ng1) * f1b;
+    const float k1b = ng1b / (2.f * ng1);
+    cosib += 2.f * e1 * e1 * cosi * k1b;
+    acc3(nb, sa(cosib, d));
+    // dn = (nn dN - w Nt) / nl3
+    V3a Ntb = va(0.f, 0.f, 0.f);
+    float nnb = 0.f, nl3b = 0.f;
+    V3a dNub = sa(nn * inl3, dnub), dNvb = sa(nn * inl3, dnvb);
+    const float wub = -da(dnub, Nt) * inl3, wvb = -da(dnvb, Nt) * inl3;
+    acc3(dNub, sa(wub, Nt));
+    acc3(dNvb, sa(wvb, Nt));
+    acc3(Ntb, sa(wub, dNu));
+    acc3(Ntb, sa(wvb, dNv));
+    acc3(Ntb, sa(-wu * inl3, dnub));
+    acc3(Ntb, sa(-wv * inl3, dnvb));
+    nnb += (da(dnub, dNu) + da(dnvb, dNv)) * inl3;
+    nl3b -= (da(dnub, dnu) + da(dnvb, dnv)) * inl3;
+    nnb += 1.5f * nlen * nl3b;
+    // dN = (Nxx D.x + Nxy D.y, Nyx D.x + Nyy D.y, 0)
+    Sb[3] = dNub.x * Du1.x + dNvb.x * Dv1.x;  // Nxx
+    Sb[5] = dNub.x * Du1.y + dNvb.x * Dv1.y;  // Nxy
+    Sb[4] = dNub.y * Du1.x + dNvb.y * Dv1.x;  // Nyx
+    Sb[6] = dNub.y * Du1.y + dNvb.y * Dv1.y;  // Nyy
+    Du1b.x += dNub.x * Nxx + dNub.y * Nyx;
+    Du1b.y += dNub.x * Nxy + dNub.y * Nyy;
+    Dv1b.x += dNvb.x * Nxx + dNvb.y * Nyx;
+    Dv1b.y += dNvb.x * Nxy + dNvb.y * Nyy;
+    // Du1 = (du0, 0, 0) - au d, au = du0 n.x / nd (Dv1 with n.y)
+    const float aub = -da(Du1b, d), avb = -da(Dv1b, d);
+    nb.x += aub * P.du0 / nd;
+    nb.y += avb * P.du0 / nd;
+    const float ndb = -(aub * au + avb * av) / nd;
+    acc3(nb, sa(ndb, d));
+    // n = Nt / sqrt(nn)
+    acc3(Ntb, sa(inl, nb));
+    const float inlb = da(nb, Nt);
+    nnb += -0.5f * inl / nn * inlb;
+    Sb[0] = hzb;
+    Sb[1] = Ntb.x + 2.f * Nx * nnb;
+    Sb[2] = Ntb.y + 2.f * Ny * nnb;
+    return true;
+}
+
 // Bilinear footprint of a world position on the height-field grid (texel centres at
 // integers, clamped to the border).
 struct Bilin {
@@ -505,30 +705,9 @@ __global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
             b = bilin(px, py, P.texel, a.H, a.W);
             float s[K];
             surface_scalars(a.h, a.H, a.W, P.texel, b, s);
-            Dual v[K];
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                v[k] = dconst(s[k]);
-                v[k].d[k] = 1.f;
-            }
-            Dual xr, yr, Dux, Duy, Dvx, Dvy;
-            plate_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], px, py, P, xr, yr, Dux,
-                              Duy, Dvx, Dvy);
-            const Dual den = Dux * Dvy - Duy * Dvx;
-            if (den.v == 0.f) {
-                active = false;  // degenerate photon: skipped by the splat, no gradient
-            } else {
-                const Dual f = dconst(2.f) / den;
-                const float gE = a.gE[i];
-                const float g0 = a.gM[i], g1 = a.gM[n + i], g3 = a.gM[3 * n + i],
-                            g4 = a.gM[4 * n + i];
-                // L = gE Ep + gx xr + gy yr + sum gM Mp, as a dual over the seven scalars
-                Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
-                L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
-                L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
-#pragma unroll
-                for (int k = 0; k < K; ++k) c[k] = L.d[k];
-            }
+            active = plate_chain_adjoint(s, px, py, P, a.gX[i], a.gX[n + i], a.gM[i],
+                                         a.gM[n + i], a.gM[3 * n + i], a.gM[4 * n + i],
+                                         4.f * a.flux[i] * a.gE[i], c);
         }
         const PatchAcc acc = patch_begin(smem, bb, active, b.x0, b.y0, a.gh, a.H, a.W);
         if (active) scatter_patch(a.H, a.W, texel, b, c, acc);
