@@ -738,17 +738,17 @@ def run_reference_gpu(args, rank, world, device):
 
 # ------------------------------------------------------------------ Landweber workloads --
 
-def plate_setup(n_field, image, per_texel, device, seed=0, texel=0.1, dist=50.0):
+def plate_setup(n_field, image, per_texel, device, seed=0, texel=0.1, dist=50.0, amp=0.05):
     """Height-field plate of the Landweber workloads: a 1 mm base plus 32 Gaussian bumps
-    (amplitude U[0, 50] um, width U[4, 24] texels), collimated light at normal incidence,
-    n = 1.5, receiver 50 mm below; photons jittered per texel."""
+    (amplitude U[0, amp] mm, 50 um by default, width U[4, 24] texels), collimated light at
+    normal incidence, n = 1.5, receiver 50 mm below; photons jittered per texel."""
     from shapefromcaustics_b200 import scene as SC
     half = 0.5 * n_field * texel * 1.1
     scene = SC.PlateScene(texel=texel, ior=1.5, receiver_distance=dist, receiver_half=half)
     h = SC.height_field_bumps(n_field, n_field, seed=seed, bumps=32, base=1.0,
-                              amp=(0.0, 0.05), width=(4.0, 24.0)).float().to(device)
+                              amp=(0.0, amp), width=(4.0, 24.0)).float().to(device)
     t = SC.height_field_bumps(n_field, n_field, seed=seed + 1, bumps=32, base=1.0,
-                              amp=(0.0, 0.05), width=(4.0, 24.0)).float().to(device)
+                              amp=(0.0, amp), width=(4.0, 24.0)).float().to(device)
     return scene, h, t
 
 
@@ -1001,7 +1001,7 @@ def run_reconstruction(args, rank, world, device):
     from shapefromcaustics_b200.landweber import LandweberParams, iteration_phases, reconstruct
     torch.cuda.set_device(device)
     nf = 1024
-    scene, h_true, _ = plate_setup(nf, nf, 4, device, seed=7)
+    scene, h_true, _ = plate_setup(nf, nf, 4, device, seed=7, amp=args.recon_amplitude)
     d_true = h_true - 1.0
     vol = float(d_true.sum())
     params = LandweberParams(tau=args.recon_tau, d1=0.75 * vol, d2=1.25 * vol)
@@ -1010,7 +1010,8 @@ def run_reconstruction(args, rank, world, device):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
-    res = reconstruct(h_true, 1.0, scene, iterations=iters, sims=16, per_texel=4, image=nf,
+    sims = args.recon_sims
+    res = reconstruct(h_true, 1.0, scene, iterations=iters, sims=sims, per_texel=4, image=nf,
                       footprint_px=args.recon_footprint, params=params, seed=rank,
                       keep_plan=False, log_every=max(iters // 10, 1),
                       objective=args.recon_objective)
@@ -1020,17 +1021,18 @@ def run_reconstruction(args, rank, world, device):
     peak = torch.cuda.max_memory_allocated(device)
     # the phases of an iteration at the start (flat field), whatever the step size did later
     phases = iteration_phases(1.0, res["target"], scene, torch.zeros_like(h_true),
-                              torch.ones_like(h_true), params, sims=16, per_texel=4, image=nf,
+                              torch.ones_like(h_true), params, sims=sims, per_texel=4, image=nf,
                               footprint_px=args.recon_footprint, seed=rank + 99,
                               objective=args.recon_objective)
     return {"metric": "Landweber it/s", "value": iters / (ms / 1e3), "unit": "it/s",
             "n_gpus": world, "steps": iters, "warmup": 0, "ms_per_step": ms / iters,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "recon1024: 1024^2 field, 16 sims x 2^22 photons per "
+            "config": {"workload": f"recon1024: 1024^2 field, {sims} sims x 2^22 photons per "
                                    "iteration into 1024^2, positions recomputed in backward",
                        "photons_per_iteration": res["photons_per_iteration"],
                        "objective": args.recon_objective, "tau": args.recon_tau,
+                       "bump_amplitude_mm": args.recon_amplitude,
                        "footprint_px": args.recon_footprint},
             "final_height_rmse_mm": res["rmse"],
             "initial_height_rmse_mm": float((d_true ** 2).mean().sqrt()),
@@ -1068,6 +1070,10 @@ def main():
     ap.add_argument("--recon-tau", type=float, default=1e-7,
                     help="recon1024: gradient step (the reference's tau_pixel; its default "
                          "0.1 diverges on this scene with the l2_sq data term)")
+    ap.add_argument("--recon-sims", type=int, default=16,
+                    help="recon1024: simulations per iteration (2^22 photons each)")
+    ap.add_argument("--recon-amplitude", type=float, default=0.05,
+                    help="recon1024: largest bump amplitude of the true field (mm)")
     ap.add_argument("--recon-footprint", type=float, default=3.0,
                     help="recon1024: initial photon footprint in receiver pixels")
     args = ap.parse_args()

@@ -14,11 +14,13 @@
 //                       (model/caustics.py:224-239); degenerate photons get channel -1
 // and writes the splat inputs (Ep, xp, Mp, cp, radius) in the reference's layouts.
 //
-// The backward recomputes the chain from h (nothing is stored between the passes) in
-// forward-mode dual numbers over the seven height-dependent scalars of the photon (height,
-// N~x, N~y and their x/y derivatives), contracts with the splat-input gradients, and maps
-// the result back onto the photon's 4x4 texel patch through the transposed bilinear and
-// Sobel stencils. Patches are accumulated with global float adds.
+// The backward recomputes the chain from h (nothing is stored between the passes), takes the
+// derivatives of the splat-input gradients' contraction with respect to the seven
+// height-dependent scalars of the photon (height, N~x, N~y and their x/y derivatives) -- by a
+// hand-written reverse-mode sweep for collimated light, by forward-mode dual numbers for the
+// traced point-light path -- and maps them back onto the photon's 4x4 texel patch through the
+// transposed bilinear and Sobel stencils. A CTA's patches are summed in shared memory where
+// its photons share a compact region of the field, else added with global float atomics.
 #include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
