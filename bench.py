@@ -223,6 +223,26 @@ def box_pixels(specs, photons, mpr):
     return total
 
 
+def h2d_bandwidth(device, nbytes=1 << 30, reps=3):
+    """Pinned host -> device copy bandwidth (GB/s) of one large copy, best of reps."""
+    host = torch.empty(nbytes // 4, dtype=torch.float32).pin_memory()
+    dev = torch.empty(nbytes // 4, dtype=torch.float32, device=device)
+    dev.copy_(host, non_blocking=True)
+    torch.cuda.synchronize(device)
+    best = None
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dev.copy_(host, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize(device)
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del host, dev
+    return nbytes / (best * 1e6)
+
+
 def support_pixels(specs, photons, mpr):
     """Pixels inside the kernel's support (|M d| < 1) per direction: the footprint ellipse's
     area, pi (W/2)(H/2) / |det M|, capped by its clipped box (the reference evaluates the
@@ -454,6 +474,7 @@ def run_ours(args, rank, world, device):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world, device)
+    h2d_gbs = h2d_bandwidth(device)
     clocks.stop()
 
     # ---- roofline of the dominant phase ----
@@ -507,7 +528,13 @@ def run_ours(args, rank, world, device):
                                         "inside the kernel's support",
                           "support_pixels_per_step": pix_sup, "box_pixels_per_step": pix_box},
         "e2e": {"value": photons_all / (e2e_ms / 1e3), "unit": UNIT,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4,
+                "ms_per_step": e2e_ms,
+                # the step's copies against this box's pinned host->device bandwidth
+                "h2d_gbs": h2d / (e2e_ms * 1e6), "h2d_peak_gbs": h2d_gbs,
+                "h2d_frac": (h2d / (e2e_ms * 1e6)) / h2d_gbs if h2d_gbs else None,
+                "h2d_peak_source": "one 1 GiB cudaMemcpyAsync from pinned host memory, best "
+                                   "of 3, measured in this run"},
         "roofline_step": step_roofline,
         "gpu_launches": launches_per_step * args.steps,
         "parity_vs_oracle": parity,

@@ -249,7 +249,8 @@ int pds_batch_refract_backward_f32(const float* height, int32_t rows, int32_t co
 /* Entry points of rows * cols * per_texel photons (per_texel per texel of a rows x cols
  * height field of edge `texel`, centred on the origin), each jittered uniformly inside its
  * texel (the reference's per-pixel random surface samples, model/caustics.py:78-83):
- * px[i], py[i] for photon i = texel index * per_texel + k. The offsets come from Philox4x32-10
+ * px[i], py[i] for photon i = k * rows * cols + texel index (per_texel samples of one photon
+ * per texel in raster order, as the reference's simulations sample). The offsets come from Philox4x32-10
  * (Salmon et al., SC 2011) keyed by `seed`; photons 2j and 2j + 1 use counter block
  * offset + j, so a call is a pure function of (seed, offset) and calls with offsets advanced
  * by ceil(n / 2) draw disjoint streams. */

@@ -32,7 +32,8 @@ def philox4x32_10(ctr, key):
 
 def photon_source(rows, cols, per_texel, texel, seed, offset):
     """(px, py) float32 [rows * cols * per_texel]: photons 2j, 2j + 1 from counter block
-    offset + j (words 0, 1 and 2, 3), offsets from the top 24 bits of each word."""
+    offset + j (words 0, 1 and 2, 3), offsets from the top 24 bits of each word; photon i in
+    texel i % (rows * cols) (per_texel samples of one photon per texel, raster order)."""
     n = rows * cols * per_texel
     pairs = (n + 1) // 2
     ctr = np.uint64(offset) + np.arange(pairs, dtype=np.uint64)
@@ -43,7 +44,7 @@ def photon_source(rows, cols, per_texel, texel, seed, offset):
     u[0, 0::2], u[1, 0::2], u[0, 1::2], u[1, 1::2] = r[0], r[1], r[2], r[3]
     j = (u[:, :n] >> np.uint64(8)).astype(np.float32) * np.float32(1.0 / 16777216.0)
     j = j - np.float32(0.5)
-    t = np.arange(n) // per_texel
+    t = np.arange(n) % (rows * cols)
     iy = (t // cols).astype(np.float32)
     ix = (t % cols).astype(np.float32)
     cx, cy = np.float32(0.5 * (cols - 1)), np.float32(0.5 * (rows - 1))

@@ -67,9 +67,14 @@ def _corner_offset(p_c, W, x):
 def plan_keys(photons, sims, max_pixel_radius, tile=64, apron_max=32, class_bits=6):
     """Keys of every photon. ``photons``: (Ep, xp, Mp, cp, radius) numpy arrays in the
     reference's layouts (float32 values); ``sims``: list of (n_photons, (C, H, W)), photons
-    concatenated in that order. -> (keys uint64 [N], n_tiles)."""
-    if class_bits != 6:
-        raise NotImplementedError("the restatement covers the row classes (class_bits 6)")
+    concatenated in that order. -> (keys uint64 [N], n_tiles).
+
+    class_bits 6: the full keys (the row walk's classes, computed with correctly rounded
+    operations on the device). Other class_bits: the keys with the class field zero, since the
+    band walk's area classes come from the device's approximate reciprocal square root; compare
+    ``key >> class_bits`` (simulation, channel and tile, and the two sentinels) for those."""
+    if not 1 <= class_bits <= 6:
+        raise ValueError("class_bits must be in [1, 6]")
     E, X, M, C, R = photons
     X = np.asarray(X, F32)
     M = np.asarray(M, F32)
@@ -100,7 +105,7 @@ def plan_keys(photons, sims, max_pixel_radius, tile=64, apron_max=32, class_bits
         dy0 = _corner_offset(pyc, H, X[1, sl])
         cls = row_class(M[0, 0, sl], M[0, 1, sl], M[1, 0, sl], M[1, 1, sl], dy0, W, H, rx,
                         x0 - pxc, x1 - pxc, y0 - pyc, y1 - pyc)
-        cls = np.where(ell != 0, cls, 63)
+        cls = np.where(ell != 0, cls, 63) if class_bits == 6 else np.zeros_like(cls)
         k = (t << class_bits) | cls
         keys[sl] = np.where(~valid, key_invalid, np.where(wide, key_big, k))
         b += n

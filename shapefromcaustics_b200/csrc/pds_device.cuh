@@ -338,9 +338,16 @@ __device__ __forceinline__ uint32_t plan_row_class(float m00, float m01, float m
 
 // delta = (2 p_c / w - 1) - x in double (separately rounded operations, in this order),
 // rounded once to float.
+__device__ __forceinline__ float corner_offset_step(int32_t p_c, double step, float x) {
+    return float(__dsub_rn(__dsub_rn(__dmul_rn(double(p_c), step), 1.0), double(x)));
+}
+
+// step = 2 / W of corner_offset, for callers that hoist it out of a loop over photons of one
+// image (the same correctly rounded division, so the same offsets)
+__device__ __forceinline__ double corner_step(int32_t W) { return __ddiv_rn(2.0, double(W)); }
+
 __device__ __forceinline__ float corner_offset(int32_t p_c, int32_t W, float x) {
-    return float(__dsub_rn(__dsub_rn(__dmul_rn(double(p_c), __ddiv_rn(2.0, double(W))), 1.0),
-                           double(x)));
+    return corner_offset_step(p_c, corner_step(W), x);
 }
 
 // Predicated shared-memory add without a branch (the compiler otherwise branches around

@@ -69,9 +69,10 @@ __device__ __forceinline__ void zero_window(uint32_t* hist, int window) {
 // path when PLACE, its 32-byte record. Both passes run it on the same inputs, so they agree
 // on every key.
 template <bool PLACE>
-__device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim& sim, int64_t ch,
-                                               float x, float y, float rad, float e, float m00,
-                                               float m01, float m10, float m11, Rec& r) {
+__device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim& sim, double s2w,
+                                               double s2h, int64_t ch, float x, float y,
+                                               float rad, float e, float m00, float m01,
+                                               float m10, float m11, Rec& r) {
     const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
     const uint32_t cls_max = (1u << cb) - 1u;
     if (!(ch >= 0 && ch < sim.channels)) return a.key_invalid;
@@ -84,7 +85,7 @@ __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim&
     const int tx = pcx / T, ty = pcy / T;
     const uint32_t tile = uint32_t(sim.tile_base) +
                           uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
-    const float dy0 = corner_offset(f.py_c, sim.height, y);
+    const float dy0 = corner_offset_step(f.py_c, s2h, y);
     uint32_t cls = min(uint32_t(max(f.rx, f.ry)), cls_max);
     if (cb == kRowClassBits) {
         // the row walk's classes: rows and row width inside the box
@@ -94,7 +95,7 @@ __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim&
     } else if (a.cfg.band) {
         // photons of a warp then have similar band areas (trip counts): classes of 1/k octave
         // of the area, k = 1, 2, 3 for up to 3, 4 and 5 class bits
-        const float dx0 = corner_offset(f.px_c, sim.width, x);
+        const float dx0 = corner_offset_step(f.px_c, s2w, x);
         const float sy = float(2.0 / double(sim.height));
         const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy, 0.5f * float(sim.width),
                                   0.5f * float(sim.height), float(f.rx) + 1.f);
@@ -110,7 +111,7 @@ __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim&
     }
     if (PLACE) {
         const uint32_t flags = (f.ellipse_all ? kFlagEllipseAll : 0u) | (e > 0.f ? 0u : kFlagFwdSkip);
-        r.dx0 = corner_offset(f.px_c, sim.width, x);
+        r.dx0 = corner_offset_step(f.px_c, s2w, x);
         r.dy0 = dy0;
         r.m00 = m00;
         r.m01 = m01;
@@ -162,6 +163,8 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
     int sidx = find_sim_of_photon(a.sims, min(r0 + int64_t(threadIdx.x), n - 1));
     pds_sim sim = load_sim(a.sims, sidx);
     int64_t next_begin = sim_end(a.sims, sidx);
+    // the pixel pitch in normalised coordinates (2 / W, 2 / H) of the thread's simulation
+    double s2w = corner_step(sim.width), s2h = corner_step(sim.height);
     // whole warps step together (the wide list's ballot needs every lane)
     int64_t nch = 0;
     float nx = 0.f, ny = 0.f, nrad = 0.f, ne = 0.f, n00 = 0.f, n01 = 0.f, n10 = 0.f, n11 = 0.f;
@@ -196,8 +199,10 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
                 ++sidx;
                 sim = load_sim(a.sims, sidx);
                 next_begin = sim_end(a.sims, sidx);
+                s2w = corner_step(sim.width);
+                s2h = corner_step(sim.height);
             }
-            key = bin_photon<PLACE>(a, sim, ch, x, y, rad, e, m00, m01, m10, m11, r);
+            key = bin_photon<PLACE>(a, sim, s2w, s2h, ch, x, y, rad, e, m00, m01, m10, m11, r);
         }
         const bool tile_path = key < a.key_big;
         if (PLACE) {

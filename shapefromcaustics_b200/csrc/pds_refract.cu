@@ -611,8 +611,9 @@ __device__ __forceinline__ void scatter_patch(int H, int W, float texel, const B
 }
 
 // The height-field gradient of a CTA's photons: where the CTA's photons share a compact patch
-// of the field (the photon source emits photons texel by texel, so a CTA's 256 consecutive
-// photons sit in a few texel rows), their patches are summed in shared memory and added to the
+// of the field (the photon source emits each sample's photons texel by texel in raster order,
+// so a CTA's 256 consecutive photons sit in one or two texel rows), their patches are summed
+// in shared memory and added to the
 // field once per texel; otherwise (scattered hits) each patch entry is a global atomic add.
 // Without it, every photon's 16 patch entries were global atomics on a few hot texels.
 constexpr int kPatchSmem = 8192;  // floats of the CTA's shared patch region (32 KB)
@@ -688,7 +689,9 @@ __device__ __forceinline__ void patch_end(const PatchAcc& acc, int* bb, int H, i
     __syncthreads();
 }
 
-__global__ __launch_bounds__(256) void refract_bwd_kernel(RefractArgs a) {
+// Three CTAs an SM (80 registers, a few spilled to the L1): measured 18% faster than the
+// 114-register build at two CTAs an SM (16.8 M photons of a 1024^2 field: 2.24 vs 2.73 ms).
+__global__ __launch_bounds__(256, 3) void refract_bwd_kernel(RefractArgs a) {
     __shared__ float smem[kPatchSmem];
     __shared__ int bb[4];
     const int64_t n = a.n;

@@ -1,10 +1,14 @@
 // Device photon source for the height-field plate (sm_100a): per_texel photon entry points per
-// texel, jittered uniformly inside the texel.
+// texel, jittered uniformly inside the texel, as per_texel samples of one photon per texel
+// each (photon i: sample i / texels of texel i % texels, texels in raster order).
 //
 // Reference: the per-pixel random sampling of the surface in model/caustics.py:78-83
-// (rand_like offsets of up to half a texel in each direction) and the per-simulation
-// repetition of the reference's loop; there the offsets come from torch's generator on the
-// host side of each simulation. Here they come from a counter-based generator, Philox4x32
+// (rand_like offsets of up to half a texel in each direction, one photon per texel) and the
+// per-simulation repetition of the reference's loop, which the samples follow; there the
+// offsets come from torch's generator on the host side of each simulation. Consecutive
+// photons therefore come from neighbouring texels, not from one texel: the splat's tile
+// kernels and the refraction backward's patch sums then see spread-out pixels and texels
+// instead of the same few. Here they come from a counter-based generator, Philox4x32
 // with 10 rounds (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy as 1, 2, 3",
 // SC 2011): the offsets of photon i are a pure function of (seed, offset + i), so a batch of
 // simulations draws disjoint streams by offset, with no generator state, no host round trip
@@ -43,6 +47,7 @@ __global__ __launch_bounds__(256) void source_kernel(int32_t rows, int32_t cols,
                                                      float* __restrict__ px,
                                                      float* __restrict__ py) {
     const int64_t pairs = (n + 1) >> 1;
+    const int64_t texels = int64_t(rows) * cols;
     const float cx = 0.5f * float(cols - 1), cy = 0.5f * float(rows - 1);
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < pairs;
          k += int64_t(gridDim.x) * blockDim.x) {
@@ -54,7 +59,7 @@ __global__ __launch_bounds__(256) void source_kernel(int32_t rows, int32_t cols,
         for (int h = 0; h < 2; ++h) {
             const int64_t i = 2 * k + h;
             if (i >= n) break;
-            const int64_t t = i / per_texel;
+            const int64_t t = i % texels;
             const float iy = float(t / cols), ix = float(t % cols);
             const float jx = unit24(h ? r.z : r.x) - 0.5f, jy = unit24(h ? r.w : r.y) - 0.5f;
             px[i] = (ix + jx - cx) * texel;

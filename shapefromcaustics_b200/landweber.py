@@ -70,7 +70,7 @@ def render_plate(height, scene, px, py, flux, params, shape, max_pixel_radius=20
 def photon_source(H, W, per_texel, texel, seed, offset, device, out=None):
     """Entry points of ``per_texel`` uniformly jittered photons per texel from the device
     source (``pds_photon_source_f32``: Philox4x32-10 keyed by ``seed``, counter blocks from
-    ``offset``, two photons a block). Returns ``(px, py, next_offset)``; passing
+    ``offset``, two photons a block; photon i in texel i % (H W)). Returns ``(px, py, next_offset)``; passing
     ``next_offset`` to the next call draws a disjoint stream. ``out``: optional ``(px, py)``
     float32 device tensors of ``H * W * per_texel`` elements to write into."""
     n = H * W * per_texel
@@ -88,10 +88,12 @@ def photon_source(H, W, per_texel, texel, seed, offset, device, out=None):
 
 
 def jitter(H, W, scene, per_texel, generator, device):
-    """Entry points of ``per_texel`` uniformly jittered photons per texel, on the device."""
+    """Entry points of ``per_texel`` uniformly jittered photons per texel, on the device:
+    ``per_texel`` samples of one photon per texel in raster order (photon i in texel
+    i % (H W)), like the device source."""
     n = H * W * per_texel
     idx = torch.arange(n, device=device)
-    texel = idx // per_texel
+    texel = idx % (H * W)
     iy = (texel // W).float()
     ix = (texel % W).float()
     j = torch.rand((2, n), generator=generator, device=device) - 0.5

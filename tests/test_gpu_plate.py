@@ -133,7 +133,7 @@ def test_photon_source_matches_philox_restatement(cuda):
     assert not np.array_equal(qx.cpu().numpy(), rx)
     # many photons: offsets uniform inside the texel
     px, py, _ = photon_source(64, 64, 16, 1.0, 7, 0, "cuda")
-    t = torch.arange(px.numel(), device="cuda") // 16
+    t = torch.arange(px.numel(), device="cuda") % (64 * 64)
     jx = (px - ((t % 64).float() - 31.5)).cpu().numpy()
     assert abs(jx.mean()) < 5e-3 and abs(jx.var() - 1 / 12) < 2e-3
     assert jx.min() >= -0.5 and jx.max() <= 0.5  # (ix + j rounds to the texel edge at most)

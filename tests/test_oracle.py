@@ -177,6 +177,6 @@ def test_photon_source_restatement_stays_in_texels():
     from oracle import philox as P
     px, py = P.photon_source(5, 7, 3, 0.25, seed=99, offset=4)
     assert px.shape == (105,) and px.dtype == np.float32
-    t = np.arange(105) // 3
+    t = np.arange(105) % 35  # sample-major: photon i in texel i % (rows * cols)
     assert np.all(np.abs(px / 0.25 - (t % 7 - 3.0)) <= 0.5)
     assert np.all(np.abs(py / 0.25 - (t // 7 - 2.0)) <= 0.5)
