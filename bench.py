@@ -270,9 +270,11 @@ def support_pixels(specs, photons, mpr):
 # Measured DRAM traffic per photon of each phase's kernels (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum on the 2^23-photon 1024^2 workload, profiles/*__medium.md), scaled to
 # a workload by its photon count.
-TRAFFIC_PER_PHOTON = {"forward": (260.905472e6 + 6.596352e6) / 2 ** 23,
-                      "backward": (261.127424e6 + 214.321152e6 + 401.621504e6 +
-                                   264.316160e6) / 2 ** 23}
+TRAFFIC_PER_PHOTON = {"plan": (309.575680e6 + 11.353344e6 + 350.295808e6 +
+                               254.379520e6) / 2 ** 23,
+                      "forward": (260.904448e6 + 7.644416e6) / 2 ** 23,
+                      "backward": (261.133568e6 + 214.625280e6 + 327.432192e6 +
+                                   261.902592e6) / 2 ** 23}
 
 
 # ------------------------------------------------------------------ our arm --------------
@@ -492,12 +494,16 @@ def run_ours(args, rank, world, device):
                      "algorithmic_bytes": step_bytes,
                      "achieved": step_bytes / (ms_per_step / 1e3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": step_bytes / (ms_per_step / 1e3) / 1e9 / peak,
-                     "peak_source": peak_kind}
+                     "peak_source": peak_kind,
+                     # DRAM bytes the step's kernels move per photon (ncu, medium workload)
+                     # against the 116 algorithmic bytes per photon
+                     "traffic_per_photon": sum(TRAFFIC_PER_PHOTON.values()),
+                     "traffic": sum(TRAFFIC_PER_PHOTON.values()) * n_total}
     achieved = alg[dom] / (ph_ms[dom] / 1e3) / 1e9
     simt = flops[dom] / (ph_ms[dom] / 1e3) / 1e12
-    # plan: plan_kernel, bucket_reduce/top/down, bucket_scatter, chunk_tile_kernel;
-    # forward: fwd_tiles_kernel, tail_fwd_kernel; backward: bwd_tiles_kernel, tail_bwd_kernel,
-    # grad_scatter_kernel
+    # plan: plan_pass_kernel<0> (count), bucket_reduce/top/down, plan_pass_kernel<1> (place),
+    # chunk_tile_kernel; forward: fwd_tiles_kernel, tail_fwd_kernel; backward:
+    # bwd_tiles_kernel, tail_bwd_kernel, grad_scatter4_kernel
     launches_per_step = 6 + 2 + 3
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -850,7 +856,8 @@ def run_plate_batch(args, device, steps, warmup, config=None):
     sources(0)
     target = batch.forward(h_tgt.contiguous(), px, py, flux).clone()
     base = 1.0
-    d = (h_true - base).clone()
+    d0 = (h_true - base).clone()
+    d = d0.clone()
     h = (base + d).contiguous()
     mask = torch.ones_like(d)
     vol = float(d.sum())
@@ -860,7 +867,13 @@ def run_plate_batch(args, device, steps, warmup, config=None):
     gimg = torch.empty_like(img)
     gh = torch.zeros_like(d)
 
+    # Every timed iteration starts from the same field (the true one): the iterations are
+    # timed, not the trajectory, and a step size that carried the field away (to the update's
+    # clamp bounds, with folded caustics and footprints at the radius cap) would time a
+    # different workload at every step.
     def batched_step():
+        d.copy_(d0)
+        torch.add(d, base, out=h)
         sources(0)
         batch.forward(h, px, py, flux, out=img)
         torch.sub(img, target, out=gimg)
@@ -872,6 +885,8 @@ def run_plate_batch(args, device, steps, warmup, config=None):
     t_views = batch.images(target)
 
     def plain_step():
+        d.copy_(d0)
+        torch.add(d, base, out=h)
         gh.zero_()
         off = 0
         for k, ((n, shape, p), per, (vx, vy, vf)) in enumerate(zip(sims, per_texel, views)):
@@ -922,6 +937,8 @@ def run_plate_batch(args, device, steps, warmup, config=None):
     splat = batch.splat
     with torch.cuda.stream(stream):
         for rep in range(3):
+            d.copy_(d0)
+            torch.add(d, base, out=h)
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)]
             ev[0].record(stream)
             sources(0)
@@ -956,7 +973,8 @@ def run_plate_batch(args, device, steps, warmup, config=None):
                         "N_i ~ logU[2^16, 2^22] (whole photons per texel), images "
                         "{256,512,1024}^2, light tilt <= 5 deg, wavelength U[450,650] nm "
                         "(fused silica), 3-pixel footprints; one Landweber iteration "
-                        "(sources, refraction, splat, backward, update)",
+                        "(sources, refraction, splat, backward, update), each from the true "
+                        "field",
             "batched": "one CUDA graph: 64 source launches, one batched refraction, one plan / "
                        "forward / backward, one batched refraction backward, the update",
             "plain": "per simulation from Python: source, refraction, plan, forward, "
@@ -983,13 +1001,16 @@ def run_landweber_step(args, rank, world, device):
     with torch.no_grad():
         target = PlateSplat.apply(h_tgt, px, py, flux, pp, shape, MPR, False)
     base = 1.0
-    d = (h_true - base).clone()
+    d0 = (h_true - base).clone()
+    d = d0.clone()
     mask = torch.ones_like(d)
     vol = float(d.sum())
     params = LandweberParams(d1=0.75 * vol, d2=1.25 * vol)
     tn = float((target * target).sum())
     ws = torch.empty(1 << 22, dtype=torch.uint8, device=device)
     def step():
+        # every iteration from the same field (see run_plate_batch)
+        d.copy_(d0)
         hv = (base + d).requires_grad_(True)
         im = PlateSplat.apply(hv, px, py, flux, pp, shape, MPR, True)
         loss = 0.5 * ((im - target) ** 2).sum() / tn
@@ -1016,7 +1037,8 @@ def run_landweber_step(args, rank, world, device):
             "config": {"workload": "landweber256: 256^2 height field (1 mm + 32 bumps), 4 "
                                    "jittered photons/texel (262144), n=1.5, receiver 50 mm, "
                                    "512^2 image, L2 vs second field; refraction + splat "
-                                   "fwd/bwd + fused update", "photons": n,
+                                   "fwd/bwd + fused update; each iteration from the true "
+                                   "field", "photons": n,
                        "launch_config": "library default"}}
 
 

