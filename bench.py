@@ -894,8 +894,6 @@ def run_plate_batch(args, device, steps, warmup, config=None):
             inputs = PL.refract_forward(h, vx, vy, vf, p)
             plan = SplatPlan(*inputs, shape, MPR)
             g = plan.forward() - t_views[k]
-            inputs = PL.refract_forward(h, vx, vy, vf, p)
-            plan.inputs = inputs
             gE, gX, gM = plan.backward(g)
             PL.refract_backward(h, vx, vy, vf, p, gE, gX, gM, grad_height=gh)
         landweber_update(d, gh, mask, params, ws)
@@ -931,8 +929,8 @@ def run_plate_batch(args, device, steps, warmup, config=None):
     ms_p = e0.elapsed_time(e1) / k
     del graph
     # phases of the batched step (eager, CUDA events on the stream)
-    names = ["sources", "refract_fwd", "plan", "splat_fwd", "data_grad", "refract_fwd_again",
-             "splat_bwd", "refract_bwd", "update"]
+    names = ["sources", "refract_fwd", "plan", "splat_fwd", "data_grad", "splat_bwd",
+             "refract_bwd", "update"]
     acc = {k: [] for k in names}
     splat = batch.splat
     with torch.cuda.stream(stream):
@@ -951,16 +949,13 @@ def run_plate_batch(args, device, steps, warmup, config=None):
             ev[4].record(stream)
             torch.sub(img, target, out=gimg)
             ev[5].record(stream)
-            inputs = batch._inputs(h, px, py, flux)
+            gE, gX, gM = splat.backward(gimg)  # the forward's splat inputs, kept
             ev[6].record(stream)
-            splat.inputs = inputs
-            gE, gX, gM = splat.backward(gimg)
-            ev[7].record(stream)
             gh.zero_()
             check_refract_backward(batch, h, px, py, flux, gE, gX, gM, gh)
-            ev[8].record(stream)
+            ev[7].record(stream)
             landweber_update(d, gh, mask, params, ws)
-            ev[9].record(stream)
+            ev[8].record(stream)
             torch.cuda.synchronize()
             for k, nm in enumerate(names):
                 acc[nm].append(ev[k].elapsed_time(ev[k + 1]))
@@ -976,9 +971,10 @@ def run_plate_batch(args, device, steps, warmup, config=None):
                         "(sources, refraction, splat, backward, update), each from the true "
                         "field",
             "batched": "one CUDA graph: 64 source launches, one batched refraction, one plan / "
-                       "forward / backward, one batched refraction backward, the update",
+                       "forward / backward, one batched refraction backward, the update; the "
+                       "refracted splat inputs kept from forward to backward",
             "plain": "per simulation from Python: source, refraction, plan, forward, "
-                     "refraction (recomputed), backward, refraction backward; then the update"}
+                     "backward, refraction backward; then the update"}
 
 
 def run_landweber_step(args, rank, world, device):
@@ -1044,9 +1040,9 @@ def run_landweber_step(args, rank, world, device):
 
 def run_reconstruction(args, rank, world, device):
     """Full reconstruction: 1024^2 field, 16 simulations x 4 photons per texel (2^22 each,
-    67M per iteration) into a 1024^2 image, Landweber iterations with the refracted photon
-    positions recomputed in the backward; final height RMSE, peak HBM and the CUDA-event time
-    of each phase of one iteration."""
+    67M per iteration) into a 1024^2 image, Landweber iterations (the plan and the refracted
+    splat inputs kept from forward to backward unless --recon-lean); final height RMSE, peak
+    HBM and the CUDA-event time of each phase of one iteration."""
     from shapefromcaustics_b200.landweber import LandweberParams, iteration_phases, reconstruct
     torch.cuda.set_device(device)
     nf = 1024
@@ -1062,7 +1058,7 @@ def run_reconstruction(args, rank, world, device):
     sims = args.recon_sims
     res = reconstruct(h_true, 1.0, scene, iterations=iters, sims=sims, per_texel=4, image=nf,
                       footprint_px=args.recon_footprint, params=params, seed=rank,
-                      keep_plan=False, log_every=max(iters // 10, 1),
+                      keep_plan=not args.recon_lean, log_every=max(iters // 10, 1),
                       objective=args.recon_objective)
     t1.record()
     torch.cuda.synchronize()
@@ -1072,16 +1068,18 @@ def run_reconstruction(args, rank, world, device):
     phases = iteration_phases(1.0, res["target"], scene, torch.zeros_like(h_true),
                               torch.ones_like(h_true), params, sims=sims, per_texel=4, image=nf,
                               footprint_px=args.recon_footprint, seed=rank + 99,
-                              objective=args.recon_objective)
+                              objective=args.recon_objective, keep_plan=not args.recon_lean)
     return {"metric": "Landweber it/s", "value": iters / (ms / 1e3), "unit": "it/s",
             "n_gpus": world, "steps": iters, "warmup": 0, "ms_per_step": ms / iters,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": f"recon1024: 1024^2 field, {sims} sims x 2^22 photons per "
-                                   "iteration into 1024^2, positions recomputed in backward",
+                                   "iteration into 1024^2",
                        "photons_per_iteration": res["photons_per_iteration"],
                        "objective": args.recon_objective, "tau": args.recon_tau,
                        "bump_amplitude_mm": args.recon_amplitude,
+                       "kept_for_backward": "recomputed" if args.recon_lean else
+                       "plan and refracted splat inputs",
                        "footprint_px": args.recon_footprint},
             "final_height_rmse_mm": res["rmse"],
             "initial_height_rmse_mm": float((d_true ** 2).mean().sqrt()),
@@ -1123,6 +1121,9 @@ def main():
                     help="recon1024: simulations per iteration (2^22 photons each)")
     ap.add_argument("--recon-amplitude", type=float, default=0.05,
                     help="recon1024: largest bump amplitude of the true field (mm)")
+    ap.add_argument("--recon-lean", action="store_true",
+                    help="recon1024: recompute the refraction and the plan in the backward "
+                         "instead of keeping them (less memory)")
     ap.add_argument("--recon-footprint", type=float, default=3.0,
                     help="recon1024: initial photon footprint in receiver pixels")
     args = ap.parse_args()

@@ -103,7 +103,7 @@ def jitter(H, W, scene, per_texel, generator, device):
 
 
 def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image=1024,
-                footprint_px=3.0, params=None, mask=None, seed=0, keep_plan=False, target=None,
+                footprint_px=3.0, params=None, mask=None, seed=0, keep_plan=True, target=None,
                 log_every=0, objective="l2_sq"):
     """The reference's pixel-basis Landweber loop (``shape_from_caustics.py:343-420``,
     default options) for a height-field plate, all on the device.
@@ -111,8 +111,9 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
     Each iteration splats ``sims`` simulations of ``per_texel`` freshly jittered photons
     per texel into one image (the reference's sum over simulations, ``:351-353``), takes the
     data term against the target, back-propagates to the height-field offset through the splat
-    and refraction kernels (refracted positions recomputed, not stored) and applies the fused
-    projected update. ``objective``: ``"l2_sq"`` is the reference's data term
+    and refraction kernels and applies the fused projected update. ``keep_plan``: the splat
+    plan and the refracted splat inputs are kept from forward to backward (about 120 B per
+    photon held); False recomputes both in the backward. ``objective``: ``"l2_sq"`` is the reference's data term
     ``0.5 |I - T|^2`` (``hyperparameter_helper.py:29-30``, its default ``--data_norm``), for
     which ``params.tau`` is the reference's ``tau_pixel``; ``"normalized"`` divides it by
     ``|T|^2``. The logged discrepancy is the reference's ``sqrt(2 fdis) / |T|``
@@ -161,12 +162,13 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
 
 
 def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4, image=1024,
-                     footprint_px=3.0, seed=0, offset=0, objective="l2_sq", reps=3):
+                     footprint_px=3.0, seed=0, offset=0, objective="l2_sq", reps=3,
+                     keep_plan=True):
     """CUDA-event times (ms, median of ``reps``) of the phases of one Landweber iteration of
     ``reconstruct``, run phase by phase on the current stream: photon source, refraction
-    forward, plan, splat forward, data-term gradient, refraction recomputed for the backward,
-    splat backward, refraction backward, update. The height field is ``base + d``; ``d`` is
-    updated in place."""
+    forward, plan, splat forward, data-term gradient, (with ``keep_plan`` False: the
+    refraction and the plan recomputed for the backward,) splat backward, refraction backward,
+    update. The height field is ``base + d``; ``d`` is updated in place."""
     import statistics
     from .plate import plate_params, refract_backward, refract_forward
     from .splatting import SplatPlan
@@ -178,7 +180,7 @@ def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4,
     flux = torch.full((n,), 1.0 / n, device=dev)
     ws = torch.empty(int(lib().pds_landweber_workspace_bytes(H, W)), dtype=torch.uint8, device=dev)
     scale = 1.0 if objective == "l2_sq" else 1.0 / float((target * target).sum())
-    names = ["source", "refract_fwd", "plan", "splat_fwd", "data_grad", "refract_fwd_again",
+    names = ["source", "refract_fwd", "plan", "splat_fwd", "data_grad", "recompute",
              "splat_bwd", "refract_bwd", "update"]
     times = {k: [] for k in names}
     for r in range(reps + 1):
@@ -195,7 +197,8 @@ def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4,
         ev[4].record()
         g_img = ((img - target) * scale).contiguous()
         ev[5].record()
-        Ep, xp, Mp, cp, radius = refract_forward(hv, px, py, flux, pp)
+        if not keep_plan:
+            plan = SplatPlan(*refract_forward(hv, px, py, flux, pp), shape, 20)
         ev[6].record()
         gE, gX, gM = plan.backward(g_img)
         ev[7].record()
@@ -208,5 +211,7 @@ def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4,
             for k, name in enumerate(names):
                 times[name].append(ev[k].elapsed_time(ev[k + 1]))
     out = {k: statistics.median(v) for k, v in times.items()}
+    if keep_plan:
+        del out["recompute"]
     out["total"] = sum(out.values())
     return out

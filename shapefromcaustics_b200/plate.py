@@ -96,15 +96,21 @@ class PlateSplat(torch.autograd.Function):
         ctx.params = params
         ctx.shape = tuple(int(v) for v in output_size)
         ctx.mpr = int(max_pixel_radius)
+        # keep_plan: the plan and the refracted splat inputs are kept for the backward (the
+        # reference's PDS saves its inputs, model/photon_differential.py:10); otherwise both
+        # are recomputed there (less memory: 12 B per photon held instead of about 120 B)
         ctx.plan_ws = plan.ws if keep_plan else None
+        ctx.inputs = (Ep, xp, Mp, cp, radius) if keep_plan else None
         ctx.cfg = plan.cfg
         return img
 
     @staticmethod
     def backward(ctx, grad_img):
         h, px, py, flux = ctx.saved_tensors
-        # splat inputs are recomputed, not stored
-        Ep, xp, Mp, cp, radius = refract_forward(h, px, py, flux, ctx.params)
+        if ctx.inputs is not None:
+            Ep, xp, Mp, cp, radius = ctx.inputs
+        else:
+            Ep, xp, Mp, cp, radius = refract_forward(h, px, py, flux, ctx.params)
         if ctx.plan_ws is not None:
             plan = SplatPlan.__new__(SplatPlan)
             plan.n = Ep.numel()
@@ -119,6 +125,7 @@ class PlateSplat(torch.autograd.Function):
         gE, gX, gM = plan.backward(grad_img.contiguous())
         gh = refract_backward(h, px, py, flux, ctx.params, gE, gX, gM)
         ctx.plan_ws = None
+        ctx.inputs = None
         return gh, None, None, None, None, None, None, None
 
 
@@ -240,11 +247,13 @@ class BatchedPlate:
     entry points concatenated in order. The forward refracts every photon in one batched launch
     (``pds_batch_refract_forward_f32``) and splats all simulations through one plan and one
     forward (``BatchedSplat``); the backward runs the batched splat backward and one batched
-    refraction backward into the height field's gradient (refracted photons recomputed, not
-    stored). The reference runs its simulations one after another and sums them
-    (``shape_from_caustics.py:351-353``); ``images(flat)`` gives the per-simulation images."""
+    refraction backward into the height field's gradient. ``keep_inputs``: the refracted splat
+    inputs of the forward are kept for the backward (as the reference's PDS saves them);
+    False recomputes them there (48 B per photon less held between the passes). The reference
+    runs its simulations one after another and sums them (``shape_from_caustics.py:351-353``);
+    ``images(flat)`` gives the per-simulation images."""
 
-    def __init__(self, sims, max_pixel_radius, device, config=None):
+    def __init__(self, sims, max_pixel_radius, device, config=None, keep_inputs=True):
         from .splatting import BatchedSplat
         self.splat = BatchedSplat([(n, shape) for n, shape, _ in sims], max_pixel_radius,
                                   device, config=config)
@@ -264,6 +273,7 @@ class BatchedPlate:
             self.device)
         self.begins_dev = torch.tensor(begins, dtype=torch.int64, device=self.device)
         self.image_elems = self.splat.image_elems
+        self.keep_inputs = bool(keep_inputs)
 
     def _inputs(self, height, px, py, flux):
         n = self.n_total
@@ -288,14 +298,19 @@ class BatchedPlate:
         """Flat images of all simulations (plans the splat; keeps the plan for backward)."""
         inputs = self._inputs(height, px, py, flux)
         self.splat.plan(*inputs)
-        return self.splat.forward(out)
+        img = self.splat.forward(out)
+        if not self.keep_inputs:
+            self.splat.inputs = None
+        return img
 
     def backward(self, height, px, py, flux, grad_flat, grad_height=None):
         """Adds d L / d height for the flat images' gradient (after ``forward`` on the same
         height field and photons)."""
-        inputs = self._inputs(height, px, py, flux)
-        self.splat.inputs = inputs
+        if not self.keep_inputs or self.splat.inputs is None:
+            self.splat.inputs = self._inputs(height, px, py, flux)
         gE, gX, gM = self.splat.backward(grad_flat)
+        if not self.keep_inputs:
+            self.splat.inputs = None
         if grad_height is None:
             grad_height = torch.zeros_like(height)
         with torch.cuda.device(self.device):

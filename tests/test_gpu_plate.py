@@ -345,3 +345,22 @@ def test_batched_plate_equals_the_per_simulation_plates(cuda):
         assert rel_l2(img.cpu(), ref.detach().cpu()) < 1e-5
     torch.cuda.synchronize()
     assert rel_l2(hv.grad.cpu(), gsum.cpu()) < 1e-5
+
+
+def test_batched_plate_kept_and_recomputed_inputs_agree(cuda):
+    """The backward on the forward's kept splat inputs and on inputs recomputed from the
+    height field give the same height gradient (same kernels on the same inputs; only the
+    order of the float atomic sums into the field differs)."""
+    from shapefromcaustics_b200 import plate as PL
+    h, sims, photons = plate_batch()
+    cat = [torch.cat([p[k] for p in photons]).contiguous() for k in range(3)]
+    grads = []
+    for keep in (True, False):
+        batch = PL.BatchedPlate(sims, 20, "cuda", keep_inputs=keep)
+        img = batch.forward(h, *cat)
+        g = torch.randn(img.shape, generator=torch.Generator("cuda").manual_seed(4),
+                        device="cuda")
+        grads.append(batch.backward(h, *cat, g))
+        assert (batch.splat.inputs is not None) == keep
+    torch.cuda.synchronize()
+    assert rel_l2(grads[0].cpu(), grads[1].cpu()) < 1e-6
