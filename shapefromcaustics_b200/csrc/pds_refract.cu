@@ -231,16 +231,17 @@ __device__ __forceinline__ void acc3(V3a& a, const V3a& b) {
     a.x += b.x; a.y += b.y; a.z += b.z;
 }
 
-// transfer_z: out = D - (D.z / t.z) t + s (Dd - (Dd.z / t.z) t)
-__device__ __forceinline__ V3a tz_fwd(const V3a& D, const V3a& Dd, float s, const V3a& t) {
-    const float a = D.z / t.z, b = Dd.z / t.z;
+// transfer_z: out = D - (D.z / t.z) t + s (Dd - (Dd.z / t.z) t), with itz = 1 / t.z
+__device__ __forceinline__ V3a tz_fwd(const V3a& D, const V3a& Dd, float s, const V3a& t,
+                                      float itz) {
+    const float a = D.z * itz, b = Dd.z * itz;
     return pa(ma(D, sa(a, t)), sa(s, ma(Dd, sa(b, t))));
 }
 
 // adjoint of tz_fwd: accumulates into Db (D), Ddb (Dd), sb (s) and tb (t) from ob (out)
 __device__ __forceinline__ void tz_adj(const V3a& D, const V3a& Dd, float s, const V3a& t,
-                                       const V3a& ob, V3a& Db, V3a& Ddb, float& sb, V3a& tb) {
-    const float itz = 1.f / t.z;
+                                       float itz, const V3a& ob, V3a& Db, V3a& Ddb, float& sb,
+                                       V3a& tb) {
     const float a = D.z * itz, b = Dd.z * itz;
     acc3(Db, ob);
     const float ab = -da(ob, t);
@@ -256,7 +257,8 @@ __device__ __forceinline__ void tz_adj(const V3a& D, const V3a& Dd, float s, con
 
 // d L / d S for the collimated chain; L from the splat-input gradients (as in the backward
 // kernels): gx xr + gy yr + sum of gM times Mp + 4 flux gE / |den|. False for a degenerate
-// photon (den == 0: no gradient).
+// photon (den == 0: no gradient). Each quotient's denominator is inverted once (eight
+// reciprocals) and the sweep multiplies by the inverses.
 __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, float py,
                                                     const PlateParams& P, float gx, float gy,
                                                     float g0, float g1, float g3, float g4,
@@ -271,13 +273,13 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     const float inl = 1.f / nlen;
     const V3a n = sa(inl, Nt);
     const float nd = da(n, d);
-    const float au = P.du0 * n.x / nd, av = P.du0 * n.y / nd;
+    const float ind = 1.f / nd;
+    const float au = P.du0 * n.x * ind, av = P.du0 * n.y * ind;
     const V3a Du1 = ma(va(P.du0, 0.f, 0.f), sa(au, d));
     const V3a Dv1 = ma(va(0.f, P.du0, 0.f), sa(av, d));
     const V3a dNu = va(Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, 0.f);
     const V3a dNv = va(Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, 0.f);
-    const float nl3 = nn * nlen;
-    const float inl3 = 1.f / nl3;
+    const float inl3 = inl * inl * inl;  // 1 / (nn nlen)
     const float wu = da(Nt, dNu), wv = da(Nt, dNv);
     const V3a dnu = sa(inl3, ma(sa(nn, dNu), sa(wu, Nt)));
     const V3a dnv = sa(inl3, ma(sa(nn, dNv), sa(wv, Nt)));
@@ -285,37 +287,42 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     const float cosi = da(d, n);
     const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
     const float ng1 = -sqrtf(k1);
+    const float ing1 = 1.f / ng1;
     const float coso = e1 * cosi - ng1;
     const V3a t1 = ma(sa(e1, d), sa(coso, n));
-    const float f1 = e1 - (e1 * e1) * cosi / ng1;
+    const float f1 = e1 - (e1 * e1) * cosi * ing1;
     const float ddu = da(d, dnu), ddv = da(d, dnv);
     const float qu = f1 * ddu, qv = f1 * ddv;
     const V3a Ddu = sa(-1.f, pa(sa(coso, dnu), sa(qu, n)));
     const V3a Ddv = sa(-1.f, pa(sa(coso, dnv), sa(qv, n)));
-    const float s1 = -hz / t1.z;
-    const V3a Du2 = tz_fwd(Du1, Ddu, s1, t1);
-    const V3a Dv2 = tz_fwd(Dv1, Ddv, s1, t1);
+    const float it1z = 1.f / t1.z;
+    const float s1 = -hz * it1z;
+    const V3a Du2 = tz_fwd(Du1, Ddu, s1, t1, it1z);
+    const V3a Dv2 = tz_fwd(Dv1, Ddv, s1, t1, it1z);
     const float e2 = P.ior;
     const float c2 = t1.z;
     const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
     const float ng2 = -sqrtf(k2);
+    const float ing2 = 1.f / ng2;
     const float coso2 = e2 * c2 - ng2;
     const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
-    const float f2 = e2 - (e2 * e2) * c2 / ng2;
+    const float f2 = e2 - (e2 * e2) * c2 * ing2;
     const float q2u = f2 * Ddu.z, q2v = f2 * Ddv.z;
     const V3a Ddu2 = ma(sa(e2, Ddu), va(0.f, 0.f, q2u));
     const V3a Ddv2 = ma(sa(e2, Ddv), va(0.f, 0.f, q2v));
-    const float s2 = -P.dist / t2.z;
-    const V3a Du3 = tz_fwd(Du2, Ddu2, s2, t2);
-    const V3a Dv3 = tz_fwd(Dv2, Ddv2, s2, t2);
+    const float it2z = 1.f / t2.z;
+    const float s2 = -P.dist * it2z;
+    const V3a Du3 = tz_fwd(Du2, Ddu2, s2, t2, it2z);
+    const V3a Dv3 = tz_fwd(Dv2, Ddv2, s2, t2, it2z);
     const float Dux = P.inv_half * Du3.x, Duy = P.inv_half * Du3.y;
     const float Dvx = P.inv_half * Dv3.x, Dvy = P.inv_half * Dv3.y;
     const float den = Dux * Dvy - Duy * Dvx;
     if (den == 0.f) return false;
     // ---- output adjoints: L = gx xr + gy yr + (2 / den) A + cE / |den|
-    const float f = 2.f / den;
+    const float iden = 1.f / den;
+    const float f = 2.f * iden;
     const float A = g0 * Dvy - g1 * Dvx - g3 * Duy + g4 * Dux;
-    const float denb = -f * A / den - cE * copysignf(1.f, den) / (den * den);
+    const float denb = (-f * A - cE * copysignf(1.f, den) * iden) * iden;
     const float Duxb = f * g4 + denb * Dvy, Duyb = -f * g3 - denb * Dvx;
     const float Dvxb = -f * g1 - denb * Duy, Dvyb = f * g0 + denb * Dux;
     const float p2xb = P.inv_half * gx, p2yb = P.inv_half * gy;
@@ -323,11 +330,11 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     V3a t2b = va(P.inv_half * gx * s2, P.inv_half * gy * s2, 0.f);
     float s2b = P.inv_half * (gx * t2.x + gy * t2.y);
     V3a Du2b = va(0.f, 0.f, 0.f), Dv2b = Du2b, Ddu2b = Du2b, Ddv2b = Du2b;
-    tz_adj(Du2, Ddu2, s2, t2, va(P.inv_half * Duxb, P.inv_half * Duyb, 0.f), Du2b, Ddu2b, s2b,
-           t2b);
-    tz_adj(Dv2, Ddv2, s2, t2, va(P.inv_half * Dvxb, P.inv_half * Dvyb, 0.f), Dv2b, Ddv2b, s2b,
-           t2b);
-    t2b.z += s2b * P.dist / (t2.z * t2.z);
+    tz_adj(Du2, Ddu2, s2, t2, it2z, va(P.inv_half * Duxb, P.inv_half * Duyb, 0.f), Du2b, Ddu2b,
+           s2b, t2b);
+    tz_adj(Dv2, Ddv2, s2, t2, it2z, va(P.inv_half * Dvxb, P.inv_half * Dvyb, 0.f), Dv2b, Ddv2b,
+           s2b, t2b);
+    t2b.z += s2b * P.dist * it2z * it2z;
     // bottom refraction
     V3a Dub = sa(e2, Ddu2b), Dvb = sa(e2, Ddv2b);  // adjoints of Ddu, Ddv
     const float q2ub = -Ddu2b.z, q2vb = -Ddv2b.z;
@@ -336,9 +343,9 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     const float f2b = Ddu.z * q2ub + Ddv.z * q2vb;
     V3a t1b = sa(e2, t2b);
     const float coso2b = -t2b.z;
-    float c2b = e2 * coso2b - (e2 * e2) / ng2 * f2b;
-    float ng2b = -coso2b + (e2 * e2) * c2 / (ng2 * ng2) * f2b;
-    const float k2b = ng2b / (2.f * ng2);
+    float c2b = e2 * coso2b - (e2 * e2) * ing2 * f2b;
+    float ng2b = -coso2b + (e2 * e2) * c2 * ing2 * ing2 * f2b;
+    const float k2b = 0.5f * ng2b * ing2;
     c2b += 2.f * e2 * e2 * c2 * k2b;
     t1b.z += c2b;
     // bottom transfer
@@ -346,10 +353,10 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     float s1b = p2xb * t1.x + p2yb * t1.y;
     t1b.x += p2xb * s1;
     t1b.y += p2yb * s1;
-    tz_adj(Du1, Ddu, s1, t1, Du2b, Du1b, Dub, s1b, t1b);
-    tz_adj(Dv1, Ddv, s1, t1, Dv2b, Dv1b, Dvb, s1b, t1b);
-    const float hzb = -s1b / t1.z;
-    t1b.z += s1b * hz / (t1.z * t1.z);
+    tz_adj(Du1, Ddu, s1, t1, it1z, Du2b, Du1b, Dub, s1b, t1b);
+    tz_adj(Dv1, Ddv, s1, t1, it1z, Dv2b, Dv1b, Dvb, s1b, t1b);
+    const float hzb = -s1b * it1z;
+    t1b.z += s1b * hz * it1z * it1z;
     // top refraction (Dd = 0): Ddu = -(coso dnu + qu n), qu = f1 (d . dnu)
     V3a nb = va(0.f, 0.f, 0.f);
     float cosob = -da(Dub, dnu) - da(Dvb, dnv) - da(t1b, n);
@@ -361,9 +368,9 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     const float f1b = qub * ddu + qvb * ddv;
     acc3(dnub, sa(qub * f1, d));
     acc3(dnvb, sa(qvb * f1, d));
-    float cosib = e1 * cosob - (e1 * e1) / ng1 * f1b;
-    const float ng1b = -cosob + (e1 * e1) * cosi / (ng1 * ng1) * f1b;
-    const float k1b = ng1b / (2.f * ng1);
+    float cosib = e1 * cosob - (e1 * e1) * ing1 * f1b;
+    const float ng1b = -cosob + (e1 * e1) * cosi * ing1 * ing1 * f1b;
+    const float k1b = 0.5f * ng1b * ing1;
     cosib += 2.f * e1 * e1 * cosi * k1b;
     acc3(nb, sa(cosib, d));
     // dn = (nn dN - w Nt) / nl3
@@ -391,14 +398,14 @@ __device__ __forceinline__ bool plate_chain_adjoint(const float S[K], float px, 
     Dv1b.y += dNvb.x * Nxy + dNvb.y * Nyy;
     // Du1 = (du0, 0, 0) - au d, au = du0 n.x / nd (Dv1 with n.y)
     const float aub = -da(Du1b, d), avb = -da(Dv1b, d);
-    nb.x += aub * P.du0 / nd;
-    nb.y += avb * P.du0 / nd;
-    const float ndb = -(aub * au + avb * av) / nd;
+    nb.x += aub * P.du0 * ind;
+    nb.y += avb * P.du0 * ind;
+    const float ndb = -(aub * au + avb * av) * ind;
     acc3(nb, sa(ndb, d));
     // n = Nt / sqrt(nn)
     acc3(Ntb, sa(inl, nb));
     const float inlb = da(nb, Nt);
-    nnb += -0.5f * inl / nn * inlb;
+    nnb += -0.5f * inl * inl * inl * inlb;  // d inl / d nn = -1 / (2 nn^1.5)
     Sb[0] = hzb;
     Sb[1] = Ntb.x + 2.f * Nx * nnb;
     Sb[2] = Ntb.y + 2.f * Ny * nnb;
