@@ -151,8 +151,9 @@ __device__ __forceinline__ void refract(const V3<T>& d, const V3<T>& n, const V3
 template <class T>
 __device__ __forceinline__ V3<T> transfer_z(const V3<T>& D, const V3<T>& Dd, const T& s,
                                             const V3<T>& t) {
-    const T a = D.z / t.z;
-    const T b = Dd.z / t.z;
+    const T itz = cst<T>(1.f) / t.z;  // one quotient (the same t in both of a photon's calls)
+    const T a = D.z * itz;
+    const T b = Dd.z * itz;
     return vadd(vsub(D, vscale(a, t)), vscale(s, vsub(Dd, vscale(b, t))));
 }
 
@@ -170,8 +171,9 @@ __device__ __forceinline__ void plate_chain(const T& hz, const T& Nx, const T& N
     const V3<T> n = vscale(cst<T>(1.f) / nlen, Nt);
     const T nd = vdot(n, d);
     // source-plane differentials (du0, 0, 0) and (0, du0, 0) onto the tangent plane
-    const V3<T> Du1 = vsub(V3<T>{cst<T>(P.du0), cst<T>(0.f), cst<T>(0.f)}, vscale((P.du0 * n.x) / nd, d));
-    const V3<T> Dv1 = vsub(V3<T>{cst<T>(0.f), cst<T>(P.du0), cst<T>(0.f)}, vscale((P.du0 * n.y) / nd, d));
+    const T dnd = cst<T>(P.du0) / nd;
+    const V3<T> Du1 = vsub(V3<T>{cst<T>(P.du0), cst<T>(0.f), cst<T>(0.f)}, vscale(n.x * dnd, d));
+    const V3<T> Dv1 = vsub(V3<T>{cst<T>(0.f), cst<T>(P.du0), cst<T>(0.f)}, vscale(n.y * dnd, d));
     // derivative of the normalised normal along each positional differential
     const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
     const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
