@@ -451,7 +451,8 @@ struct SurfGeo {
 __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, float texel,
                                                 const Bilin& b, float s[K],
                                                 SurfGeo* geo = nullptr) {
-    const float c = -1.f / (8.f * texel);
+    const float itex = 1.f / texel;  // one quotient; the stencils multiply by it
+    const float c = -0.125f * itex;
     float hv[2][2], nx[2][2], ny[2][2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
@@ -473,12 +474,12 @@ __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, fl
         return top + (bot - top) * b.ay;
     };
     auto ddx = [&](float v[2][2]) {
-        return ((v[0][1] - v[0][0]) * (1.f - b.ay) + (v[1][1] - v[1][0]) * b.ay) / texel;
+        return ((v[0][1] - v[0][0]) * (1.f - b.ay) + (v[1][1] - v[1][0]) * b.ay) * itex;
     };
     auto ddy = [&](float v[2][2]) {
         const float top = v[0][0] + (v[0][1] - v[0][0]) * b.ax;
         const float bot = v[1][0] + (v[1][1] - v[1][0]) * b.ax;
-        return (bot - top) / texel;
+        return (bot - top) * itex;
     };
     s[0] = val(hv);
     s[1] = val(nx);
@@ -492,7 +493,7 @@ __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, fl
         // vary along y and the y derivatives along x by it)
         geo->hx = ddx(hv);
         geo->hy = ddy(hv);
-        const float it2 = 1.f / (texel * texel);
+        const float it2 = itex * itex;
         geo->tw_nx = ((nx[1][1] - nx[1][0]) - (nx[0][1] - nx[0][0])) * it2;
         geo->tw_ny = ((ny[1][1] - ny[1][0]) - (ny[0][1] - ny[0][0])) * it2;
     }
@@ -579,8 +580,8 @@ __device__ __forceinline__ void scatter_patch(int H, int W, float texel, const B
     for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int q = 0; q < 4; ++q) patch[r][q] = 0.f;
-    const float sob = -1.f / (8.f * texel);
     const float it = 1.f / texel;
+    const float sob = -0.125f * it;
     const float wv[2][2] = {{(1.f - b.ay) * (1.f - b.ax), (1.f - b.ay) * b.ax},
                             {b.ay * (1.f - b.ax), b.ay * b.ax}};
     const float wx[2][2] = {{-(1.f - b.ay) * it, (1.f - b.ay) * it}, {-b.ay * it, b.ay * it}};
