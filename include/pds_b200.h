@@ -64,7 +64,9 @@ typedef struct pds_config {
                            (2, 3 and 4 give the same result: pixels outside the support add
                            exactly zero); default 3 */
     int32_t min_blocks; /* resident CTAs per SM the tile kernels are compiled for: 2, 3 or 4
-                           (fewer: more registers per thread; more: more warps); default 3 */
+                           (fewer: more registers per thread; more: more warps); a value sets
+                           both directions; default (0): 3 for the forward, whose CTAs also
+                           stage their next records in shared memory, and 4 for the backward */
     int32_t coop_radius; /* footprints with a radius (px) of at least this are splatted by a
                            whole warp instead of one thread; -1 never; default -1 */
 } pds_config;

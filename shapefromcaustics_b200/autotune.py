@@ -19,14 +19,15 @@ __all__ = ["DEFAULT", "CANDIDATES", "signature", "pick", "tune_batch", "cached"]
 
 # the library default first; then tile, class bits, walk, CTAs per SM and the cooperative
 # splat in all combinations, and the default with smaller and larger work chunks (sorted
-# photons a CTA takes at a time)
-DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=3, coop_radius=-1)
+# photons a CTA takes at a time). min_blocks 0 is the library's choice per direction (3 CTAs
+# an SM for the forward, 4 for the backward); 4 sets both.
+DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=0, coop_radius=-1)
 CANDIDATES = [dict(tile=t, chunk=2048, class_bits=b, walk=w, min_blocks=m, coop_radius=k)
-              for t, b, w, m, k in itertools.product((64, 32), (5, 3), (3, 1), (3, 4), (-1, 8))]
+              for t, b, w, m, k in itertools.product((64, 32), (5, 3), (3, 1), (0, 4), (-1, 8))]
 CANDIDATES += [dict(DEFAULT, chunk=c) for c in (1024, 4096)]
 # the padded-row walk with its row classes, at both tile sizes and CTA counts
 CANDIDATES += [dict(tile=t, chunk=2048, class_bits=6, walk=4, min_blocks=m, coop_radius=-1)
-               for t, m in itertools.product((64, 32), (3, 4))]
+               for t, m in itertools.product((64, 32), (0, 4))]
 
 _cache = {}
 

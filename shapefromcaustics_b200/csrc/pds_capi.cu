@@ -103,7 +103,10 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, int64_t n, Resol
     r.cfg.spans = (c.walk == 2 || c.walk == 4) ? 1 : 0;
     r.cfg.band = c.walk == 3 ? 1 : 0;
     r.cfg.rows = c.walk == 4 ? 1 : 0;
+    // default: the forward at 3 CTAs an SM (room for its record staging buffers), the
+    // backward at 4 (measured best for each); an explicit min_blocks sets both
     r.cfg.min_blocks = c.min_blocks;
+    r.cfg.min_blocks_bwd = (in && in->min_blocks) ? c.min_blocks : 4;
     r.cfg.coop_r = c.coop_radius > 0 ? c.coop_radius : 0;
     r.n_buckets = n_tiles << c.class_bits;
     r.key_big = uint32_t(r.n_buckets);

@@ -73,7 +73,8 @@ struct Cfg {
     int32_t spans;       // 1: walk only the support's rows / row spans; 0: the whole box
     int32_t band;        // 1: walk each footprint's sheared band (see Band)
     int32_t rows;        // 1: walk the bands' rows padded to a common count and width per warp
-    int32_t min_blocks;  // resident CTAs per SM the tile kernels' register budget targets
+    int32_t min_blocks;  // resident CTAs per SM the forward tile kernels' register budget targets
+    int32_t min_blocks_bwd;  // the same for the backward tile kernels
     int32_t coop_r;      // footprint radius from which a photon is splatted by a whole warp
 };
 

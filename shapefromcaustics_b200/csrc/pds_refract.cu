@@ -16,10 +16,12 @@
 //
 // The backward recomputes the chain from h (nothing is stored between the passes), takes the
 // derivatives of the splat-input gradients' contraction with respect to the seven
-// height-dependent scalars of the photon (height, N~x, N~y and their x/y derivatives) -- by a
-// hand-written reverse-mode sweep for collimated light, by forward-mode dual numbers for the
-// traced point-light path -- and maps them back onto the photon's 4x4 texel patch through the
-// transposed bilinear and Sobel stencils. A CTA's patches are summed in shared memory where
+// height-dependent scalars of the photon (height, N~x, N~y and their x/y derivatives; for the
+// point light the hit parameter in place of the height) by a hand-written reverse-mode sweep,
+// and maps them back onto the photon's 4x4 texel patch through the transposed bilinear and
+// Sobel stencils. (The chain templates take T = float here; instantiated with forward-mode
+// dual numbers on the host they give the reference derivatives the sweeps were checked
+// against.) A CTA's patches are summed in shared memory where
 // its photons share a compact region of the field, else added with global float atomics.
 #include <climits>
 #include <cstdint>
@@ -32,64 +34,6 @@ namespace pds {
 namespace {
 
 constexpr int K = 7;  // height-dependent scalars of one photon
-
-struct Dual {
-    float v;
-    float d[K];
-};
-
-__device__ __forceinline__ Dual dconst(float v) {
-    Dual r;
-    r.v = v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = 0.f;
-    return r;
-}
-__device__ __forceinline__ Dual operator+(const Dual& a, const Dual& b) {
-    Dual r; r.v = a.v + b.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] + b.d[k];
-    return r;
-}
-__device__ __forceinline__ Dual operator-(const Dual& a, const Dual& b) {
-    Dual r; r.v = a.v - b.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] - b.d[k];
-    return r;
-}
-__device__ __forceinline__ Dual operator-(const Dual& a) {
-    Dual r; r.v = -a.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = -a.d[k];
-    return r;
-}
-__device__ __forceinline__ Dual operator*(const Dual& a, const Dual& b) {
-    Dual r; r.v = a.v * b.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = fmaf(a.d[k], b.v, a.v * b.d[k]);
-    return r;
-}
-__device__ __forceinline__ Dual operator*(float s, const Dual& a) {
-    Dual r; r.v = s * a.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = s * a.d[k];
-    return r;
-}
-__device__ __forceinline__ Dual operator/(const Dual& a, const Dual& b) {
-    const float inv = 1.f / b.v;
-    Dual r; r.v = a.v * inv;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * inv;
-    return r;
-}
-__device__ __forceinline__ Dual dsqrt(const Dual& a) {
-    Dual r; r.v = sqrtf(a.v);
-    const float h = 0.5f / r.v;
-#pragma unroll
-    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * h;
-    return r;
-}
-__device__ __forceinline__ Dual dabs(const Dual& a) { return a.v < 0.f ? -a : a; }
 
 __device__ __forceinline__ float dsqrt(float a) { return sqrtf(a); }
 
@@ -110,8 +54,6 @@ template <class T>
 __device__ __forceinline__ T cst(float v);
 template <>
 __device__ __forceinline__ float cst<float>(float v) { return v; }
-template <>
-__device__ __forceinline__ Dual cst<Dual>(float v) { return dconst(v); }
 
 struct PlateParams {
     float texel, ior, dist, inv_half, du0;
@@ -818,6 +760,172 @@ __device__ __forceinline__ void point_chain(const T& t, const T& Nx, const T& Ny
     Dvy = P.inv_half * Dv3.y;
 }
 
+// Reverse mode of point_chain (the adjoint sweep of plate_chain_adjoint with the point
+// light's differences: the hit p1 = o + t d moves with t, the positional differentials are
+// t (D - (n.D / n.d) d) for the light's direction differentials D, and the top refraction
+// carries those direction differentials). Returns d L / d t at fixed normal scalars (tb) and
+// d L / d S_k for the six normal scalars S[1..6]; L as in plate_chain_adjoint. False for a
+// degenerate photon.
+__device__ __forceinline__ bool point_chain_adjoint(float t, const float S[K], const Ray& r,
+                                                    const V3<float>& Dth,
+                                                    const V3<float>& Dph,
+                                                    const PlateParams& P, float gx, float gy,
+                                                    float g0, float g1, float g3, float g4,
+                                                    float cE, float& tb, float Sb[K]) {
+    const float Nx = S[1], Ny = S[2], Nxx = S[3], Nyx = S[4], Nxy = S[5], Nyy = S[6];
+    const V3a d = va(r.dx, r.dy, r.dz);
+    const V3a Dt = va(Dth.x, Dth.y, Dth.z), Dp = va(Dph.x, Dph.y, Dph.z);
+    // ---- forward
+    const V3a p1 = va(r.ox + t * d.x, r.oy + t * d.y, r.oz + t * d.z);
+    const V3a Nt = va(Nx, Ny, 1.f);
+    const float nn = Nx * Nx + Ny * Ny + 1.f;
+    const float nlen = sqrtf(nn);
+    const float inl = 1.f / nlen;
+    const V3a n = sa(inl, Nt);
+    const float nd = da(n, d);
+    const float ind = 1.f / nd;
+    const float aT = da(n, Dt) * ind, aP = da(n, Dp) * ind;
+    const V3a Eu = ma(Dt, sa(aT, d)), Ev = ma(Dp, sa(aP, d));
+    const V3a Du1 = sa(t, Eu), Dv1 = sa(t, Ev);
+    const V3a dNu = va(Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, 0.f);
+    const V3a dNv = va(Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, 0.f);
+    const float inl3 = inl * inl * inl;
+    const float wu = da(Nt, dNu), wv = da(Nt, dNv);
+    const V3a dnu = sa(inl3, ma(sa(nn, dNu), sa(wu, Nt)));
+    const V3a dnv = sa(inl3, ma(sa(nn, dNv), sa(wv, Nt)));
+    const float e1 = 1.f / P.ior;
+    const float cosi = da(d, n);
+    const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
+    const float ng1 = -sqrtf(k1);
+    const float ing1 = 1.f / ng1;
+    const float coso = e1 * cosi - ng1;
+    const V3a t1 = ma(sa(e1, d), sa(coso, n));
+    const float f1 = e1 - (e1 * e1) * cosi * ing1;
+    const float ddu = da(Dt, n) + da(d, dnu), ddv = da(Dp, n) + da(d, dnv);
+    const float qu = f1 * ddu, qv = f1 * ddv;
+    const V3a Ddu = ma(sa(e1, Dt), pa(sa(coso, dnu), sa(qu, n)));
+    const V3a Ddv = ma(sa(e1, Dp), pa(sa(coso, dnv), sa(qv, n)));
+    const float it1z = 1.f / t1.z;
+    const float s1 = -p1.z * it1z;
+    const V3a Du2 = tz_fwd(Du1, Ddu, s1, t1, it1z);
+    const V3a Dv2 = tz_fwd(Dv1, Ddv, s1, t1, it1z);
+    const float e2 = P.ior;
+    const float c2 = t1.z;
+    const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
+    const float ng2 = -sqrtf(k2);
+    const float ing2 = 1.f / ng2;
+    const float coso2 = e2 * c2 - ng2;
+    const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
+    const float f2 = e2 - (e2 * e2) * c2 * ing2;
+    const float q2u = f2 * Ddu.z, q2v = f2 * Ddv.z;
+    const V3a Ddu2 = ma(sa(e2, Ddu), va(0.f, 0.f, q2u));
+    const V3a Ddv2 = ma(sa(e2, Ddv), va(0.f, 0.f, q2v));
+    const float it2z = 1.f / t2.z;
+    const float s2 = -P.dist * it2z;
+    const V3a Du3 = tz_fwd(Du2, Ddu2, s2, t2, it2z);
+    const V3a Dv3 = tz_fwd(Dv2, Ddv2, s2, t2, it2z);
+    const float Dux = P.inv_half * Du3.x, Duy = P.inv_half * Du3.y;
+    const float Dvx = P.inv_half * Dv3.x, Dvy = P.inv_half * Dv3.y;
+    const float den = Dux * Dvy - Duy * Dvx;
+    if (den == 0.f) return false;
+    // ---- output adjoints
+    const float iden = 1.f / den;
+    const float f = 2.f * iden;
+    const float A = g0 * Dvy - g1 * Dvx - g3 * Duy + g4 * Dux;
+    const float denb = (-f * A - cE * copysignf(1.f, den) * iden) * iden;
+    const float Duxb = f * g4 + denb * Dvy, Duyb = -f * g3 - denb * Dvx;
+    const float Dvxb = -f * g1 - denb * Duy, Dvyb = f * g0 + denb * Dux;
+    const float p2xb = P.inv_half * gx, p2yb = P.inv_half * gy;
+    // ---- reverse sweep: receiver transfer and bottom refraction as for collimated light
+    V3a t2b = va(P.inv_half * gx * s2, P.inv_half * gy * s2, 0.f);
+    float s2b = P.inv_half * (gx * t2.x + gy * t2.y);
+    V3a Du2b = va(0.f, 0.f, 0.f), Dv2b = Du2b, Ddu2b = Du2b, Ddv2b = Du2b;
+    tz_adj(Du2, Ddu2, s2, t2, it2z, va(P.inv_half * Duxb, P.inv_half * Duyb, 0.f), Du2b, Ddu2b,
+           s2b, t2b);
+    tz_adj(Dv2, Ddv2, s2, t2, it2z, va(P.inv_half * Dvxb, P.inv_half * Dvyb, 0.f), Dv2b, Ddv2b,
+           s2b, t2b);
+    t2b.z += s2b * P.dist * it2z * it2z;
+    V3a Dub = sa(e2, Ddu2b), Dvb = sa(e2, Ddv2b);  // adjoints of Ddu, Ddv
+    const float q2ub = -Ddu2b.z, q2vb = -Ddv2b.z;
+    Dub.z += f2 * q2ub;
+    Dvb.z += f2 * q2vb;
+    const float f2b = Ddu.z * q2ub + Ddv.z * q2vb;
+    V3a t1b = sa(e2, t2b);
+    const float coso2b = -t2b.z;
+    float c2b = e2 * coso2b - (e2 * e2) * ing2 * f2b;
+    const float ng2b = -coso2b + (e2 * e2) * c2 * ing2 * ing2 * f2b;
+    const float k2b = 0.5f * ng2b * ing2;
+    c2b += 2.f * e2 * e2 * c2 * k2b;
+    t1b.z += c2b;
+    // bottom transfer from the hit p1 (p2 = p1 + s1 t1, s1 = -p1.z / t1.z)
+    V3a Du1b = va(0.f, 0.f, 0.f), Dv1b = Du1b;
+    float s1b = p2xb * t1.x + p2yb * t1.y;
+    t1b.x += p2xb * s1;
+    t1b.y += p2yb * s1;
+    tz_adj(Du1, Ddu, s1, t1, it1z, Du2b, Du1b, Dub, s1b, t1b);
+    tz_adj(Dv1, Ddv, s1, t1, it1z, Dv2b, Dv1b, Dvb, s1b, t1b);
+    const float p1zb = -s1b * it1z;
+    t1b.z += s1b * p1.z * it1z * it1z;
+    tb = p2xb * d.x + p2yb * d.y + p1zb * d.z;
+    // top refraction with the light's direction differentials:
+    // Ddu = e1 Dt - (coso dnu + qu n), qu = f1 (Dt . n + d . dnu)
+    V3a nb = va(0.f, 0.f, 0.f);
+    const float cosob = -da(Dub, dnu) - da(Dvb, dnv) - da(t1b, n);
+    V3a dnub = sa(-coso, Dub), dnvb = sa(-coso, Dvb);
+    const float qub = -da(Dub, n), qvb = -da(Dvb, n);
+    acc3(nb, sa(-qu, Dub));
+    acc3(nb, sa(-qv, Dvb));
+    acc3(nb, sa(-coso, t1b));
+    const float f1b = qub * ddu + qvb * ddv;
+    const float ddub = qub * f1, ddvb = qvb * f1;
+    acc3(dnub, sa(ddub, d));
+    acc3(dnvb, sa(ddvb, d));
+    acc3(nb, sa(ddub, Dt));
+    acc3(nb, sa(ddvb, Dp));
+    float cosib = e1 * cosob - (e1 * e1) * ing1 * f1b;
+    const float ng1b = -cosob + (e1 * e1) * cosi * ing1 * ing1 * f1b;
+    const float k1b = 0.5f * ng1b * ing1;
+    cosib += 2.f * e1 * e1 * cosi * k1b;
+    acc3(nb, sa(cosib, d));
+    // dn = (nn dN - w Nt) / nn^1.5
+    V3a Ntb = va(0.f, 0.f, 0.f);
+    float nnb = 0.f, nl3b = 0.f;
+    V3a dNub = sa(nn * inl3, dnub), dNvb = sa(nn * inl3, dnvb);
+    const float wub = -da(dnub, Nt) * inl3, wvb = -da(dnvb, Nt) * inl3;
+    acc3(dNub, sa(wub, Nt));
+    acc3(dNvb, sa(wvb, Nt));
+    acc3(Ntb, sa(wub, dNu));
+    acc3(Ntb, sa(wvb, dNv));
+    acc3(Ntb, sa(-wu * inl3, dnub));
+    acc3(Ntb, sa(-wv * inl3, dnvb));
+    nnb += (da(dnub, dNu) + da(dnvb, dNv)) * inl3;
+    nl3b -= (da(dnub, dnu) + da(dnvb, dnv)) * inl3;
+    nnb += 1.5f * nlen * nl3b;
+    Sb[3] = dNub.x * Du1.x + dNvb.x * Dv1.x;  // Nxx
+    Sb[5] = dNub.x * Du1.y + dNvb.x * Dv1.y;  // Nxy
+    Sb[4] = dNub.y * Du1.x + dNvb.y * Dv1.x;  // Nyx
+    Sb[6] = dNub.y * Du1.y + dNvb.y * Dv1.y;  // Nyy
+    Du1b.x += dNub.x * Nxx + dNub.y * Nyx;
+    Du1b.y += dNub.x * Nxy + dNub.y * Nyy;
+    Dv1b.x += dNvb.x * Nxx + dNvb.y * Nyx;
+    Dv1b.y += dNvb.x * Nxy + dNvb.y * Nyy;
+    // Du1 = t (Dt - aT d), aT = (n . Dt) / nd (Dv1 with Dp)
+    tb += da(Du1b, Eu) + da(Dv1b, Ev);
+    const float aTb = -t * da(Du1b, d), aPb = -t * da(Dv1b, d);
+    acc3(nb, sa(aTb * ind, Dt));
+    acc3(nb, sa(aPb * ind, Dp));
+    const float ndb = -(aTb * aT + aPb * aP) * ind;
+    acc3(nb, sa(ndb, d));
+    // n = Nt / sqrt(nn)
+    acc3(Ntb, sa(inl, nb));
+    const float inlb = da(nb, Nt);
+    nnb += -0.5f * inl * inl * inl * inlb;
+    Sb[0] = 0.f;  // the height enters through t only
+    Sb[1] = Ntb.x + 2.f * Nx * nnb;
+    Sb[2] = Ntb.y + 2.f * Ny * nnb;
+    return true;
+}
+
 struct PointArgs {
     const float* h;
     int H, W;
@@ -890,40 +998,24 @@ __global__ __launch_bounds__(256) void point_bwd_kernel(PointArgs a) {
         Bilin b;
         SurfGeo geo;
         if (!trace_hit(a.h, a.H, a.W, a.P.texel, a.plane_z, r, t, b, s, geo, fp)) continue;
-        // component 0: the hit parameter t (the scalars follow the hit along the ray: their
-        // position derivatives times d); components 1-6: the normal scalars at a fixed position
-        Dual v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            v[k] = dconst(s[k]);
-            v[k].d[k] = 1.f;
-        }
-        v[0].v = t;
-        v[1].d[0] = s[3] * r.dx + s[5] * r.dy;
-        v[2].d[0] = s[4] * r.dx + s[6] * r.dy;
-        v[3].d[0] = geo.tw_nx * r.dy;
-        v[4].d[0] = geo.tw_ny * r.dy;
-        v[5].d[0] = geo.tw_nx * r.dx;
-        v[6].d[0] = geo.tw_ny * r.dx;
         const V3<float> Dt = {a.dth[i], a.dth[n + i], a.dth[2 * n + i]};
         const V3<float> Dp = {a.dph[i], a.dph[n + i], a.dph[2 * n + i]};
-        Dual xr, yr, Dux, Duy, Dvx, Dvy;
-        point_chain<Dual>(v[0], v[1], v[2], v[3], v[4], v[5], v[6], r, Dt, Dp, a.P, xr, yr, Dux,
-                          Duy, Dvx, Dvy);
-        const Dual den = Dux * Dvy - Duy * Dvx;
-        if (den.v == 0.f) continue;
-        const Dual f = dconst(2.f) / den;
-        const float gE = a.gE[i];
-        const float g0 = a.gM[i], g1 = a.gM[n + i], g3 = a.gM[3 * n + i], g4 = a.gM[4 * n + i];
-        Dual L = a.gX[i] * xr + a.gX[n + i] * yr;
-        L = L + g0 * (f * Dvy) + (-g1) * (f * Dvx) + (-g3) * (f * Duy) + g4 * (f * Dux);
-        L = L + (4.f * a.flux[i] * gE) * (dconst(1.f) / dabs(den));
-        // the hit moves with the heights: dt / dh_j = w_j / f'(t) for the bilinear weights w_j
-        // of the hit's cell
+        float tb, Sb[K];
+        if (!point_chain_adjoint(t, s, r, Dt, Dp, a.P, a.gX[i], a.gX[n + i], a.gM[i],
+                                 a.gM[n + i], a.gM[3 * n + i], a.gM[4 * n + i],
+                                 4.f * a.flux[i] * a.gE[i], tb, Sb))
+            continue;
+        // d L / d t along the ray: t itself, and the normal scalars following the hit (their
+        // position derivatives times d); the hit moves with the heights, dt / dh_j = w_j / f'(t)
+        // for the bilinear weights w_j of the hit's cell
+        const float Lt = tb + Sb[1] * (s[3] * r.dx + s[5] * r.dy) +
+                         Sb[2] * (s[4] * r.dx + s[6] * r.dy) +
+                         (Sb[3] * geo.tw_nx + Sb[4] * geo.tw_ny) * r.dy +
+                         (Sb[5] * geo.tw_nx + Sb[6] * geo.tw_ny) * r.dx;
         float c[K];
-        c[0] = L.d[0] / fp;
+        c[0] = Lt / fp;
 #pragma unroll
-        for (int k = 1; k < K; ++k) c[k] = L.d[k];
+        for (int k = 1; k < K; ++k) c[k] = Sb[k];
         // traced hits follow the photons' random directions, not the field's texel order:
         // global adds
         PatchAcc acc;

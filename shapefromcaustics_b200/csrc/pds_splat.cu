@@ -430,6 +430,27 @@ __device__ __forceinline__ bool use_coop(const Rec& r, int coop_r) {
            (rec_rx(p) >= coop_r || rec_ry(p) >= coop_r);
 }
 
+// Records of the next batch of photons are copied global -> shared asynchronously while the
+// current batch is splatted (two buffers of kTileThreads records after the tile's shared
+// region). Each thread copies and later reads only its own slot, so no barrier is needed:
+// cp.async.wait_group makes the thread's own copies visible to it.
+__device__ __forceinline__ int stage_offset_floats(int sw) { return (sw * sw + 3) & ~3; }
+
+__device__ __forceinline__ void stage_rec_async(Rec* dst, const Rec* src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    const char* g = reinterpret_cast<const char*>(src);
+    asm volatile(
+        "cp.async.cg.shared.global [%0], [%1], 16;\n\t"
+        "cp.async.cg.shared.global [%2], [%3], 16;"
+        :: "r"(d), "l"(g), "r"(d + 16u), "l"(g + 16) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ Rec shfl_rec(const Rec& r, int src) {
     Rec o;
     o.dx0 = __shfl_sync(0xFFFFFFFFu, r.dx0, src);
@@ -610,6 +631,7 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     __shared__ int sb[4];
     const Cfg cfg = a.cfg;
     const int sw = cfg.sw;
+    Rec* stage = reinterpret_cast<Rec*>(acc + stage_offset_floats(sw));
     for (int k = threadIdx.x; k < sw * sw; k += NT) acc[k] = 0.f;
     if (threadIdx.x == 0) {
         sb[0] = INT_MAX; sb[1] = INT_MIN; sb[2] = INT_MAX; sb[3] = INT_MIN;
@@ -622,13 +644,19 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     for (int64_t c = next_chunk(a.queue, &chunk_slot); c < nchunks;
          c = next_chunk(a.queue, &chunk_slot)) {
         const int64_t p0 = c * cfg.chunk, p1 = min(p0 + cfg.chunk, n_tile);
+        if (p0 + threadIdx.x < p1) stage_rec_async(stage + threadIdx.x, a.srecs + p0 + threadIdx.x);
+        cp_async_commit();
         Segment sg = first_segment(a, c, p0);
         TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
-        for (int64_t base = p0; base < p1; base += NT) {
+        int buf = 0;
+        for (int64_t base = p0; base < p1; base += NT, buf ^= 1) {
             const int64_t i = base + threadIdx.x;
             const bool have = i < p1;
+            cp_async_wait_all();
             Rec r = {};
-            if (have) r = a.srecs[i];
+            if (have) r = stage[buf * NT + threadIdx.x];
+            if (i + NT < p1) stage_rec_async(stage + (buf ^ 1) * NT + threadIdx.x, a.srecs + i + NT);
+            cp_async_commit();
             const int64_t bend = min(base + NT, p1);
             // The batch's segments (runs of one tile) are consecutive thread ranges; each
             // pass handles one and flushes the tile's accumulator when the next one starts.
@@ -1411,9 +1439,17 @@ cudaError_t set_smem(K kernel, size_t smem) {
 }  // namespace
 
 
+// Dynamic shared memory of a tile kernel: the tile's region (sw x sw floats) and, for the
+// band forward (staged), the two record buffers after it.
+size_t tile_smem(const TileArgs& a, bool staged) {
+    const size_t sw = size_t(a.cfg.sw);
+    if (!staged) return sw * sw * sizeof(float);
+    return (((sw * sw + 3) & ~size_t(3)) * sizeof(float)) + 2 * size_t(kTileThreads) * sizeof(Rec);
+}
+
 template <int MINB, bool ROWS>
 cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
-    const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
+    const size_t smem = tile_smem(a, !ROWS);
     auto kern = ROWS ? fwd_rows_kernel<kTileThreads, MINB> : fwd_tiles_kernel<kTileThreads, MINB>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
@@ -1432,7 +1468,7 @@ cudaError_t launch_forward_t(const TileArgs& a, cudaStream_t st) {
 
 template <int MINB, bool ROWS>
 cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
-    const size_t smem = size_t(a.cfg.sw) * a.cfg.sw * sizeof(float);
+    const size_t smem = tile_smem(a, false);
     auto kern = ROWS ? bwd_rows_kernel<kTileThreads, MINB> : bwd_tiles_kernel<kTileThreads, MINB>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
@@ -1478,12 +1514,12 @@ cudaError_t launch_forward(const TileArgs& a, cudaStream_t st) {
 
 cudaError_t launch_backward(const TileArgs& a, cudaStream_t st) {
     if (a.cfg.rows) {
-        if (a.cfg.min_blocks >= 4) return launch_backward_t<4, true>(a, st);
-        return a.cfg.min_blocks == 3 ? launch_backward_t<3, true>(a, st)
+        if (a.cfg.min_blocks_bwd >= 4) return launch_backward_t<4, true>(a, st);
+        return a.cfg.min_blocks_bwd == 3 ? launch_backward_t<3, true>(a, st)
                                      : launch_backward_t<2, true>(a, st);
     }
-    if (a.cfg.min_blocks >= 4) return launch_backward_t<4, false>(a, st);
-    return a.cfg.min_blocks == 3 ? launch_backward_t<3, false>(a, st)
+    if (a.cfg.min_blocks_bwd >= 4) return launch_backward_t<4, false>(a, st);
+    return a.cfg.min_blocks_bwd == 3 ? launch_backward_t<3, false>(a, st)
                                  : launch_backward_t<2, false>(a, st);
 }
 

@@ -2,8 +2,9 @@
 candidate list and the rule that picks a winner from the measured times."""
 from shapefromcaustics_b200 import autotune as AT
 
-# the library defaults of pds_config (include/pds_b200.h)
-DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=3, coop_radius=-1)
+# the library defaults of pds_config (include/pds_b200.h; min_blocks 0: the library's choice
+# per direction)
+DEFAULT = dict(tile=64, chunk=2048, class_bits=5, walk=3, min_blocks=0, coop_radius=-1)
 
 
 def test_first_candidate_is_the_library_default_and_all_are_valid():
@@ -16,7 +17,7 @@ def test_first_candidate_is_the_library_default_and_all_are_valid():
         assert c["chunk"] % 256 == 0
         assert 1 <= c["class_bits"] <= 6
         assert c["walk"] in (1, 2, 3, 4)
-        assert 2 <= c["min_blocks"] <= 4
+        assert c["min_blocks"] == 0 or 2 <= c["min_blocks"] <= 4
         assert c["coop_radius"] == -1 or c["coop_radius"] >= 1
 
 
