@@ -96,7 +96,7 @@ __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim&
         // photons of a warp then have similar band areas (trip counts): classes of 1/k octave
         // of the area, k = 1, 2, 3 for up to 3, 4 and 5 class bits
         const float dx0 = corner_offset_step(f.px_c, s2w, x);
-        const float sy = float(2.0 / double(sim.height));
+        const float sy = float(s2h);  // 2 / H, the division done once per simulation
         const Band bd = make_band(m00, m01, m10, m11, dx0, dy0, sy, 0.5f * float(sim.width),
                                   0.5f * float(sim.height), float(f.rx) + 1.f);
         int area = (2 * f.rx + 1) * (2 * f.ry + 1);

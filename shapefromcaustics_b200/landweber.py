@@ -146,6 +146,7 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
     d = torch.zeros_like(h_true)
     ws = torch.empty(int(lib().pds_landweber_workspace_bytes(H, W)), dtype=torch.uint8, device=dev)
     hist = {"discrepancy": [], "rmse": []}
+    logged = []
     for it in range(iterations):
         px, py, offset = photon_source(H, W, per_texel * sims, scene.texel, seed, offset, dev)
         hv = (base + d).requires_grad_(True)
@@ -155,8 +156,12 @@ def reconstruct(h_true, base, scene, iterations=200, sims=16, per_texel=4, image
         (fdis * scale).backward()
         landweber_update(d, hv.grad, mask, params, ws)
         if log_every and (it % log_every == 0 or it == iterations - 1):
-            hist["discrepancy"].append((it, float((2.0 * fdis.detach()).sqrt()) / tnorm2 ** 0.5))
-            hist["rmse"].append((it, float(((d - d_true) ** 2).mean().sqrt())))
+            # kept on the device (no synchronisation inside the loop), read after it
+            logged.append((it, (2.0 * fdis.detach()).sqrt() / tnorm2 ** 0.5,
+                           ((d - d_true) ** 2).mean().sqrt()))
+    for it, dis, err in logged:
+        hist["discrepancy"].append((it, float(dis)))
+        hist["rmse"].append((it, float(err)))
     rmse = float(((d - d_true) ** 2).mean().sqrt())
     return {"d": d, "rmse": rmse, "history": hist, "target": target, "photons_per_iteration": n}
 
