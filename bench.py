@@ -812,15 +812,18 @@ def plate_batch_setup(device, seed=1000, n_sims=64, n_field=256, footprint_px=3.
     return scene, h_true, h_tgt, sims, per_texel
 
 
-def check_refract_backward(batch, h, px, py, flux, gE, gX, gM, gh):
-    """The batched refraction backward alone (the last step of BatchedPlate.backward)."""
+def check_refract_backward(batch, h, px, py, flux, gh):
+    """The batched refraction backward alone (the last step of BatchedPlate.backward), from
+    the gradient records the splat backward left in the plan's workspace."""
+    import ctypes
     from shapefromcaustics_b200._lib import check, lib
     from shapefromcaustics_b200.splatting import _ptr, _stream
+    sp = batch.splat
     with torch.cuda.device(batch.device):
-        check(lib().pds_batch_refract_backward_f32(
+        check(lib().pds_batch_refract_backward_planned_f32(
             _ptr(h), h.shape[0], h.shape[1], _ptr(batch.plates_dev), _ptr(batch.begins_dev),
-            batch.n_sims, _ptr(px), _ptr(py), _ptr(flux), batch.n_total, _ptr(gE), _ptr(gX),
-            _ptr(gM), _ptr(gh), _stream(batch.device)))
+            batch.n_sims, _ptr(px), _ptr(py), _ptr(flux), batch.n_total, sp.n_tiles,
+            _ptr(sp.ws), sp.ws.numel(), ctypes.byref(sp.cfg), _ptr(gh), _stream(batch.device)))
 
 
 def run_plate_batch(args, device, steps, warmup, config=None):
@@ -894,8 +897,8 @@ def run_plate_batch(args, device, steps, warmup, config=None):
             inputs = PL.refract_forward(h, vx, vy, vf, p)
             plan = SplatPlan(*inputs, shape, MPR)
             g = plan.forward() - t_views[k]
-            gE, gX, gM = plan.backward(g)
-            PL.refract_backward(h, vx, vy, vf, p, gE, gX, gM, grad_height=gh)
+            plan.backward(g, records=True)
+            PL.refract_backward_planned(h, vx, vy, vf, p, plan, grad_height=gh)
         landweber_update(d, gh, mask, params, ws)
         torch.add(d, base, out=h)
 
@@ -949,10 +952,10 @@ def run_plate_batch(args, device, steps, warmup, config=None):
             ev[4].record(stream)
             torch.sub(img, target, out=gimg)
             ev[5].record(stream)
-            gE, gX, gM = splat.backward(gimg)  # the forward's splat inputs, kept
+            splat.backward(gimg, records=True)  # the forward's splat inputs, kept
             ev[6].record(stream)
             gh.zero_()
-            check_refract_backward(batch, h, px, py, flux, gE, gX, gM, gh)
+            check_refract_backward(batch, h, px, py, flux, gh)
             ev[7].record(stream)
             landweber_update(d, gh, mask, params, ws)
             ev[8].record(stream)

@@ -125,6 +125,8 @@ int pds_forward_planned_f32(const float* Ep, const float* xp, const float* Mp,
                             int64_t channels, int64_t height, int64_t width,
                             int32_t max_pixel_radius, float* out, void* workspace,
                             size_t workspace_bytes, const pds_config* cfg, void* stream);
+/* grad_Ep, grad_xp and grad_Mp all NULL: the gradients stay in the workspace as per-photon
+ * records for pds_refract_backward_planned_f32 (the batch variant likewise). */
 int pds_backward_planned_f32(const float* grad_pds, const float* Ep, const float* xp,
                              const float* Mp, const int64_t* cp, const float* radius,
                              int64_t n_photons, int64_t channels, int64_t height,
@@ -247,6 +249,29 @@ int pds_batch_refract_backward_f32(const float* height, int32_t rows, int32_t co
                                    const float* flux, int64_t n_photons, const float* grad_Ep,
                                    const float* grad_xp, const float* grad_Mp,
                                    float* grad_height, void* stream);
+
+/* The refraction backward reading the splat gradients from a plan's gradient records instead
+ * of grad_Ep / grad_xp / grad_Mp: pds_backward_planned_f32 (or the batch variant) called with
+ * grad_Ep = grad_xp = grad_Mp = NULL leaves each photon's gradients in the workspace as a
+ * 32-byte record, and these calls read them there, so the spread into the reference's layouts
+ * and its re-read are skipped. The plan must be of the refracted photons of these calls, in
+ * the same order, on the same workspace: channels, height, width and cfg (one simulation) or
+ * n_tiles_total and cfg (a batch) as passed to the splat calls. Photons that touch no pixel
+ * add nothing. */
+int pds_refract_backward_planned_f32(const float* height, int32_t rows, int32_t cols,
+                                     const pds_plate* plate, const float* px, const float* py,
+                                     const float* flux, int64_t n_photons, int64_t channels,
+                                     int64_t image_height, int64_t image_width,
+                                     const void* workspace, size_t workspace_bytes,
+                                     const pds_config* cfg, float* grad_height, void* stream);
+int pds_batch_refract_backward_planned_f32(const float* height, int32_t rows, int32_t cols,
+                                           const pds_plate* plates_dev,
+                                           const int64_t* begins_dev, int32_t n_sims,
+                                           const float* px, const float* py, const float* flux,
+                                           int64_t n_photons, int64_t n_tiles_total,
+                                           const void* workspace, size_t workspace_bytes,
+                                           const pds_config* cfg, float* grad_height,
+                                           void* stream);
 
 /* Entry points of rows * cols * per_texel photons (per_texel per texel of a rows x cols
  * height field of edge `texel`, centred on the origin), each jittered uniformly inside its

@@ -100,6 +100,12 @@ SIGNATURES = {
                                                      _P, _I64, _P, _P, _P, _P, _P, _P]),
     "pds_batch_refract_backward_f32": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P,
                                                       _I64, _P, _P, _P, _P, _P]),
+    "pds_refract_backward_planned_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate),
+                                                        _P, _P, _P, _I64, _I64, _I64, _I64, _P,
+                                                        _SZ, _CFG, _P, _P]),
+    "pds_batch_refract_backward_planned_f32": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P,
+                                                              _P, _P, _I64, _I64, _P, _SZ, _CFG,
+                                                              _P, _P]),
     "pds_refract_point_forward_f32": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(PdsPlate),
                                                      ctypes.POINTER(PdsPointLight), _P, _P, _P,
                                                      _P, _P, _I64, _P, _P, _P, _P, _P, _P]),

@@ -336,7 +336,9 @@ int forward_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tile
 int backward_impl(const float* grad, const pds::Photons& ph, const pds::SimTable& st,
                   int64_t n_tiles, int64_t image_elems, int32_t mpr, float* gE, float* gX,
                   float* gM, const pds_config* cfg, void* ws, size_t ws_bytes, cudaStream_t s) {
-    if (ph.n > 0 && (!grad || !gE || !gX || !gM))
+    // all three outputs null: the gradients stay in the workspace as records
+    const bool records = !gE && !gX && !gM;
+    if (ph.n > 0 && (!grad || (!records && (!gE || !gX || !gM))))
         return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
     pds::TileArgs a;
     int rc = tile_args(ph, st, n_tiles, mpr, cfg, ws, ws_bytes, a);
@@ -644,6 +646,74 @@ int pds_batch_refract_backward_f32(const float* h, int32_t rows, int32_t cols,
                                         nullptr, nullptr, nullptr, gE, gX, gM, gh,
                                         static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel (batch)");
+    return PDS_OK;
+}
+
+// The gradient records of a plan in ws (n photons over n_tiles tiles, configuration cfg).
+static int plan_records(const void* ws, size_t ws_bytes, int64_t n, int64_t n_tiles,
+                        const pds_config* cfg, pds::GradRecords* rec) {
+    const int64_t nb = bucket_count(cfg, n_tiles);
+    if (nb <= 0) {
+        pds_config c;
+        int rc = resolve_cfg(cfg, c);
+        return rc ? rc : fail(PDS_ERR_UNSUPPORTED, "tile count outside [1, 2^30)");
+    }
+    const Layout L = make_layout(n, nb);
+    int rc = check_ws(const_cast<void*>(ws), ws_bytes, L.total);
+    if (rc) return rc;
+    const Bufs b = bufs(const_cast<void*>(ws), L);
+    rec->inv = b.inv;
+    rec->stage = reinterpret_cast<const float*>(b.stage);
+    rec->counters = b.counters;
+    return PDS_OK;
+}
+
+int pds_refract_backward_planned_f32(const float* h, int32_t rows, int32_t cols,
+                                     const pds_plate* plate, const float* px, const float* py,
+                                     const float* flux, int64_t n, int64_t C, int64_t H,
+                                     int64_t W, const void* ws, size_t ws_bytes,
+                                     const pds_config* cfg, float* gh, void* stream) {
+    int rc = check_plate(h, rows, cols, plate, px, py, flux, n);
+    if (rc) return rc;
+    if (n > 0 && !gh) return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
+    pds_sim sim;
+    int64_t nt;
+    rc = single_tiles(cfg, C, H, W, &nt, &sim, n);
+    if (rc) return rc;
+    pds::GradRecords rec;
+    rc = plan_records(ws, ws_bytes, n, nt, cfg, &rec);
+    if (rc) return rc;
+    cudaError_t e = pds::launch_refract(true, h, rows, cols, *plate, nullptr, nullptr, 0, px, py,
+                                        flux, nullptr, n, nullptr, nullptr, nullptr, nullptr,
+                                        nullptr, nullptr, nullptr, nullptr, gh,
+                                        static_cast<cudaStream_t>(stream), &rec);
+    if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel (records)");
+    return PDS_OK;
+}
+
+int pds_batch_refract_backward_planned_f32(const float* h, int32_t rows, int32_t cols,
+                                           const pds_plate* plates_dev, const int64_t* begins_dev,
+                                           int32_t n_sims, const float* px, const float* py,
+                                           const float* flux, int64_t n, int64_t n_tiles,
+                                           const void* ws, size_t ws_bytes,
+                                           const pds_config* cfg, float* gh, void* stream) {
+    if (!plates_dev || !begins_dev || n_sims < 1)
+        return fail(PDS_ERR_INVALID_ARGUMENT, "null or empty plate table");
+    if (rows < 1 || cols < 1 || !h) return fail(PDS_ERR_INVALID_ARGUMENT, "empty height field");
+    if (n < 0) return fail(PDS_ERR_INVALID_ARGUMENT, "negative photon count");
+    if (n > 0 && (!px || !py || !flux)) return fail(PDS_ERR_INVALID_ARGUMENT, "null photon array");
+    if (n > 0 && !gh) return fail(PDS_ERR_INVALID_ARGUMENT, "null gradient array");
+    pds::GradRecords rec;
+    int rc = plan_records(ws, ws_bytes, n, n_tiles, cfg, &rec);
+    if (rc) return rc;
+    pds_plate unused;
+    std::memset(&unused, 0, sizeof(unused));
+    unused.receiver_half = 1.f;
+    cudaError_t e = pds::launch_refract(true, h, rows, cols, unused, plates_dev, begins_dev,
+                                        n_sims, px, py, flux, nullptr, n, nullptr, nullptr,
+                                        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, gh,
+                                        static_cast<cudaStream_t>(stream), &rec);
+    if (e != cudaSuccess) return cuda_fail(e, "refract_bwd_kernel (batch, records)");
     return PDS_OK;
 }
 

@@ -12,12 +12,22 @@ namespace pds {
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // refraction to the receiver (pds_refract.cu)
+// A splat plan's per-photon gradient records (the backward's output before the spread into
+// grad_Ep / grad_xp / grad_Mp): the inverse map, the 32-byte records, the plan's counters.
+struct GradRecords {
+    const uint32_t* inv;
+    const float* stage;
+    const uint32_t* counters;
+};
+
+// backward: the splat gradients from gE / gX / gM, or from rec when rec is non-null
 cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pds_plate& plate,
                            const pds_plate* plates, const int64_t* begins, int32_t n_sims,
                            const float* px, const float* py, const float* flux,
                            const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
                            int64_t* cp, float* radius, const float* gE, const float* gX,
-                           const float* gM, float* gh, cudaStream_t st);
+                           const float* gM, float* gh, cudaStream_t st,
+                           const GradRecords* rec = nullptr);
 
 cudaError_t launch_refract_point(bool backward, const float* h, int H, int W,
                                  const pds_plate& plate, const pds_point_light& light,

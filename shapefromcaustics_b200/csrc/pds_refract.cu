@@ -29,6 +29,7 @@
 
 #include "../../include/pds_b200.h"
 #include "pds_chain.cuh"
+#include "pds_device.cuh"
 #include "pds_internal.h"
 
 namespace pds {
@@ -140,12 +141,32 @@ struct RefractArgs {
     float* Mp;
     int64_t* cp;
     float* radius;
-    // backward inputs / output
+    // backward inputs / output: the splat gradients as arrays, or (rec_inv non-null) as a
+    // plan's gradient records
     const float* gE;
     const float* gX;
     const float* gM;
+    const uint32_t* rec_inv;
+    const float4* rec_stage;
+    const uint32_t* rec_counters;
     float* gh;
 };
+
+// The splat gradients of photon i (d L / d Ep, xp, Mp[0,0..1], Mp[1,0..1]) from the plan's
+// gradient records: the values the gradient spread would write, without the spread and its
+// re-read. False for a photon that touches no pixel (zero gradients).
+__device__ __forceinline__ bool photon_grads(const RefractArgs& a, int64_t i, int64_t n_tile,
+                                             float& gE, float& gx, float& gy, float& g0,
+                                             float& g1, float& g3, float& g4) {
+    const int64_t n = a.n;
+    const uint32_t v = __ldg(a.rec_inv + i);
+    const int64_t slot = (v & kWideBit) ? n_tile + int64_t(v & ~kWideBit) : int64_t(v);
+    if (v == kInvalidPos || slot >= n) return false;
+    const float4 lo = __ldg(a.rec_stage + 2 * slot), hi = __ldg(a.rec_stage + 2 * slot + 1);
+    gE = lo.x; gx = lo.y; gy = lo.z; g0 = lo.w;
+    g1 = hi.x; g3 = hi.y; g4 = hi.z;
+    return true;
+}
 
 // The plate of photon i: its simulation's in a batch (photons of a simulation are
 // contiguous; bisection over the simulations' first photons), else the call's.
@@ -323,10 +344,13 @@ __device__ __forceinline__ void patch_end(const PatchAcc& acc, int* bb, int H, i
 
 // Three CTAs an SM (80 registers, a few spilled to the L1): measured 18% faster than the
 // 114-register build at two CTAs an SM (16.8 M photons of a 1024^2 field: 2.24 vs 2.73 ms).
+template <bool REC>
 __global__ __launch_bounds__(256, 3) void refract_bwd_kernel(RefractArgs a) {
     __shared__ float smem[kPatchSmem];
     __shared__ int bb[4];
     const int64_t n = a.n;
+    // tile-path photons of the plan whose gradient records are read (records mode)
+    const int64_t n_tile = REC ? min(int64_t(__ldg(a.rec_counters)), n) : 0;
     // CTA-contiguous blocks of 256 photons (their patches share a shared-memory region)
     for (int64_t blk = int64_t(blockIdx.x) * blockDim.x; blk < n;
          blk += int64_t(gridDim.x) * blockDim.x) {
@@ -342,9 +366,16 @@ __global__ __launch_bounds__(256, 3) void refract_bwd_kernel(RefractArgs a) {
             b = bilin(px, py, P.texel, a.H, a.W);
             float s[K];
             surface_scalars(a.h, a.H, a.W, P.texel, b, s);
-            active = plate_chain_adjoint(s, px, py, P, a.gX[i], a.gX[n + i], a.gM[i],
-                                         a.gM[n + i], a.gM[3 * n + i], a.gM[4 * n + i],
-                                         4.f * a.flux[i] * a.gE[i], c);
+            if (REC) {
+                float gE, gx, gy, g0, g1, g3, g4;
+                active = photon_grads(a, i, n_tile, gE, gx, gy, g0, g1, g3, g4) &&
+                         plate_chain_adjoint(s, px, py, P, gx, gy, g0, g1, g3, g4,
+                                             4.f * a.flux[i] * gE, c);
+            } else {
+                active = plate_chain_adjoint(s, px, py, P, a.gX[i], a.gX[n + i], a.gM[i],
+                                             a.gM[n + i], a.gM[3 * n + i], a.gM[4 * n + i],
+                                             4.f * a.flux[i] * a.gE[i], c);
+            }
         }
         const PatchAcc acc = patch_begin(smem, bb, active, b.x0, b.y0, a.gh, a.H, a.W);
         if (active) scatter_patch(a.H, a.W, texel, b, c, acc);
@@ -548,7 +579,7 @@ cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pd
                            const float* px, const float* py, const float* flux,
                            const int64_t* channel, int64_t n, float* Ep, float* xp, float* Mp,
                            int64_t* cp, float* radius, const float* gE, const float* gX,
-                           const float* gM, float* gh, cudaStream_t st) {
+                           const float* gM, float* gh, cudaStream_t st, const GradRecords* rec) {
     if (n <= 0) return cudaSuccess;
     RefractArgs a;
     a.h = h;
@@ -571,9 +602,14 @@ cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pd
     a.gE = gE;
     a.gX = gX;
     a.gM = gM;
+    a.rec_inv = rec ? rec->inv : nullptr;
+    a.rec_stage = rec ? reinterpret_cast<const float4*>(rec->stage) : nullptr;
+    a.rec_counters = rec ? rec->counters : nullptr;
     a.gh = gh;
-    if (backward)
-        refract_bwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+    if (backward && rec)
+        refract_bwd_kernel<true><<<grid_for(n), 256, 0, st>>>(a);
+    else if (backward)
+        refract_bwd_kernel<false><<<grid_for(n), 256, 0, st>>>(a);
     else
         refract_fwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
     return cudaGetLastError();

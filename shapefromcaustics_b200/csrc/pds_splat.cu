@@ -1484,6 +1484,9 @@ cudaError_t launch_backward_t(const TileArgs& a, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         // the quad form needs the inverse map 16-byte aligned (the workspace is) and every
         // output 4-byte aligned; the rows' own alignment is handled per store
+        // no outputs: the gradients stay in the workspace as records (read by the refraction
+        // backward's records mode)
+        if (!a.gE) return cudaSuccess;
         const auto al = [](const void* p, uintptr_t m) {
             return (reinterpret_cast<uintptr_t>(p) & m) == 0;
         };

@@ -175,7 +175,7 @@ def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4,
     refraction and the plan recomputed for the backward,) splat backward, refraction backward,
     update. The height field is ``base + d``; ``d`` is updated in place."""
     import statistics
-    from .plate import plate_params, refract_backward, refract_forward
+    from .plate import plate_params, refract_backward_planned, refract_forward
     from .splatting import SplatPlan
     dev = d.device
     H, W = d.shape
@@ -205,9 +205,9 @@ def iteration_phases(base, target, scene, d, mask, params, sims=16, per_texel=4,
         if not keep_plan:
             plan = SplatPlan(*refract_forward(hv, px, py, flux, pp), shape, 20)
         ev[6].record()
-        gE, gX, gM = plan.backward(g_img)
+        plan.backward(g_img, records=True)
         ev[7].record()
-        gh = refract_backward(hv, px, py, flux, pp, gE, gX, gM)
+        gh = refract_backward_planned(hv, px, py, flux, pp, plan)
         ev[8].record()
         landweber_update(d, gh, mask, params, ws)
         ev[9].record()

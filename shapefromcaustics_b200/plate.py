@@ -83,6 +83,22 @@ def refract_backward(height, px, py, flux, params, gE, gX, gM, grad_height=None)
     return grad_height
 
 
+def refract_backward_planned(height, px, py, flux, params, plan, grad_height=None):
+    """Adds d L / d height from the gradient records that ``plan.backward(g, records=True)``
+    left in the plan's workspace (``pds_refract_backward_planned_f32``): the refraction
+    backward without the gradients' spread into grad_Ep / grad_xp / grad_Mp. ``plan`` is the
+    ``SplatPlan`` of these photons' refracted splat inputs."""
+    n = px.numel()
+    if grad_height is None:
+        grad_height = torch.zeros_like(height)
+    with torch.cuda.device(height.device):
+        check(_fn("pds_refract_backward_planned_f32")(
+            _ptr(height), height.shape[0], height.shape[1], ctypes.byref(params), _ptr(px),
+            _ptr(py), _ptr(flux), n, plan.C, plan.H, plan.W, _ptr(plan.ws), plan.ws.numel(),
+            ctypes.byref(plan.cfg), _ptr(grad_height), _stream(height.device)))
+    return grad_height
+
+
 class PlateSplat(torch.autograd.Function):
     """Caustic image of a height-field plate; differentiable in the height field."""
 
@@ -122,8 +138,10 @@ class PlateSplat(torch.autograd.Function):
             plan.ws = ctx.plan_ws
         else:
             plan = SplatPlan(Ep, xp, Mp, cp, radius, ctx.shape, ctx.mpr, config=ctx.cfg)
-        gE, gX, gM = plan.backward(grad_img.contiguous())
-        gh = refract_backward(h, px, py, flux, ctx.params, gE, gX, gM)
+        # the splat gradients stay in the plan's workspace as records, read there by the
+        # refraction backward
+        plan.backward(grad_img.contiguous(), records=True)
+        gh = refract_backward_planned(h, px, py, flux, ctx.params, plan)
         ctx.plan_ws = None
         ctx.inputs = None
         return gh, None, None, None, None, None, None, None
@@ -246,8 +264,9 @@ class BatchedPlate:
     ``sims`` is a list of ``(n_photons, (C, H, W), pds_plate)``; photons are the simulations'
     entry points concatenated in order. The forward refracts every photon in one batched launch
     (``pds_batch_refract_forward_f32``) and splats all simulations through one plan and one
-    forward (``BatchedSplat``); the backward runs the batched splat backward and one batched
-    refraction backward into the height field's gradient. ``keep_inputs``: the refracted splat
+    forward (``BatchedSplat``); the backward runs the batched splat backward, leaving its
+    gradients as records in the plan's workspace, and one batched refraction backward that
+    reads them there into the height field's gradient. ``keep_inputs``: the refracted splat
     inputs of the forward are kept for the backward (as the reference's PDS saves them);
     False recomputes them there (48 B per photon less held between the passes). The reference
     runs its simulations one after another and sums them (``shape_from_caustics.py:351-353``);
@@ -308,17 +327,20 @@ class BatchedPlate:
         height field and photons)."""
         if not self.keep_inputs or self.splat.inputs is None:
             self.splat.inputs = self._inputs(height, px, py, flux)
-        gE, gX, gM = self.splat.backward(grad_flat)
+        # the splat gradients stay in the plan's workspace as records, read there by the
+        # batched refraction backward
+        self.splat.backward(grad_flat, records=True)
         if not self.keep_inputs:
             self.splat.inputs = None
         if grad_height is None:
             grad_height = torch.zeros_like(height)
+        sp = self.splat
         with torch.cuda.device(self.device):
-            check(_fn("pds_batch_refract_backward_f32")(
+            check(_fn("pds_batch_refract_backward_planned_f32")(
                 _ptr(height), height.shape[0], height.shape[1], _ptr(self.plates_dev),
                 _ptr(self.begins_dev), self.n_sims, _ptr(px), _ptr(py), _ptr(flux),
-                self.n_total, _ptr(gE), _ptr(gX), _ptr(gM), _ptr(grad_height),
-                _stream(self.device)))
+                self.n_total, sp.n_tiles, _ptr(sp.ws), sp.ws.numel(), ctypes.byref(sp.cfg),
+                _ptr(grad_height), _stream(self.device)))
         return grad_height
 
     def images(self, flat):

@@ -125,21 +125,27 @@ class SplatPlan:
                                                 ctypes.byref(self.cfg), _stream(self.device)))
         return out
 
-    def backward(self, grad_pds, out=None):
+    def backward(self, grad_pds, out=None, records=False):
+        """[grad_Ep, grad_xp, grad_Mp]; with ``records`` the gradients stay in the plan's
+        workspace as per-photon records (for ``plate.refract_backward_planned``) and None is
+        returned."""
         _check_input(grad_pds, "grad_pds")
         if tuple(grad_pds.shape) != (self.C, self.H, self.W) or grad_pds.dtype != torch.float32:
             raise RuntimeError("grad_pds must be a float32 tensor of the forward's output_size")
         Ep, xp, Mp = self.inputs[:3]
-        if out is None:
-            out = (torch.empty_like(Ep), torch.empty_like(xp), torch.empty_like(Mp))
-        gE, gx, gM = out
+        if records:
+            gE = gx = gM = None
+        else:
+            if out is None:
+                out = (torch.empty_like(Ep), torch.empty_like(xp), torch.empty_like(Mp))
+            gE, gx, gM = out
         with torch.cuda.device(self.device):
             check(lib().pds_backward_planned_f32(_ptr(grad_pds), *(_ptr(t) for t in self.inputs),
                                                  self.n, self.C, self.H, self.W, self.mpr,
                                                  _ptr(gE), _ptr(gx), _ptr(gM), _ptr(self.ws),
                                                  self.ws.numel(), ctypes.byref(self.cfg),
                                                  _stream(self.device)))
-        return [gE, gx, gM]
+        return None if records else [gE, gx, gM]
 
 
 def pds_forward(Ep, xp, Mp, cp, radius, output_size, max_pixel_radius):
@@ -258,13 +264,19 @@ class BatchedSplat:
                                                       _stream(self.device)))
         return out
 
-    def backward(self, grad_flat, out=None):
+    def backward(self, grad_flat, out=None, records=False):
+        """(grad_Ep, grad_xp, grad_Mp) of the batch's photons; with ``records`` the gradients
+        stay in the plan's workspace as per-photon records (for
+        ``plate.BatchedPlate.backward``) and None is returned."""
         self._planned("backward")
         self._check_flat(grad_flat, "grad")
         Ep, xp, Mp = self.inputs[:3]
-        if out is None:
-            out = (torch.empty_like(Ep), torch.empty_like(xp), torch.empty_like(Mp))
-        gE, gx, gM = out
+        if records:
+            gE = gx = gM = None
+        else:
+            if out is None:
+                out = (torch.empty_like(Ep), torch.empty_like(xp), torch.empty_like(Mp))
+            gE, gx, gM = out
         with torch.cuda.device(self.device):
             check(lib().pds_batch_backward_planned_f32(_ptr(grad_flat),
                                                        *(_ptr(t) for t in self.inputs),
@@ -273,7 +285,7 @@ class BatchedSplat:
                                                        _ptr(gx), _ptr(gM), _ptr(self.ws),
                                                        self.ws.numel(), ctypes.byref(self.cfg),
                                                        _stream(self.device)))
-        return gE, gx, gM
+        return None if records else (gE, gx, gM)
 
     def images(self, flat):
         return [flat[o:o + C * H * W].view(C, H, W)

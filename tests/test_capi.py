@@ -112,3 +112,34 @@ def test_batch_image_ranges_are_checked_on_host():
     t[2].image_offset = -1
     with pytest.raises(_lib.PdsError, match="negative"):
         _lib.check(lib.pds_batch_image_elems(t, 3, ctypes.byref(n)))
+
+
+def test_records_mode_argument_errors_without_a_device():
+    # the refraction backward from a plan's gradient records: plate, gradient and workspace
+    # are checked before anything is enqueued; a splat backward with some but not all of its
+    # gradient outputs null is rejected (all null: the records mode)
+    lib = _lib.lib()
+    p = ctypes.c_void_p(256)
+    plate = _lib.PdsPlate()
+    plate.texel, plate.ior, plate.receiver_half, plate.receiver_distance = 0.1, 1.5, 10.0, 50.0
+    rc = lib.pds_refract_backward_planned_f32(p, 8, 8, None, p, p, p, 5, 1, 8, 8, p, 1 << 20,
+                                              None, p, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"plate" in lib.pds_last_error()
+    rc = lib.pds_refract_backward_planned_f32(p, 8, 8, ctypes.byref(plate), p, p, p, 5, 1, 8, 8,
+                                              p, 1 << 20, None, None, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"null" in lib.pds_last_error()
+    rc = lib.pds_refract_backward_planned_f32(p, 8, 8, ctypes.byref(plate), p, p, p, 5, 1, 8, 8,
+                                              p, 10, None, p, None)
+    assert rc == _lib.PDS_ERR_WORKSPACE
+    rc = lib.pds_refract_backward_planned_f32(p, 8, 8, ctypes.byref(plate), p, p, p, 5, 1, 8, 8,
+                                              ctypes.c_void_p(16), 1 << 20, None, p, None)
+    assert rc == _lib.PDS_ERR_WORKSPACE and b"aligned" in lib.pds_last_error()
+    rc = lib.pds_batch_refract_backward_planned_f32(p, 8, 8, None, None, 0, p, p, p, 5, 4, p,
+                                                    1 << 20, None, p, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"plate table" in lib.pds_last_error()
+    rc = lib.pds_batch_refract_backward_planned_f32(p, 8, 8, p, p, 1, p, p, p, 5, 4, p, 10,
+                                                    None, p, None)
+    assert rc == _lib.PDS_ERR_WORKSPACE
+    rc = lib.pds_backward_planned_f32(p, p, p, p, p, p, 5, 1, 8, 8, 20, p, None, None, p, 1 << 20,
+                                      None, None)
+    assert rc == _lib.PDS_ERR_INVALID_ARGUMENT and b"null gradient" in lib.pds_last_error()

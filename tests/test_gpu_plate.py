@@ -364,3 +364,45 @@ def test_batched_plate_kept_and_recomputed_inputs_agree(cuda):
         assert (batch.splat.inputs is not None) == keep
     torch.cuda.synchronize()
     assert rel_l2(grads[0].cpu(), grads[1].cpu()) < 1e-6
+
+
+def test_refraction_backward_from_gradient_records_equals_arrays(cuda):
+    """The refraction backward reading the splat gradients from the plan's gradient records
+    (``records=True`` + ``pds_refract_backward_planned_f32``, the batch variant likewise)
+    gives the height gradient of the spread arrays' path (same values; only the order of the
+    float atomic sums into the field differs)."""
+    from shapefromcaustics_b200 import plate as PL
+    from shapefromcaustics_b200._lib import check, lib
+    from shapefromcaustics_b200.splatting import SplatPlan, _ptr, _stream
+    scene, h, ph, du0 = scene_and_photons(seed=9)
+    params = PL.plate_params(scene, du0)
+    h = h.cuda()
+    px, py, flux = (t.float().cuda() for t in (ph[0], ph[1], ph[4]))
+    shape = (1, 96, 96)
+    plan = SplatPlan(*PL.refract_forward(h, px, py, flux, params), shape, 20)
+    g = torch.randn(shape, generator=torch.Generator("cuda").manual_seed(5), device="cuda")
+    plan.forward()
+    gE, gX, gM = plan.backward(g)
+    gh_arrays = PL.refract_backward(h, px, py, flux, params, gE, gX, gM)
+    assert plan.backward(g, records=True) is None
+    gh_records = PL.refract_backward_planned(h, px, py, flux, params, plan)
+    torch.cuda.synchronize()
+    assert float(gh_arrays.abs().max()) > 0
+    assert rel_l2(gh_records.cpu(), gh_arrays.cpu()) < 1e-6
+    # a batch of plates: BatchedPlate.backward (records) against the arrays' path
+    hb, sims, photons = plate_batch()
+    cat = [torch.cat([p[k] for p in photons]).contiguous() for k in range(3)]
+    batch = PL.BatchedPlate(sims, 20, "cuda")
+    img = batch.forward(hb, *cat)
+    gb = torch.randn(img.shape, generator=torch.Generator("cuda").manual_seed(6), device="cuda")
+    gh_b_records = batch.backward(hb, *cat, gb)
+    gE, gX, gM = batch.splat.backward(gb)
+    gh_b_arrays = torch.zeros_like(hb)
+    with torch.cuda.device(hb.device):
+        check(lib().pds_batch_refract_backward_f32(
+            _ptr(hb), hb.shape[0], hb.shape[1], _ptr(batch.plates_dev), _ptr(batch.begins_dev),
+            batch.n_sims, _ptr(cat[0]), _ptr(cat[1]), _ptr(cat[2]), batch.n_total, _ptr(gE),
+            _ptr(gX), _ptr(gM), _ptr(gh_b_arrays), _stream(hb.device)))
+    torch.cuda.synchronize()
+    assert float(gh_b_arrays.abs().max()) > 0
+    assert rel_l2(gh_b_records.cpu(), gh_b_arrays.cpu()) < 1e-6
