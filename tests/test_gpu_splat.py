@@ -79,7 +79,7 @@ def test_uniform_cluster_512(cuda):
                                  dict(walk=3, class_bits=5), dict(walk=4, min_blocks=2),
                                  dict(walk=4, class_bits=5), dict(walk=4, tile=32),
                                  dict(walk=4, coop_radius=4), dict(walk=4, class_bits=-1),
-                                 dict(walk=4, tile=16, apron_max=5)])
+                                 dict(walk=4, tile=16, apron_max=5), dict(min_blocks=3)])
 def test_tuning_variants(cuda, cfg):
     ph = S.uniform_cluster_photons(2 ** 15, 256, 256, seed=1)
     assert_parity(ph, (1, 256, 256), 20, cfg=cfg)
@@ -336,3 +336,10 @@ def test_autotuner_picks_and_caches_a_candidate(cuda):
                                       candidates=cands, reps=1)
     assert best in cands and len(times) == 2 and all(t > 0 for t in times.values())
     assert autotune.cached(specs, 20) == best
+
+
+def test_largest_apron_with_the_forward_record_staging(cuda):
+    # max_pixel_radius 40: the 32-pixel apron, a 129 x 129 shared accumulator plus the
+    # forward's two record staging buffers (82.9 KB a CTA), footprints up to the radius cap
+    ph = S.caustic_curve_photons(2 ** 15, 384, 384, seed=21, s_range=(0.5, 40.0))
+    assert_parity(ph, (1, 384, 384), 40)
