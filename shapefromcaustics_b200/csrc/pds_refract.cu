@@ -519,12 +519,21 @@ __global__ __launch_bounds__(256) void point_bwd_kernel(PointArgs a) {
     }
 }
 
-int grid_for(int64_t n) {
-    int dev = 0, sms = 148;
+// Grid of a grid-stride refraction kernel: whole waves of resident CTAs (the occupancy of
+// this kernel x SMs, times `waves`), capped by the work. A grid with a partial last wave (the
+// backward at three CTAs an SM under a fixed 8-CTAs-an-SM grid: 2.67 waves) leaves the CTAs
+// of that wave running their whole share after the others finished (the backward 2% faster
+// in one wave; the forward, at four CTAs an SM, measured best at two).
+template <typename Kern>
+int grid_for(Kern kernel, int64_t n, int waves = 1) {
+    int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
     const int64_t blocks = (n + 255) / 256;
-    const int64_t cap = int64_t(sms) * 8;
+    const int64_t cap = int64_t(sms) * per_sm * waves;
     return int(blocks < cap ? blocks : cap);
 }
 
@@ -568,9 +577,9 @@ cudaError_t launch_refract_point(bool backward, const float* h, int H, int W,
     a.gM = gM;
     a.gh = gh;
     if (backward)
-        point_bwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+        point_bwd_kernel<<<grid_for(point_bwd_kernel, n), 256, 0, st>>>(a);
     else
-        point_fwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+        point_fwd_kernel<<<grid_for(point_fwd_kernel, n), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -607,11 +616,11 @@ cudaError_t launch_refract(bool backward, const float* h, int H, int W, const pd
     a.rec_counters = rec ? rec->counters : nullptr;
     a.gh = gh;
     if (backward && rec)
-        refract_bwd_kernel<true><<<grid_for(n), 256, 0, st>>>(a);
+        refract_bwd_kernel<true><<<grid_for(refract_bwd_kernel<true>, n), 256, 0, st>>>(a);
     else if (backward)
-        refract_bwd_kernel<false><<<grid_for(n), 256, 0, st>>>(a);
+        refract_bwd_kernel<false><<<grid_for(refract_bwd_kernel<false>, n), 256, 0, st>>>(a);
     else
-        refract_fwd_kernel<<<grid_for(n), 256, 0, st>>>(a);
+        refract_fwd_kernel<<<grid_for(refract_fwd_kernel, n, 2), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -205,10 +205,14 @@ cudaError_t launch_source(int32_t rows, int32_t cols, int32_t per_texel, float t
     if (n <= 0) return cudaSuccess;
     const int64_t pairs = (n + 1) / 2;
     const int64_t blocks = (pairs + 255) / 256;
-    int dev = 0, sms = 148;
+    // one wave of resident CTAs (a grid-stride loop; partial extra waves would idle SMs)
+    int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t cap = int64_t(sms) * 16;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, source_kernel, 256, 0) !=
+            cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t cap = int64_t(sms) * per_sm;
     source_kernel<<<unsigned(blocks < cap ? blocks : cap), 256, 0, st>>>(
         rows, cols, per_texel, texel, seed, offset, n, px, py);
     return cudaGetLastError();
