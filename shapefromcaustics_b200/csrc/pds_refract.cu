@@ -57,12 +57,6 @@ __device__ __forceinline__ Bilin bilin(float px, float py, float texel, int H, i
     return b;
 }
 
-__device__ __forceinline__ float hat(const float* h, int H, int W, int i, int j) {
-    i = min(max(i, 0), H - 1);
-    j = min(max(j, 0), W - 1);
-    return __ldg(h + int64_t(i) * W + j);
-}
-
 // Position derivatives of the surface at a sample (for the traced hit).
 struct SurfGeo {
     float hx, hy;        // slope of the bilinear height
@@ -70,25 +64,37 @@ struct SurfGeo {
 };
 
 // The seven scalars of one photon: height, Sobel normal (x, y) and their x/y derivatives;
-// with geo, also the position derivatives of the sample.
+// with geo, also the position derivatives of the sample. The cell's two rows and columns
+// with their Sobel neighbours span the 4x4 texels y0-1..y0+2 x x0-1..x0+2; each is loaded
+// once, with its row and column clamped into the field (replicate padding: a texel outside
+// the field reads its nearest border texel, for every stencil tap alike).
 __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, float texel,
                                                 const Bilin& b, float s[K],
                                                 SurfGeo* geo = nullptr) {
     const float itex = 1.f / texel;  // one quotient; the stencils multiply by it
     const float c = -0.125f * itex;
+    int col[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) col[q] = min(max(b.x0 - 1 + q, 0), W - 1);
+    float t[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const float* row = h + int64_t(min(max(b.y0 - 1 + r, 0), H - 1)) * W;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[r][q] = __ldg(row + col[q]);
+    }
+    // cell corner (r, q) is texel (r + 1, q + 1); its Sobel taps are rows r .. r + 2 and
+    // columns q .. q + 2
     float hv[2][2], nx[2][2], ny[2][2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const int i = b.y0 + r, j = min(b.x0 + q, W - 1);
-            hv[r][q] = hat(h, H, W, i, j);
-            nx[r][q] = c * (hat(h, H, W, i - 1, j + 1) - hat(h, H, W, i - 1, j - 1) +
-                            2.f * (hat(h, H, W, i, j + 1) - hat(h, H, W, i, j - 1)) +
-                            hat(h, H, W, i + 1, j + 1) - hat(h, H, W, i + 1, j - 1));
-            ny[r][q] = c * (hat(h, H, W, i + 1, j - 1) - hat(h, H, W, i - 1, j - 1) +
-                            2.f * (hat(h, H, W, i + 1, j) - hat(h, H, W, i - 1, j)) +
-                            hat(h, H, W, i + 1, j + 1) - hat(h, H, W, i - 1, j + 1));
+            hv[r][q] = t[r + 1][q + 1];
+            nx[r][q] = c * (t[r][q + 2] - t[r][q] + 2.f * (t[r + 1][q + 2] - t[r + 1][q]) +
+                            t[r + 2][q + 2] - t[r + 2][q]);
+            ny[r][q] = c * (t[r + 2][q] - t[r][q] + 2.f * (t[r + 2][q + 1] - t[r][q + 1]) +
+                            t[r + 2][q + 2] - t[r][q + 2]);
         }
     }
     auto val = [&](float v[2][2]) {
