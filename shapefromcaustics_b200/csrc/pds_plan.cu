@@ -82,7 +82,10 @@ __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim&
     if (f.rx > A || f.ry > A) return a.key_big;
     const int pcx = min(max(f.px_c, 0), sim.width - 1);
     const int pcy = min(max(f.py_c, 0), sim.height - 1);
-    const int tx = pcx / T, ty = pcy / T;
+    // the tile edge is a power of two (16, 32 or 64, checked by the configuration), so the
+    // tile of a (non-negative) centre pixel is a shift, not an integer division
+    const int tsh = __ffs(T) - 1;
+    const int tx = pcx >> tsh, ty = pcy >> tsh;
     const uint32_t tile = uint32_t(sim.tile_base) +
                           uint32_t((int32_t(ch) * sim.tiles_y + ty) * sim.tiles_x + tx);
     const float dy0 = corner_offset_step(f.py_c, s2h, y);

@@ -807,10 +807,16 @@ __device__ __forceinline__ int band_row_start(const Band& bd, const BandWalk& bw
 // change; sum t g kx^2 and sum t^2 g run over the whole band. The masked pixel of an odd row
 // (just outside the box) is read from the staged tile's spare column (the pitch is odd:
 // tile + 2 apron + 1, and a box never reaches past column tile + 2 apron - 1) and its product
-// discarded.
+// discarded. The two pixels of a step are evaluated as the two lanes of sm_100's packed FP32
+// instructions (__ffma2_rn / __fmul2_rn / __fadd2_rn: one instruction for both pixels, each
+// lane rounded as its scalar counterpart); the even and odd pixels keep separate partial sums,
+// added where a row or the band ends.
 struct BandMoments {
     float sE, A0t, B1t, B2, Sy, Sxy, Syy;
 };
+
+__device__ __forceinline__ float2 pair(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float hsum(float2 v) { return v.x + v.y; }
 
 __device__ __forceinline__ BandMoments gather_band_rows(const Band& bd, const BandWalk& bw,
                                                         int ky, int ky1, const float* row,
@@ -819,48 +825,50 @@ __device__ __forceinline__ BandMoments gather_band_rows(const Band& bd, const Ba
                                                         float sy, float dy0, float sx,
                                                         float dx0) {
     BandMoments m = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float A0 = 0.f, B1 = 0.f;
+    const float2 A00 = pair(a00), A10 = pair(a10);
+    float2 C0 = pair(c0), C1 = pair(c1);
+    float2 SE = pair(0.f), B2 = pair(0.f), A0 = pair(0.f), B1 = pair(0.f);
     int xs = band_row_start(bd, bw, ky);
-    float kf = float(xs);
+    float2 KF = make_float2(float(xs), float(xs + 1));
     const float* q = row + xs;
     int rem = bw.npairs;
     for (;;) {
-        const float u0 = fmaf(kf, a00, c0), u1 = fmaf(kf, a10, c1);
-        const float v0 = u0 + a00, v1 = u1 + a10;
-        const float s = fmaf(u0, u0, u1 * u1), s2 = fmaf(v0, v0, v1 * v1);
-        const float t = fmaxf(1.f - s, 0.f), t2 = fmaxf(1.f - s2, 0.f);
-        const float g = t * q[0];
-        const float g2 = rem == bw.tail ? 0.f : t2 * q[1];
-        const float kf1 = kf + 1.f;
-        m.sE = fmaf(t, g, m.sE);
-        m.sE = fmaf(t2, g2, m.sE);
-        A0 += g + g2;
-        const float tk = g * kf, tk2 = g2 * kf1;
-        B1 += tk + tk2;
-        m.B2 = fmaf(tk, kf, m.B2);
-        m.B2 = fmaf(tk2, kf1, m.B2);
-        kf += 2.f;
+        // u = M d at the two pixels, s = |u|^2, t = max(1 - s, 0)
+        const float2 U0 = __ffma2_rn(KF, A00, C0), U1 = __ffma2_rn(KF, A10, C1);
+        const float2 S = __ffma2_rn(U0, U0, __fmul2_rn(U1, U1));
+        const float2 T = make_float2(fmaxf(1.f - S.x, 0.f), fmaxf(1.f - S.y, 0.f));
+        const float2 Q = make_float2(q[0], rem == bw.tail ? 0.f : q[1]);
+        const float2 G = __fmul2_rn(T, Q);
+        SE = __ffma2_rn(T, G, SE);
+        A0 = __fadd2_rn(A0, G);
+        const float2 TK = __fmul2_rn(G, KF);
+        B1 = __fadd2_rn(B1, TK);
+        B2 = __ffma2_rn(TK, KF, B2);
+        KF = __fadd2_rn(KF, pair(2.f));
         q += 2;
         if (--rem == 0) {
+            const float a0 = hsum(A0), b1 = hsum(B1);
             const float dy = fmaf(float(ky), sy, dy0);
-            const float sdx = fmaf(sx, B1, dx0 * A0);
-            m.Sy = fmaf(dy, A0, m.Sy);
+            const float sdx = fmaf(sx, b1, dx0 * a0);
+            m.Sy = fmaf(dy, a0, m.Sy);
             m.Sxy = fmaf(dy, sdx, m.Sxy);
-            m.Syy = fmaf(dy * dy, A0, m.Syy);
-            m.A0t += A0;
-            m.B1t += B1;
+            m.Syy = fmaf(dy * dy, a0, m.Syy);
+            m.A0t += a0;
+            m.B1t += b1;
             if (++ky > ky1) break;
-            A0 = 0.f;
-            B1 = 0.f;
+            A0 = pair(0.f);
+            B1 = pair(0.f);
             rem = bw.npairs;
             xs = band_row_start(bd, bw, ky);
-            kf = float(xs);
-            c0 += m01sy;
-            c1 += m11sy;
+            KF = make_float2(float(xs), float(xs + 1));
+            C0 = __fadd2_rn(C0, pair(m01sy));
+            C1 = __fadd2_rn(C1, pair(m11sy));
             row += sw;
             q = row + xs;
         }
     }
+    m.sE = hsum(SE);
+    m.B2 = hsum(B2);
     return m;
 }
 
