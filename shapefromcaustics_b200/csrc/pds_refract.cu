@@ -333,16 +333,22 @@ __device__ __forceinline__ PatchAcc patch_begin(float* smem, int* bb, bool activ
     return acc;
 }
 
-// Adds the CTA's shared region to the field (all threads call it).
+// Adds the CTA's shared region to the field (all threads call it): warps take rows, lanes
+// take consecutive columns (coalesced adds, and no division to find a texel's row).
 __device__ __forceinline__ void patch_end(const PatchAcc& acc, int* bb, int H, int W) {
     __syncthreads();
     if (acc.buf) {
-        const int x1 = min(bb[1] + 2, W - 1), y1 = min(bb[3] + 2, H - 1);
+        const int y1 = min(bb[3] + 2, H - 1);
         const int rh = y1 - acc.y0 + 1;
-        for (int k = threadIdx.x; k < acc.rw * rh; k += blockDim.x) {
-            const float v = acc.buf[k];
-            if (v != 0.f)
-                atomicAdd(acc.gh + int64_t(acc.y0 + k / acc.rw) * W + acc.x0 + k % acc.rw, v);
+        const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
+        const int nw = int(blockDim.x >> 5);
+        for (int ry = warp; ry < rh; ry += nw) {
+            const float* srow = acc.buf + ry * acc.rw;
+            float* grow = acc.gh + int64_t(acc.y0 + ry) * W + acc.x0;
+            for (int rx = lane; rx < acc.rw; rx += 32) {
+                const float v = srow[rx];
+                if (v != 0.f) atomicAdd(grow + rx, v);
+            }
         }
     }
     __syncthreads();

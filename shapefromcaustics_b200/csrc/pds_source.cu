@@ -59,8 +59,19 @@ __global__ __launch_bounds__(256) void source_kernel(int32_t rows, int32_t cols,
         for (int h = 0; h < 2; ++h) {
             const int64_t i = 2 * k + h;
             if (i >= n) break;
-            const int64_t t = i % texels;
-            const float iy = float(t / cols), ix = float(t % cols);
+            // texel of photon i (32-bit quotients where the index fits: a 64-bit division is
+            // a long software sequence)
+            int64_t t, ty;
+            if (uint64_t(i) <= 0xFFFFFFFFull && texels <= 0xFFFFFFFFll) {
+                const uint32_t t32 = uint32_t(i) % uint32_t(texels);
+                const uint32_t y32 = t32 / uint32_t(cols);
+                t = t32;
+                ty = y32;
+            } else {
+                t = i % texels;
+                ty = t / cols;
+            }
+            const float iy = float(ty), ix = float(t - ty * cols);
             const float jx = unit24(h ? r.z : r.x) - 0.5f, jy = unit24(h ? r.w : r.y) - 0.5f;
             px[i] = (ix + jx - cx) * texel;
             py[i] = (iy + jy - cy) * texel;
