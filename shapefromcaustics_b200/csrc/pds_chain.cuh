@@ -23,6 +23,20 @@ constexpr int K = 7;  // height-dependent scalars of one photon
 
 PDS_HD float dsqrt(float a) { return sqrtf(a); }
 
+// Single-precision quotients of the chain. On the device they take the hardware reciprocal
+// (__fdividef: within 2 ulp of the correctly rounded quotient; a reciprocal and a multiply
+// where the IEEE quotient adds a refinement sequence and a range check), on the host (the
+// dual-number check's build) the IEEE quotient. Dual numbers divide as they define.
+PDS_HD float qdiv(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+template <class T>
+PDS_HD T qdiv(const T& a, const T& b) { return a / b; }
+
 template <class T>
 struct V3 {
     T x, y, z;
@@ -69,7 +83,7 @@ PDS_HD void refract(const V3<T>& d, const V3<T>& n, const V3<T>& Dd,
     const T neg_sq = -dsqrt(k);
     const T coso = eta * cosi - neg_sq;
     out = vsub(vscale(eta, d), vscale(coso, n));
-    const T f = cst<T>(eta) - (eta * eta) * cosi / neg_sq;
+    const T f = cst<T>(eta) - qdiv((eta * eta) * cosi, neg_sq);
     const T q = f * (vdot(Dd, n) + vdot(d, dn));
     Dout = vsub(vscale(eta, Dd), vadd(vscale(coso, dn), vscale(q, n)));
 }
@@ -79,7 +93,7 @@ PDS_HD void refract(const V3<T>& d, const V3<T>& n, const V3<T>& Dd,
 template <class T>
 PDS_HD V3<T> transfer_z(const V3<T>& D, const V3<T>& Dd, const T& s,
                                             const V3<T>& t) {
-    const T itz = cst<T>(1.f) / t.z;  // one quotient (the same t in both of a photon's calls)
+    const T itz = qdiv(cst<T>(1.f), t.z);  // one quotient (the same t in both of a photon's calls)
     const T a = D.z * itz;
     const T b = Dd.z * itz;
     return vadd(vsub(D, vscale(a, t)), vscale(s, vsub(Dd, vscale(b, t))));
@@ -96,25 +110,25 @@ PDS_HD void plate_chain(const T& hz, const T& Nx, const T& Ny, const T& Nxx,
     const V3<T> Nt = {Nx, Ny, cst<T>(1.f)};
     const T nn = vdot(Nt, Nt);
     const T nlen = dsqrt(nn);
-    const V3<T> n = vscale(cst<T>(1.f) / nlen, Nt);
+    const V3<T> n = vscale(qdiv(cst<T>(1.f), nlen), Nt);
     const T nd = vdot(n, d);
     // source-plane differentials (du0, 0, 0) and (0, du0, 0) onto the tangent plane
-    const T dnd = cst<T>(P.du0) / nd;
+    const T dnd = qdiv(cst<T>(P.du0), nd);
     const V3<T> Du1 = vsub(V3<T>{cst<T>(P.du0), cst<T>(0.f), cst<T>(0.f)}, vscale(n.x * dnd, d));
     const V3<T> Dv1 = vsub(V3<T>{cst<T>(0.f), cst<T>(P.du0), cst<T>(0.f)}, vscale(n.y * dnd, d));
     // derivative of the normalised normal along each positional differential
     const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
     const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
     const T nl3 = nn * nlen;
-    const V3<T> dnu = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
-    const V3<T> dnv = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
+    const V3<T> dnu = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
+    const V3<T> dnv = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
     // air -> glass at the top face
     const V3<T> zero = {cst<T>(0.f), cst<T>(0.f), cst<T>(0.f)};
     V3<T> t1, Ddu, Ddv, tmp;
-    refract(d, n, zero, dnu, 1.f / P.ior, t1, Ddu);
-    refract(d, n, zero, dnv, 1.f / P.ior, tmp, Ddv);
+    refract(d, n, zero, dnu, qdiv(1.f, P.ior), t1, Ddu);
+    refract(d, n, zero, dnv, qdiv(1.f, P.ior), tmp, Ddv);
     // to the bottom face z = 0
-    const T s1 = -hz / t1.z;
+    const T s1 = qdiv(-hz, t1.z);
     const V3<T> p2 = {cst<T>(px) + s1 * t1.x, cst<T>(py) + s1 * t1.y, cst<T>(0.f)};
     const V3<T> Du2 = transfer_z(Du1, Ddu, s1, t1);
     const V3<T> Dv2 = transfer_z(Dv1, Ddv, s1, t1);
@@ -124,7 +138,7 @@ PDS_HD void plate_chain(const T& hz, const T& Nx, const T& Ny, const T& Nxx,
     refract(t1, ez, Ddu, zero, P.ior, t2, Ddu2);
     refract(t1, ez, Ddv, zero, P.ior, tmp, Ddv2);
     // to the receiver plane z = -dist
-    const T s2 = cst<T>(-P.dist) / t2.z;
+    const T s2 = qdiv(cst<T>(-P.dist), t2.z);
     const V3<T> Du3 = transfer_z(Du2, Ddu2, s2, t2);
     const V3<T> Dv3 = transfer_z(Dv2, Ddv2, s2, t2);
     xr = P.inv_half * (p2.x + s2 * t2.x);
@@ -200,10 +214,10 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const V3a Nt = va(Nx, Ny, 1.f);
     const float nn = Nx * Nx + Ny * Ny + 1.f;
     const float nlen = sqrtf(nn);
-    const float inl = 1.f / nlen;
+    const float inl = qdiv(1.f, nlen);
     const V3a n = sa(inl, Nt);
     const float nd = da(n, d);
-    const float ind = 1.f / nd;
+    const float ind = qdiv(1.f, nd);
     const float au = P.du0 * n.x * ind, av = P.du0 * n.y * ind;
     const V3a Du1 = ma(va(P.du0, 0.f, 0.f), sa(au, d));
     const V3a Dv1 = ma(va(0.f, P.du0, 0.f), sa(av, d));
@@ -213,11 +227,11 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const float wu = da(Nt, dNu), wv = da(Nt, dNv);
     const V3a dnu = sa(inl3, ma(sa(nn, dNu), sa(wu, Nt)));
     const V3a dnv = sa(inl3, ma(sa(nn, dNv), sa(wv, Nt)));
-    const float e1 = 1.f / P.ior;
+    const float e1 = qdiv(1.f, P.ior);
     const float cosi = da(d, n);
     const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
     const float ng1 = -sqrtf(k1);
-    const float ing1 = 1.f / ng1;
+    const float ing1 = qdiv(1.f, ng1);
     const float coso = e1 * cosi - ng1;
     const V3a t1 = ma(sa(e1, d), sa(coso, n));
     const float f1 = e1 - (e1 * e1) * cosi * ing1;
@@ -225,7 +239,7 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const float qu = f1 * ddu, qv = f1 * ddv;
     const V3a Ddu = sa(-1.f, pa(sa(coso, dnu), sa(qu, n)));
     const V3a Ddv = sa(-1.f, pa(sa(coso, dnv), sa(qv, n)));
-    const float it1z = 1.f / t1.z;
+    const float it1z = qdiv(1.f, t1.z);
     const float s1 = -hz * it1z;
     const V3a Du2 = tz_fwd(Du1, Ddu, s1, t1, it1z);
     const V3a Dv2 = tz_fwd(Dv1, Ddv, s1, t1, it1z);
@@ -233,14 +247,14 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const float c2 = t1.z;
     const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
     const float ng2 = -sqrtf(k2);
-    const float ing2 = 1.f / ng2;
+    const float ing2 = qdiv(1.f, ng2);
     const float coso2 = e2 * c2 - ng2;
     const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
     const float f2 = e2 - (e2 * e2) * c2 * ing2;
     const float q2u = f2 * Ddu.z, q2v = f2 * Ddv.z;
     const V3a Ddu2 = ma(sa(e2, Ddu), va(0.f, 0.f, q2u));
     const V3a Ddv2 = ma(sa(e2, Ddv), va(0.f, 0.f, q2v));
-    const float it2z = 1.f / t2.z;
+    const float it2z = qdiv(1.f, t2.z);
     const float s2 = -P.dist * it2z;
     const V3a Du3 = tz_fwd(Du2, Ddu2, s2, t2, it2z);
     const V3a Dv3 = tz_fwd(Dv2, Ddv2, s2, t2, it2z);
@@ -249,7 +263,7 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const float den = Dux * Dvy - Duy * Dvx;
     if (den == 0.f) return false;
     // ---- output adjoints: L = gx xr + gy yr + (2 / den) A + cE / |den|
-    const float iden = 1.f / den;
+    const float iden = qdiv(1.f, den);
     const float f = 2.f * iden;
     const float A = g0 * Dvy - g1 * Dvx - g3 * Duy + g4 * Dux;
     const float denb = (-f * A - cE * copysignf(1.f, den) * iden) * iden;
@@ -362,20 +376,20 @@ PDS_HD void point_chain(const T& t, const T& Nx, const T& Ny, const T& Nxx,
     const V3<T> Nt = {Nx, Ny, cst<T>(1.f)};
     const T nn = vdot(Nt, Nt);
     const T nlen = dsqrt(nn);
-    const V3<T> n = vscale(cst<T>(1.f) / nlen, Nt);
+    const V3<T> n = vscale(qdiv(cst<T>(1.f), nlen), Nt);
     const T nd = vdot(n, d);
     // positional differentials carried from the light over t onto the tangent plane
-    const V3<T> Du1 = vscale(t, vsub(Dt, vscale(vdot(n, Dt) / nd, d)));
-    const V3<T> Dv1 = vscale(t, vsub(Dp, vscale(vdot(n, Dp) / nd, d)));
+    const V3<T> Du1 = vscale(t, vsub(Dt, vscale(qdiv(vdot(n, Dt), nd), d)));
+    const V3<T> Dv1 = vscale(t, vsub(Dp, vscale(qdiv(vdot(n, Dp), nd), d)));
     const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
     const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
     const T nl3 = nn * nlen;
-    const V3<T> dnu = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
-    const V3<T> dnv = vscale(cst<T>(1.f) / nl3, vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
+    const V3<T> dnu = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
+    const V3<T> dnv = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
     V3<T> t1, Ddu, Ddv, tmp;
-    refract(d, n, Dt, dnu, 1.f / P.ior, t1, Ddu);
-    refract(d, n, Dp, dnv, 1.f / P.ior, tmp, Ddv);
-    const T s1 = -p1.z / t1.z;
+    refract(d, n, Dt, dnu, qdiv(1.f, P.ior), t1, Ddu);
+    refract(d, n, Dp, dnv, qdiv(1.f, P.ior), tmp, Ddv);
+    const T s1 = qdiv(-p1.z, t1.z);
     const V3<T> p2 = {p1.x + s1 * t1.x, p1.y + s1 * t1.y, cst<T>(0.f)};
     const V3<T> Du2 = transfer_z(Du1, Ddu, s1, t1);
     const V3<T> Dv2 = transfer_z(Dv1, Ddv, s1, t1);
@@ -384,7 +398,7 @@ PDS_HD void point_chain(const T& t, const T& Nx, const T& Ny, const T& Nxx,
     V3<T> t2, Ddu2, Ddv2;
     refract(t1, ez, Ddu, zero, P.ior, t2, Ddu2);
     refract(t1, ez, Ddv, zero, P.ior, tmp, Ddv2);
-    const T s2 = cst<T>(-P.dist) / t2.z;
+    const T s2 = qdiv(cst<T>(-P.dist), t2.z);
     const V3<T> Du3 = transfer_z(Du2, Ddu2, s2, t2);
     const V3<T> Dv3 = transfer_z(Dv2, Ddv2, s2, t2);
     xr = P.inv_half * (p2.x + s2 * t2.x);
@@ -415,10 +429,10 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const V3a Nt = va(Nx, Ny, 1.f);
     const float nn = Nx * Nx + Ny * Ny + 1.f;
     const float nlen = sqrtf(nn);
-    const float inl = 1.f / nlen;
+    const float inl = qdiv(1.f, nlen);
     const V3a n = sa(inl, Nt);
     const float nd = da(n, d);
-    const float ind = 1.f / nd;
+    const float ind = qdiv(1.f, nd);
     const float aT = da(n, Dt) * ind, aP = da(n, Dp) * ind;
     const V3a Eu = ma(Dt, sa(aT, d)), Ev = ma(Dp, sa(aP, d));
     const V3a Du1 = sa(t, Eu), Dv1 = sa(t, Ev);
@@ -428,11 +442,11 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const float wu = da(Nt, dNu), wv = da(Nt, dNv);
     const V3a dnu = sa(inl3, ma(sa(nn, dNu), sa(wu, Nt)));
     const V3a dnv = sa(inl3, ma(sa(nn, dNv), sa(wv, Nt)));
-    const float e1 = 1.f / P.ior;
+    const float e1 = qdiv(1.f, P.ior);
     const float cosi = da(d, n);
     const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
     const float ng1 = -sqrtf(k1);
-    const float ing1 = 1.f / ng1;
+    const float ing1 = qdiv(1.f, ng1);
     const float coso = e1 * cosi - ng1;
     const V3a t1 = ma(sa(e1, d), sa(coso, n));
     const float f1 = e1 - (e1 * e1) * cosi * ing1;
@@ -440,7 +454,7 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const float qu = f1 * ddu, qv = f1 * ddv;
     const V3a Ddu = ma(sa(e1, Dt), pa(sa(coso, dnu), sa(qu, n)));
     const V3a Ddv = ma(sa(e1, Dp), pa(sa(coso, dnv), sa(qv, n)));
-    const float it1z = 1.f / t1.z;
+    const float it1z = qdiv(1.f, t1.z);
     const float s1 = -p1.z * it1z;
     const V3a Du2 = tz_fwd(Du1, Ddu, s1, t1, it1z);
     const V3a Dv2 = tz_fwd(Dv1, Ddv, s1, t1, it1z);
@@ -448,14 +462,14 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const float c2 = t1.z;
     const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
     const float ng2 = -sqrtf(k2);
-    const float ing2 = 1.f / ng2;
+    const float ing2 = qdiv(1.f, ng2);
     const float coso2 = e2 * c2 - ng2;
     const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
     const float f2 = e2 - (e2 * e2) * c2 * ing2;
     const float q2u = f2 * Ddu.z, q2v = f2 * Ddv.z;
     const V3a Ddu2 = ma(sa(e2, Ddu), va(0.f, 0.f, q2u));
     const V3a Ddv2 = ma(sa(e2, Ddv), va(0.f, 0.f, q2v));
-    const float it2z = 1.f / t2.z;
+    const float it2z = qdiv(1.f, t2.z);
     const float s2 = -P.dist * it2z;
     const V3a Du3 = tz_fwd(Du2, Ddu2, s2, t2, it2z);
     const V3a Dv3 = tz_fwd(Dv2, Ddv2, s2, t2, it2z);
@@ -464,7 +478,7 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const float den = Dux * Dvy - Duy * Dvx;
     if (den == 0.f) return false;
     // ---- output adjoints
-    const float iden = 1.f / den;
+    const float iden = qdiv(1.f, den);
     const float f = 2.f * iden;
     const float A = g0 * Dvy - g1 * Dvx - g3 * Duy + g4 * Dux;
     const float denb = (-f * A - cE * copysignf(1.f, den) * iden) * iden;

@@ -45,8 +45,8 @@ struct Bilin {
 };
 
 __device__ __forceinline__ Bilin bilin(float px, float py, float texel, int H, int W) {
-    float fx = px / texel + 0.5f * float(W - 1);
-    float fy = py / texel + 0.5f * float(H - 1);
+    float fx = qdiv(px, texel) + 0.5f * float(W - 1);
+    float fy = qdiv(py, texel) + 0.5f * float(H - 1);
     fx = fminf(fmaxf(fx, 0.f), float(W - 1));
     fy = fminf(fmaxf(fy, 0.f), float(H - 1));
     Bilin b;
@@ -71,7 +71,7 @@ struct SurfGeo {
 __device__ __forceinline__ void surface_scalars(const float* h, int H, int W, float texel,
                                                 const Bilin& b, float s[K],
                                                 SurfGeo* geo = nullptr) {
-    const float itex = 1.f / texel;  // one quotient; the stencils multiply by it
+    const float itex = qdiv(1.f, texel);  // one quotient; the stencils multiply by it
     const float c = -0.125f * itex;
     int col[4];
 #pragma unroll
@@ -200,7 +200,7 @@ __global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
                            Duy, Dvx, Dvy);
         const float den = Dux * Dvy - Duy * Dvx;
         const bool good = den != 0.f;
-        const float f = 2.f / (good ? den : 1.f);
+        const float f = qdiv(2.f, good ? den : 1.f);
         a.Mp[i] = f * Dvy;
         a.Mp[n + i] = -f * Dvx;
         a.Mp[2 * n + i] = 0.f;
@@ -210,7 +210,7 @@ __global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
         a.xp[i] = xr;
         a.xp[n + i] = yr;
         a.radius[i] = 0.5f * fmaxf(sqrtf(Dux * Dux + Duy * Duy), sqrtf(Dvx * Dvx + Dvy * Dvy));
-        a.Ep[i] = 4.f * a.flux[i] / (good ? fabsf(den) : 1.f);
+        a.Ep[i] = qdiv(4.f * a.flux[i], good ? fabsf(den) : 1.f);
         const int64_t ch = a.channel ? a.channel[i] : 0;
         a.cp[i] = good ? ch : -1;
     }
@@ -229,7 +229,7 @@ __device__ __forceinline__ void scatter_patch(int H, int W, float texel, const B
     for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int q = 0; q < 4; ++q) patch[r][q] = 0.f;
-    const float it = 1.f / texel;
+    const float it = qdiv(1.f, texel);
     const float sob = -0.125f * it;
     const float wv[2][2] = {{(1.f - b.ay) * (1.f - b.ax), (1.f - b.ay) * b.ax},
                             {b.ay * (1.f - b.ax), b.ay * b.ax}};
@@ -409,7 +409,7 @@ __global__ __launch_bounds__(256, 3) void refract_bwd_kernel(RefractArgs a) {
 __device__ __forceinline__ bool trace_hit(const float* h, int H, int W, float texel,
                                           float plane_z, const Ray& r, float& t, Bilin& b,
                                           float s[K], SurfGeo& geo, float& fp) {
-    t = (r.oz - plane_z) / (-r.dz);
+    t = qdiv(r.oz - plane_z, -r.dz);
     const float cx = 0.5f * float(W - 1), cy = 0.5f * float(H - 1);
     for (int it = 0; it < 10; ++it) {
         const float px = r.ox + t * r.dx, py = r.oy + t * r.dy, pz = r.oz + t * r.dz;
@@ -417,12 +417,12 @@ __device__ __forceinline__ bool trace_hit(const float* h, int H, int W, float te
         surface_scalars(h, H, W, texel, b, s, &geo);
         fp = r.dz - (geo.hx * r.dx + geo.hy * r.dy);
         if (!(fabsf(fp) > 1e-6f)) return false;
-        const float step = (pz - s[0]) / fp;
+        const float step = qdiv(pz - s[0], fp);
         t -= step;
         if (fabsf(step) <= 1e-7f * fabsf(t)) break;
     }
     const float px = r.ox + t * r.dx, py = r.oy + t * r.dy;
-    const float fx = px / texel + cx, fy = py / texel + cy;
+    const float fx = qdiv(px, texel) + cx, fy = qdiv(py, texel) + cy;
     if (!(fx >= 0.f && fx <= float(W - 1) && fy >= 0.f && fy <= float(H - 1))) return false;
     b = bilin(px, py, texel, H, W);
     surface_scalars(h, H, W, texel, b, s, &geo);
@@ -477,7 +477,7 @@ __global__ __launch_bounds__(256) void point_fwd_kernel(PointArgs a) {
         }
         const float den = Dux * Dvy - Duy * Dvx;
         const bool good = hit && den != 0.f;
-        const float f = 2.f / (good ? den : 1.f);
+        const float f = qdiv(2.f, good ? den : 1.f);
         a.Mp[i] = f * Dvy;
         a.Mp[n + i] = -f * Dvx;
         a.Mp[2 * n + i] = 0.f;
@@ -487,7 +487,7 @@ __global__ __launch_bounds__(256) void point_fwd_kernel(PointArgs a) {
         a.xp[i] = xr;
         a.xp[n + i] = yr;
         a.radius[i] = 0.5f * fmaxf(sqrtf(Dux * Dux + Duy * Duy), sqrtf(Dvx * Dvx + Dvy * Dvy));
-        a.Ep[i] = 4.f * a.flux[i] / (good ? fabsf(den) : 1.f);
+        a.Ep[i] = qdiv(4.f * a.flux[i], good ? fabsf(den) : 1.f);
         const int64_t ch = a.channel ? a.channel[i] : 0;
         a.cp[i] = good ? ch : -1;
     }
@@ -517,7 +517,7 @@ __global__ __launch_bounds__(256) void point_bwd_kernel(PointArgs a) {
                          (Sb[3] * geo.tw_nx + Sb[4] * geo.tw_ny) * r.dy +
                          (Sb[5] * geo.tw_nx + Sb[6] * geo.tw_ny) * r.dx;
         float c[K];
-        c[0] = Lt / fp;
+        c[0] = qdiv(Lt, fp);
 #pragma unroll
         for (int k = 1; k < K; ++k) c[k] = Sb[k];
         // traced hits follow the photons' random directions, not the field's texel order:
