@@ -23,20 +23,6 @@ constexpr int K = 7;  // height-dependent scalars of one photon
 
 PDS_HD float dsqrt(float a) { return sqrtf(a); }
 
-// Single-precision quotients of the chain. On the device they take the hardware reciprocal
-// (__fdividef: within 2 ulp of the correctly rounded quotient; a reciprocal and a multiply
-// where the IEEE quotient adds a refinement sequence and a range check), on the host (the
-// dual-number check's build) the IEEE quotient. Dual numbers divide as they define.
-PDS_HD float qdiv(float a, float b) {
-#ifdef __CUDA_ARCH__
-    return __fdividef(a, b);
-#else
-    return a / b;
-#endif
-}
-template <class T>
-PDS_HD T qdiv(const T& a, const T& b) { return a / b; }
-
 template <class T>
 struct V3 {
     T x, y, z;
@@ -54,6 +40,34 @@ template <class T>
 PDS_HD T cst(float v);
 template <>
 PDS_HD float cst<float>(float v) { return v; }
+
+// Single-precision quotients of the chain. On the device they take the hardware reciprocal
+// (__fdividef: within 2 ulp of the correctly rounded quotient; a reciprocal and a multiply
+// where the IEEE quotient adds a refinement sequence and a range check), on the host (the
+// dual-number check's build) the IEEE quotient. Dual numbers divide as they define.
+PDS_HD float qdiv(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+template <class T>
+PDS_HD T qdiv(const T& a, const T& b) { return a / b; }
+
+// 1 / sqrt(a) of the chain: on the device the hardware reciprocal square root (rsqrtf, within
+// 2 ulp), from which the chain also forms sqrt(a) = a / sqrt(a) (its roots are of norms >= 1
+// and of Snell's 1 - eta^2 sin^2, positive short of total internal reflection); on the host
+// the IEEE quotient of the IEEE root.
+PDS_HD float rsq(float a) {
+#ifdef __CUDA_ARCH__
+    return rsqrtf(a);
+#else
+    return 1.f / sqrtf(a);
+#endif
+}
+template <class T>
+PDS_HD T rsq(const T& a) { return cst<T>(1.f) / dsqrt(a); }
 
 struct PlateParams {
     float texel, ior, dist, inv_half, du0;
@@ -80,10 +94,11 @@ PDS_HD void refract(const V3<T>& d, const V3<T>& n, const V3<T>& Dd,
                                         const V3<T>& dn, float eta, V3<T>& out, V3<T>& Dout) {
     T cosi = vdot(d, n);
     const T k = cst<T>(1.f) - eta * eta * (cst<T>(1.f) - cosi * cosi);
-    const T neg_sq = -dsqrt(k);
+    const T rk = rsq(k);
+    const T neg_sq = -(k * rk);
     const T coso = eta * cosi - neg_sq;
     out = vsub(vscale(eta, d), vscale(coso, n));
-    const T f = cst<T>(eta) - qdiv((eta * eta) * cosi, neg_sq);
+    const T f = cst<T>(eta) + (eta * eta) * cosi * rk;
     const T q = f * (vdot(Dd, n) + vdot(d, dn));
     Dout = vsub(vscale(eta, Dd), vadd(vscale(coso, dn), vscale(q, n)));
 }
@@ -109,8 +124,8 @@ PDS_HD void plate_chain(const T& hz, const T& Nx, const T& Ny, const T& Nxx,
     const V3<T> d = {cst<T>(P.lx), cst<T>(P.ly), cst<T>(P.lz)};
     const V3<T> Nt = {Nx, Ny, cst<T>(1.f)};
     const T nn = vdot(Nt, Nt);
-    const T nlen = dsqrt(nn);
-    const V3<T> n = vscale(qdiv(cst<T>(1.f), nlen), Nt);
+    const T inl = rsq(nn);
+    const V3<T> n = vscale(inl, Nt);
     const T nd = vdot(n, d);
     // source-plane differentials (du0, 0, 0) and (0, du0, 0) onto the tangent plane
     const T dnd = qdiv(cst<T>(P.du0), nd);
@@ -119,9 +134,9 @@ PDS_HD void plate_chain(const T& hz, const T& Nx, const T& Ny, const T& Nxx,
     // derivative of the normalised normal along each positional differential
     const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
     const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
-    const T nl3 = nn * nlen;
-    const V3<T> dnu = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
-    const V3<T> dnv = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
+    const T inl3 = inl * inl * inl;  // 1 / (nn |Nt|)
+    const V3<T> dnu = vscale(inl3, vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
+    const V3<T> dnv = vscale(inl3, vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
     // air -> glass at the top face
     const V3<T> zero = {cst<T>(0.f), cst<T>(0.f), cst<T>(0.f)};
     V3<T> t1, Ddu, Ddv, tmp;
@@ -213,8 +228,8 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     // ---- forward
     const V3a Nt = va(Nx, Ny, 1.f);
     const float nn = Nx * Nx + Ny * Ny + 1.f;
-    const float nlen = sqrtf(nn);
-    const float inl = qdiv(1.f, nlen);
+    const float inl = rsq(nn);
+    const float nlen = nn * inl;
     const V3a n = sa(inl, Nt);
     const float nd = da(n, d);
     const float ind = qdiv(1.f, nd);
@@ -230,8 +245,9 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const float e1 = qdiv(1.f, P.ior);
     const float cosi = da(d, n);
     const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
-    const float ng1 = -sqrtf(k1);
-    const float ing1 = qdiv(1.f, ng1);
+    const float rk1 = rsq(k1);
+    const float ng1 = -(k1 * rk1);
+    const float ing1 = -rk1;
     const float coso = e1 * cosi - ng1;
     const V3a t1 = ma(sa(e1, d), sa(coso, n));
     const float f1 = e1 - (e1 * e1) * cosi * ing1;
@@ -246,8 +262,9 @@ PDS_HD bool plate_chain_adjoint(const float S[K], float px, float py,
     const float e2 = P.ior;
     const float c2 = t1.z;
     const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
-    const float ng2 = -sqrtf(k2);
-    const float ing2 = qdiv(1.f, ng2);
+    const float rk2 = rsq(k2);
+    const float ng2 = -(k2 * rk2);
+    const float ing2 = -rk2;
     const float coso2 = e2 * c2 - ng2;
     const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
     const float f2 = e2 - (e2 * e2) * c2 * ing2;
@@ -375,17 +392,17 @@ PDS_HD void point_chain(const T& t, const T& Nx, const T& Ny, const T& Nxx,
     const V3<T> p1 = {cst<T>(r.ox) + t * d.x, cst<T>(r.oy) + t * d.y, cst<T>(r.oz) + t * d.z};
     const V3<T> Nt = {Nx, Ny, cst<T>(1.f)};
     const T nn = vdot(Nt, Nt);
-    const T nlen = dsqrt(nn);
-    const V3<T> n = vscale(qdiv(cst<T>(1.f), nlen), Nt);
+    const T inl = rsq(nn);
+    const V3<T> n = vscale(inl, Nt);
     const T nd = vdot(n, d);
     // positional differentials carried from the light over t onto the tangent plane
     const V3<T> Du1 = vscale(t, vsub(Dt, vscale(qdiv(vdot(n, Dt), nd), d)));
     const V3<T> Dv1 = vscale(t, vsub(Dp, vscale(qdiv(vdot(n, Dp), nd), d)));
     const V3<T> dNu = {Nxx * Du1.x + Nxy * Du1.y, Nyx * Du1.x + Nyy * Du1.y, cst<T>(0.f)};
     const V3<T> dNv = {Nxx * Dv1.x + Nxy * Dv1.y, Nyx * Dv1.x + Nyy * Dv1.y, cst<T>(0.f)};
-    const T nl3 = nn * nlen;
-    const V3<T> dnu = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
-    const V3<T> dnv = vscale(qdiv(cst<T>(1.f), nl3), vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
+    const T inl3 = inl * inl * inl;  // 1 / (nn |Nt|)
+    const V3<T> dnu = vscale(inl3, vsub(vscale(nn, dNu), vscale(vdot(Nt, dNu), Nt)));
+    const V3<T> dnv = vscale(inl3, vsub(vscale(nn, dNv), vscale(vdot(Nt, dNv), Nt)));
     V3<T> t1, Ddu, Ddv, tmp;
     refract(d, n, Dt, dnu, qdiv(1.f, P.ior), t1, Ddu);
     refract(d, n, Dp, dnv, qdiv(1.f, P.ior), tmp, Ddv);
@@ -428,8 +445,8 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const V3a p1 = va(r.ox + t * d.x, r.oy + t * d.y, r.oz + t * d.z);
     const V3a Nt = va(Nx, Ny, 1.f);
     const float nn = Nx * Nx + Ny * Ny + 1.f;
-    const float nlen = sqrtf(nn);
-    const float inl = qdiv(1.f, nlen);
+    const float inl = rsq(nn);
+    const float nlen = nn * inl;
     const V3a n = sa(inl, Nt);
     const float nd = da(n, d);
     const float ind = qdiv(1.f, nd);
@@ -445,8 +462,9 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const float e1 = qdiv(1.f, P.ior);
     const float cosi = da(d, n);
     const float k1 = 1.f - e1 * e1 * (1.f - cosi * cosi);
-    const float ng1 = -sqrtf(k1);
-    const float ing1 = qdiv(1.f, ng1);
+    const float rk1 = rsq(k1);
+    const float ng1 = -(k1 * rk1);
+    const float ing1 = -rk1;
     const float coso = e1 * cosi - ng1;
     const V3a t1 = ma(sa(e1, d), sa(coso, n));
     const float f1 = e1 - (e1 * e1) * cosi * ing1;
@@ -461,8 +479,9 @@ PDS_HD bool point_chain_adjoint(float t, const float S[K], const Ray& r,
     const float e2 = P.ior;
     const float c2 = t1.z;
     const float k2 = 1.f - e2 * e2 * (1.f - c2 * c2);
-    const float ng2 = -sqrtf(k2);
-    const float ing2 = qdiv(1.f, ng2);
+    const float rk2 = rsq(k2);
+    const float ng2 = -(k2 * rk2);
+    const float ing2 = -rk2;
     const float coso2 = e2 * c2 - ng2;
     const V3a t2 = ma(sa(e2, t1), va(0.f, 0.f, coso2));
     const float f2 = e2 - (e2 * e2) * c2 * ing2;
