@@ -272,10 +272,10 @@ __device__ __forceinline__ void scatter_patch(int H, int W, float texel, const B
 // The height-field gradient of a CTA's photons: where the CTA's photons share a compact patch
 // of the field (the photon source emits each sample's photons texel by texel in raster order,
 // so a CTA's 256 consecutive photons sit in one or two texel rows), their patches are summed
-// in shared memory and added to the
-// field once per texel; otherwise (scattered hits) each patch entry is a global atomic add.
-// Without it, every photon's 16 patch entries were global atomics on a few hot texels.
-constexpr int kPatchSmem = 8192;  // floats of the CTA's shared patch region (32 KB)
+// in shared memory and added to the field once per texel; otherwise (scattered hits) each
+// patch entry is a global atomic add. Without it, every photon's 16 patch entries were global
+// atomics on a few hot texels.
+constexpr int kPatchSmem = 8192;  // floats of the CTA's two shared patch regions (32 KB)
 
 struct PatchAcc {
     float* buf;   // shared region, rw x rh floats, or nullptr: global atomics
@@ -292,25 +292,10 @@ struct PatchAcc {
 
 // Sets up the CTA's region from its active photons' cells (bx0, by0; ignored when !active):
 // all threads call it. Returns the accumulator (shared region zeroed, or global).
-__device__ __forceinline__ PatchAcc patch_begin(float* smem, int* bb, bool active, int bx0,
-                                                int by0, float* gh, int H, int W) {
-    if (threadIdx.x == 0) {
-        bb[0] = INT_MAX; bb[1] = INT_MIN; bb[2] = INT_MAX; bb[3] = INT_MIN;
-    }
-    __syncthreads();
-    int lx0 = active ? bx0 : INT_MAX, lx1 = active ? bx0 : INT_MIN;
-    int ly0 = active ? by0 : INT_MAX, ly1 = active ? by0 : INT_MIN;
-    lx0 = __reduce_min_sync(0xFFFFFFFFu, lx0);
-    lx1 = __reduce_max_sync(0xFFFFFFFFu, lx1);
-    ly0 = __reduce_min_sync(0xFFFFFFFFu, ly0);
-    ly1 = __reduce_max_sync(0xFFFFFFFFu, ly1);
-    if ((threadIdx.x & 31) == 0 && lx0 <= lx1) {
-        atomicMin(bb + 0, lx0);
-        atomicMax(bb + 1, lx1);
-        atomicMin(bb + 2, ly0);
-        atomicMax(bb + 3, ly1);
-    }
-    __syncthreads();
+// The accumulator of the region bounded by the cells in bb (min x, max x, min y, max y): the
+// shared buffer (cap floats) when the region fits, else global atomics.
+__device__ __forceinline__ PatchAcc region_acc(float* buf, int cap, const int* bb, float* gh,
+                                               int H, int W) {
     PatchAcc acc;
     acc.gh = gh;
     acc.W = W;
@@ -321,22 +306,27 @@ __device__ __forceinline__ PatchAcc patch_begin(float* smem, int* bb, bool activ
         const int x0 = max(bb[0] - 1, 0), x1 = min(bb[1] + 2, W - 1);
         const int y0 = max(bb[2] - 1, 0), y1 = min(bb[3] + 2, H - 1);
         const int rw = x1 - x0 + 1, rh = y1 - y0 + 1;
-        if (int64_t(rw) * rh <= kPatchSmem) {
-            acc.buf = smem;
+        if (int64_t(rw) * rh <= cap) {
+            acc.buf = buf;
             acc.x0 = x0;
             acc.y0 = y0;
             acc.rw = rw;
-            for (int k = threadIdx.x; k < rw * rh; k += blockDim.x) smem[k] = 0.f;
         }
     }
-    __syncthreads();
     return acc;
 }
 
-// Adds the CTA's shared region to the field (all threads call it): warps take rows, lanes
-// take consecutive columns (coalesced adds, and no division to find a texel's row).
-__device__ __forceinline__ void patch_end(const PatchAcc& acc, int* bb, int H, int W) {
-    __syncthreads();
+// Clears a shared region (all threads call it).
+__device__ __forceinline__ void region_zero(const PatchAcc& acc, const int* bb, int H) {
+    if (acc.buf) {
+        const int rh = min(bb[3] + 2, H - 1) - acc.y0 + 1;
+        for (int k = threadIdx.x; k < acc.rw * rh; k += blockDim.x) acc.buf[k] = 0.f;
+    }
+}
+
+// Adds a shared region to the field (all threads call it): warps take rows, lanes take
+// consecutive columns (coalesced adds, and no division to find a texel's row).
+__device__ __forceinline__ void region_flush(const PatchAcc& acc, const int* bb, int H, int W) {
     if (acc.buf) {
         const int y1 = min(bb[3] + 2, H - 1);
         const int rh = y1 - acc.y0 + 1;
@@ -351,21 +341,55 @@ __device__ __forceinline__ void patch_end(const PatchAcc& acc, int* bb, int H, i
             }
         }
     }
-    __syncthreads();
 }
 
-// Three CTAs an SM (80 registers, a few spilled to the L1): measured 18% faster than the
-// 114-register build at two CTAs an SM (16.8 M photons of a 1024^2 field: 2.24 vs 2.73 ms).
+// The bounds of the CTA's active cells into bb (reset beforehand): a warp reduction, then one
+// shared atomic per warp and bound.
+__device__ __forceinline__ void region_bounds(int* bb, bool active, int bx0, int by0) {
+    int lx0 = active ? bx0 : INT_MAX, lx1 = active ? bx0 : INT_MIN;
+    int ly0 = active ? by0 : INT_MAX, ly1 = active ? by0 : INT_MIN;
+    lx0 = __reduce_min_sync(0xFFFFFFFFu, lx0);
+    lx1 = __reduce_max_sync(0xFFFFFFFFu, lx1);
+    ly0 = __reduce_min_sync(0xFFFFFFFFu, ly0);
+    ly1 = __reduce_max_sync(0xFFFFFFFFu, ly1);
+    if ((threadIdx.x & 31) == 0 && lx0 <= lx1) {
+        atomicMin(bb + 0, lx0);
+        atomicMax(bb + 1, lx1);
+        atomicMin(bb + 2, ly0);
+        atomicMax(bb + 3, ly1);
+    }
+}
+
+__device__ __forceinline__ void bounds_reset(int* bb) {
+    bb[0] = INT_MAX; bb[1] = INT_MIN; bb[2] = INT_MAX; bb[3] = INT_MIN;
+}
+
+// Three CTAs an SM (80 registers): measured 18% faster than the 114-register build at two
+// CTAs an SM (16.8 M photons of a 1024^2 field: 2.24 vs 2.73 ms).
+//
+// Consecutive blocks of a CTA alternate between two shared regions (half of kPatchSmem each)
+// and two bound arrays, so that a block's flush needs no barrier after it and the next
+// block's bounds need none before them: three barriers a block instead of five. Buffer p of
+// block k was last read by block k - 2's flush, which every thread finished before block
+// k - 1's first barrier; its bounds are reset by thread 0 after that barrier, and block k's
+// bound atomics come after block k - 1's last barrier (recon1024: 4.68 -> 4.49 ms).
 template <bool REC>
 __global__ __launch_bounds__(256, 3) void refract_bwd_kernel(RefractArgs a) {
-    __shared__ float smem[kPatchSmem];
-    __shared__ int bb[4];
+    constexpr int kHalf = kPatchSmem / 2;
+    __shared__ float smem[2 * kHalf];
+    __shared__ int bbs[2][4];
+    if (threadIdx.x == 0) {
+        bounds_reset(bbs[0]);
+        bounds_reset(bbs[1]);
+    }
+    __syncthreads();
+    int p = 0;
     const int64_t n = a.n;
     // tile-path photons of the plan whose gradient records are read (records mode)
     const int64_t n_tile = REC ? min(int64_t(__ldg(a.rec_counters)), n) : 0;
     // CTA-contiguous blocks of 256 photons (their patches share a shared-memory region)
     for (int64_t blk = int64_t(blockIdx.x) * blockDim.x; blk < n;
-         blk += int64_t(gridDim.x) * blockDim.x) {
+         blk += int64_t(gridDim.x) * blockDim.x, p ^= 1) {
         const int64_t i = blk + threadIdx.x;
         bool active = i < n;
         Bilin b = {0, 0, 0.f, 0.f};
@@ -389,9 +413,16 @@ __global__ __launch_bounds__(256, 3) void refract_bwd_kernel(RefractArgs a) {
                                              4.f * a.flux[i] * a.gE[i], c);
             }
         }
-        const PatchAcc acc = patch_begin(smem, bb, active, b.x0, b.y0, a.gh, a.H, a.W);
+        int* bb = bbs[p];
+        region_bounds(bb, active, b.x0, b.y0);
+        __syncthreads();
+        if (threadIdx.x == 0) bounds_reset(bbs[p ^ 1]);
+        const PatchAcc acc = region_acc(smem + p * kHalf, kHalf, bb, a.gh, a.H, a.W);
+        region_zero(acc, bb, a.H);
+        __syncthreads();
         if (active) scatter_patch(a.H, a.W, texel, b, c, acc);
-        patch_end(acc, bb, a.H, a.W);
+        __syncthreads();
+        region_flush(acc, bb, a.H, a.W);
     }
 }
 

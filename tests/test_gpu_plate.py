@@ -406,3 +406,52 @@ def test_refraction_backward_from_gradient_records_equals_arrays(cuda):
     torch.cuda.synchronize()
     assert float(gh_b_arrays.abs().max()) > 0
     assert rel_l2(gh_b_records.cpu(), gh_b_arrays.cpu()) < 1e-6
+
+
+def test_landweber_iteration_replays_from_a_cuda_graph(cuda):
+    """The autograd Landweber iteration (refraction + splat forward, data term, backward
+    through both, fused update) captured once in a CUDA graph: each replay gives the eager
+    iteration's update (the forward's sums are reassociated by the plan's photon order, so
+    to within float rounding, not bit for bit)."""
+    from shapefromcaustics_b200 import plate as PL
+    from shapefromcaustics_b200.landweber import LandweberParams, landweber_update
+    scene, h, ph, du0 = scene_and_photons(seed=11)
+    params = PL.plate_params(scene, du0)
+    dev = torch.device("cuda")
+    px, py, flux = (t.float().to(dev) for t in (ph[0], ph[1], ph[4]))
+    shape = (1, 128, 128)
+    with torch.no_grad():
+        target = PL.PlateSplat.apply(h.to(dev) * 1.02, px, py, flux, params, shape, 20, False)
+    base = 1.0
+    d0 = (h.to(dev) - base).contiguous()
+    d = d0.clone()
+    mask = torch.ones_like(d)
+    vol = float(d0.sum())
+    lp = LandweberParams(tau=1e-2, d1=0.75 * vol, d2=1.25 * vol)
+    ws = torch.empty(1 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        d.copy_(d0)
+        hv = (base + d).requires_grad_(True)
+        img = PL.PlateSplat.apply(hv, px, py, flux, params, shape, 20, True)
+        (0.5 * ((img - target) ** 2).sum()).backward()
+        landweber_update(d, hv.grad, mask, lp, ws)
+
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            step()
+    torch.cuda.synchronize()
+    eager = d.clone()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        step()
+    for _ in range(2):
+        d.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        upd = (eager - d0).norm()
+        assert float(upd) > 0
+        assert float((d - eager).norm() / upd) < 1e-4
+    del graph
