@@ -186,11 +186,27 @@ __device__ __forceinline__ PlateParams photon_params(const RefractArgs& a, int64
     return to_params(a.plates[lo]);
 }
 
-__global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
+// Each thread loads its next photon's entry point and flux while it refracts the current one
+// (the texel loads depend on the entry point, so an unprefetched photon waits for two memory
+// latencies in a row); five CTAs an SM (48 registers) keep the occupancy the prefetch's
+// registers would otherwise cost (recon1024: 1.44 -> 1.37 ms).
+__global__ __launch_bounds__(256, 5) void refract_fwd_kernel(RefractArgs a) {
     const int64_t n = a.n;
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * blockDim.x) {
-        const float px = a.px[i], py = a.py[i];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    float npx = 0.f, npy = 0.f, nfl = 0.f;
+    if (i < n) {
+        npx = a.px[i];
+        npy = a.py[i];
+        nfl = a.flux[i];
+    }
+    for (; i < n; i += stride) {
+        const float px = npx, py = npy, fl = nfl;
+        if (i + stride < n) {
+            npx = a.px[i + stride];
+            npy = a.py[i + stride];
+            nfl = a.flux[i + stride];
+        }
         const PlateParams P = photon_params(a, i);
         const Bilin b = bilin(px, py, P.texel, a.H, a.W);
         float s[K];
@@ -210,7 +226,7 @@ __global__ __launch_bounds__(256) void refract_fwd_kernel(RefractArgs a) {
         a.xp[i] = xr;
         a.xp[n + i] = yr;
         a.radius[i] = 0.5f * fmaxf(sqrtf(Dux * Dux + Duy * Duy), sqrtf(Dvx * Dvx + Dvy * Dvy));
-        a.Ep[i] = qdiv(4.f * a.flux[i], good ? fabsf(den) : 1.f);
+        a.Ep[i] = qdiv(4.f * fl, good ? fabsf(den) : 1.f);
         const int64_t ch = a.channel ? a.channel[i] : 0;
         a.cp[i] = good ? ch : -1;
     }
