@@ -455,3 +455,33 @@ def test_landweber_iteration_replays_from_a_cuda_graph(cuda):
         assert float(upd) > 0
         assert float((d - eager).norm() / upd) < 1e-4
     del graph
+
+
+def test_refract_backward_independent_of_photon_order(cuda):
+    """The refraction backward sums a CTA's patches in a shared region when its photons' cells
+    are compact (raster order) and adds them with global atomics when they are scattered; both
+    paths, and regions that alternate between consecutive blocks, give the same field gradient
+    (to within the float reassociation of the sums). 262 144 photons give each CTA of the
+    three-a-SM grid two or three blocks of 256."""
+    from shapefromcaustics_b200 import plate as PL
+    scene, h, ph, du0 = scene_and_photons(n=256, seed=13)
+    params = PL.plate_params(scene, du0)
+    n = ph[0].numel()
+    g = torch.Generator().manual_seed(5)
+    gE = torch.randn(n, generator=g)
+    gX = torch.randn((2, n), generator=g)
+    gM = torch.randn((2, 3, n), generator=g) * 1e-3
+    gM[:, 2] = 0
+    px, py, flux = (t.float() for t in (ph[0], ph[1], ph[4]))
+    dev = torch.device("cuda")
+    hd = h.to(dev)
+    ordered = PL.refract_backward(hd, px.to(dev), py.to(dev), flux.to(dev), params, gE.to(dev),
+                                  gX.to(dev), gM.to(dev))
+    perm = torch.randperm(n, generator=g)
+    shuffled = PL.refract_backward(hd, px[perm].to(dev), py[perm].to(dev), flux[perm].to(dev),
+                                   params, gE[perm].to(dev), gX[:, perm].contiguous().to(dev),
+                                   gM[:, :, perm].contiguous().to(dev))
+    torch.cuda.synchronize()
+    assert n > 2 * 256 * 148 * 3
+    assert float(ordered.norm()) > 0
+    assert rel_l2(shuffled.cpu(), ordered.cpu()) < 1e-5
