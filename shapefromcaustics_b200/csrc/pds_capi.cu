@@ -116,11 +116,12 @@ int resolve(const pds_config* in, int32_t mpr, int64_t n_tiles, int64_t n, Resol
 
 // The plan's workspace: the inverse map, the wide list, the records in sorted order, the
 // bucket counts, starts and cursors, each plan CTA's window histogram (kept from the count pass
-// for the place pass), the chunks' tiles, and the backward's gradient records (stage, 32 bytes
-// a photon).
+// for the place pass), the chunks' tiles, each tile's largest box radius (sized by the bucket
+// count, which bounds the tile count), and the backward's gradient records (stage, 32 bytes a
+// photon).
 struct Layout {
     size_t counters, inv, wide, stage, srecs, counts, start, cursor, part, cta_hist, chunk_tile,
-        total;
+        tile_r, total;
 };
 
 // Photon count n, bucket count nb (tiles << class bits).
@@ -141,13 +142,14 @@ Layout make_layout(int64_t n, int64_t nb) {
     L.cta_hist = off;
     off += pds::align_up(size_t(pds::plan_hist_entries(int64_t(nn), int64_t(nbb))) * 4, 256);
     L.chunk_tile = off; off += pds::align_up((nn / 256 + 2) * 4, 256);  // chunks >= 256
+    L.tile_r = off; off += pds::align_up(nbb * 4, 256);
     L.total = off;
     return L;
 }
 
 struct Bufs {
     uint32_t* counters;
-    uint32_t *inv, *wide, *counts, *start, *cursor, *part, *cta_hist, *chunk_tile;
+    uint32_t *inv, *wide, *counts, *start, *cursor, *part, *cta_hist, *chunk_tile, *tile_r;
     pds::Rec* srecs;
     pds::GradRec* stage;
 };
@@ -164,6 +166,7 @@ Bufs bufs(void* ws, const Layout& L) {
     r.part = reinterpret_cast<uint32_t*>(b + L.part);
     r.cta_hist = reinterpret_cast<uint32_t*>(b + L.cta_hist);
     r.chunk_tile = reinterpret_cast<uint32_t*>(b + L.chunk_tile);
+    r.tile_r = reinterpret_cast<uint32_t*>(b + L.tile_r);
     r.srecs = reinterpret_cast<pds::Rec*>(b + L.srecs);
     r.stage = reinterpret_cast<pds::GradRec*>(b + L.stage);
     return r;
@@ -250,6 +253,7 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     const Bufs b = bufs(ws, L);
     cudaError_t e = cudaMemsetAsync(b.counters, 0, 16, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.counts, 0, size_t(r.n_buckets) * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.tile_r, 0, size_t(n_tiles) * 4, s);
     if (e != cudaSuccess) return cuda_fail(e, "plan: counter reset");
     pds::PlanArgs a;
     a.ph = ph;
@@ -265,6 +269,7 @@ int plan_impl(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.cta_hist = b.cta_hist;
     a.cursor = b.cursor;
     a.srecs = b.srecs;
+    a.tile_r = b.tile_r;
     pds::plan_shape(ph.n, r.n_buckets, &a.window, &a.range);
     e = pds::launch_plan_count(a, s);
     if (e != cudaSuccess) return cuda_fail(e, "plan count pass");
@@ -309,6 +314,7 @@ int tile_args(const pds::Photons& ph, const pds::SimTable& st, int64_t n_tiles, 
     a.chunk_tile = b.chunk_tile;
     a.inv = b.inv;
     a.wide = b.wide;
+    a.tile_r = b.tile_r;
     a.stage = b.stage;
     a.counters = b.counters;
     a.queue = b.counters + 4;  // [0..3) plan counters; [4] the tile kernels' work counter

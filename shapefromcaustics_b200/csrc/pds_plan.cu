@@ -65,14 +65,14 @@ __device__ __forceinline__ void zero_window(uint32_t* hist, int window) {
     for (int j = threadIdx.x; j < window; j += blockDim.x) hist[j] = 0u;
 }
 
-// The bucket of one photon (key_invalid, key_big, or (tile << cb) | class) and, for the tile
-// path when PLACE, its 32-byte record. Both passes run it on the same inputs, so they agree
-// on every key.
+// The bucket of one photon (key_invalid, key_big, or (tile << cb) | class), for the tile path
+// its box radius max(rx, ry) in rmax, and when PLACE its 32-byte record. Both passes run it on
+// the same inputs, so they agree on every key.
 template <bool PLACE>
 __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim& sim, double s2w,
                                                double s2h, int64_t ch, float x, float y,
                                                float rad, float e, float m00, float m01,
-                                               float m10, float m11, Rec& r) {
+                                               float m10, float m11, Rec& r, int& rmax) {
     const int T = a.cfg.tile, A = a.cfg.apron, cb = a.cfg.class_bits;
     const uint32_t cls_max = (1u << cb) - 1u;
     if (!(ch >= 0 && ch < sim.channels)) return a.key_invalid;
@@ -80,6 +80,7 @@ __device__ __forceinline__ uint32_t bin_photon(const PlanArgs& a, const pds_sim&
     int32_t x0, x1, y0, y1;
     if (!clip_box(f, sim.height, sim.width, x0, x1, y0, y1)) return a.key_invalid;
     if (f.rx > A || f.ry > A) return a.key_big;
+    rmax = max(f.rx, f.ry);
     const int pcx = min(max(f.px_c, 0), sim.width - 1);
     const int pcy = min(max(f.py_c, 0), sim.height - 1);
     // the tile edge is a power of two (16, 32 or 64, checked by the configuration), so the
@@ -202,6 +203,7 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
             }
         }
         uint32_t key = a.key_invalid;
+        int rmax = 0;
         Rec r;
         if (valid) {
             while (i >= next_begin) {  // at most the table's length in all
@@ -215,7 +217,7 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
             }
             key = bin_photon<PLACE>(a, sim, PLACE ? corner_step(sim.width) : s2w,
                                     PLACE ? corner_step(sim.height) : s2h, ch, x, y, rad, e,
-                                    m00, m01, m10, m11, r);
+                                    m00, m01, m10, m11, r, rmax);
         }
         const bool tile_path = key < a.key_big;
         if (PLACE) {
@@ -240,6 +242,11 @@ __global__ __launch_bounds__(kPlanKernelThreads) void plan_pass_kernel(PlanArgs 
             const uint32_t j = key - kb0;
             if (j < uint32_t(a.window)) atomicAdd(hist + j, 1u);
             else atomicAdd(a.counts + key, 1u);
+            // the tile's largest box radius (the backward stages only the tile's pixels within
+            // it): an atomic only where the photon's radius exceeds the value seen (a stale,
+            // lower value only costs a redundant atomic; the value only grows)
+            uint32_t* tr = a.tile_r + (key >> a.cfg.class_bits);
+            if (uint32_t(rmax) > *tr) atomicMax(tr, uint32_t(rmax));
         }
         // wide photons: appended to the wide list (one atomic per warp)
         const uint32_t wm = __ballot_sync(0xFFFFFFFFu, wide);

@@ -685,12 +685,17 @@ __global__ __launch_bounds__(NT, MINB) void fwd_tiles_kernel(TileArgs a) {
     }
 }
 
-// Stages the tile+apron of the upstream gradient (clipped to the image): warps take rows,
+// Stages the upstream gradient that a tile's photons read (clipped to the image): the tile and
+// the pixels within r of it, r the largest box radius of the tile's photons (the plan's
+// tile_r, at most the apron), and the column after them (the band walk reads, and discards,
+// the pixel after an odd row's end; the pitch sw = tile + 2 apron + 1 has room for it). The
+// apron's outer margin, which no photon of the tile reaches, is not loaded. Warps take rows,
 // lanes take consecutive columns.
 __device__ __forceinline__ void load_region(float* tg, int sw, const TileInfo& ti,
-                                            const float* grad) {
-    const int gx0 = max(ti.ox, 0), gx1 = min(ti.ox + sw, ti.W);
-    const int gy0 = max(ti.oy, 0), gy1 = min(ti.oy + sw, ti.H);
+                                            const float* grad, int apron, uint32_t r) {
+    const int m = apron - int(min(r, uint32_t(apron)));
+    const int gx0 = max(ti.ox + m, 0), gx1 = min(ti.ox + sw - m, ti.W);
+    const int gy0 = max(ti.oy + m, 0), gy1 = min(ti.oy + sw - m, ti.H);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
     const float* img = grad + ti.img_off;
@@ -1023,7 +1028,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
         Segment sg = first_segment(a, c, p0);
         TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
         // next_chunk's barrier ends the previous chunk's reads of the staged tile
-        load_region(tg, sw, ti, a.grad);
+        load_region(tg, sw, ti, a.grad, cfg.apron, __ldg(a.tile_r + sg.tile));
         __syncthreads();
         for (int64_t base = p0; base < p1; base += NT) {
             const int64_t i = base + threadIdx.x;
@@ -1047,7 +1052,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_tiles_kernel(TileArgs a) {
                 sg = next_segment(a, sg);
                 ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
                 __syncthreads();
-                load_region(tg, sw, ti, a.grad);
+                load_region(tg, sw, ti, a.grad, cfg.apron, __ldg(a.tile_r + sg.tile));
                 __syncthreads();
             }
         }
@@ -1161,7 +1166,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_rows_kernel(TileArgs a) {
         Segment sg = first_segment(a, c, p0);
         TileInfo ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
         // next_chunk's barrier ends the previous chunk's reads of the staged tile
-        load_region(tg, sw, ti, a.grad);
+        load_region(tg, sw, ti, a.grad, cfg.apron, __ldg(a.tile_r + sg.tile));
         __syncthreads();
         for (int base = p0; base < p1; base += NT) {
             const int i = base + int(threadIdx.x);
@@ -1197,7 +1202,7 @@ __global__ __launch_bounds__(NT, MINB) void bwd_rows_kernel(TileArgs a) {
                 sg = next_segment(a, sg);
                 ti = decode_tile(a.sims, sg.tile, cfg, a.image_elems);
                 __syncthreads();
-                load_region(tg, sw, ti, a.grad);
+                load_region(tg, sw, ti, a.grad, cfg.apron, __ldg(a.tile_r + sg.tile));
                 __syncthreads();
             }
         }

@@ -32,6 +32,8 @@ struct PlanArgs {
     uint32_t* cta_hist;  // [plan_hist_entries] each CTA's window histogram, count -> place
     uint32_t* cursor;    // [key_big] place cursors (the bucket starts, from the scan)
     Rec* srecs;          // [n] out: records in sorted order (place pass)
+    uint32_t* tile_r;    // [tiles] out: the largest box radius max(rx, ry) of each tile's
+                         // tile-path photons (count pass); zeroed by the caller
     int64_t range;       // photons per CTA (plan_shape)
     int32_t window;      // buckets of each CTA's shared histogram (plan_shape)
 };
@@ -59,6 +61,7 @@ struct TileArgs {
     const uint32_t* chunk_tile;  // tile of each chunk's first photon
     const uint32_t* inv;         // per photon: sorted position, kWideBit | k, or kInvalidPos
     const uint32_t* wide;        // photon index of each wide photon
+    const uint32_t* tile_r;      // largest box radius of each tile's photons (plan)
     const uint32_t* counters;
     uint32_t* queue;             // chunk work counter of the tile kernel (zeroed before launch)
     float* out;                  // forward: flat image buffer (zeroed by caller)
