@@ -270,11 +270,11 @@ def support_pixels(specs, photons, mpr):
 # Measured DRAM traffic per photon of each phase's kernels (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum on the 2^23-photon 1024^2 workload, profiles/*__medium.md), scaled to
 # a workload by its photon count.
-TRAFFIC_PER_PHOTON = {"plan": (309.589760e6 + 11.491328e6 + 349.773568e6 +
-                               255.969024e6) / 2 ** 23,
-                      "forward": (260.904704e6 + 7.052800e6) / 2 ** 23,
-                      "backward": (262.546432e6 + 219.418880e6 + 327.270912e6 +
-                                   262.082816e6) / 2 ** 23}
+TRAFFIC_PER_PHOTON = {"plan": (309.602816e6 + 11.343360e6 + 349.815040e6 +
+                               255.564032e6) / 2 ** 23,
+                      "forward": (261.056000e6 + 6.905344e6) / 2 ** 23,
+                      "backward": (262.672896e6 + 216.617984e6 + 327.180800e6 +
+                                   263.077888e6) / 2 ** 23}
 
 
 # ------------------------------------------------------------------ our arm --------------
